@@ -1,0 +1,263 @@
+/*
+ * svdb200.h -- C ABI of the B200 implementation of single-svdlib's hot path.
+ *
+ * The boundary is the reference crate's public API (single-svdlib 1.0.9):
+ * one call here per Rust entry point, with plain pointers and sizes.  Each
+ * declaration names the reference item it replaces (paths relative to the
+ * crate root).  All dense arrays are row-major.  Host arrays passed in are
+ * borrowed for the duration of the call only (the crate's &CsrMatrix borrow);
+ * results are allocated by the library and released with svdb_rec_free.
+ *
+ * Errors: every entry point returns an svdb_status.  SvdLibError variants map
+ * one to one (src/error.rs:4-21); conditions the crate reports by panicking
+ * (assert!, todo!) return SVDB_ERR_SHAPE / SVDB_ERR_UNSUPPORTED.  The message
+ * of the last error on the calling thread is svdb_last_error_message().
+ *
+ * Threading: a matrix handle is bound to the CUDA device that was current when
+ * it was created.  Calls on different handles may run concurrently from
+ * different host threads; calls on one handle are serialised internally.
+ */
+#ifndef SVDB200_H
+#define SVDB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  1..5 are SvdLibError (src/error.rs:4-21). */
+typedef enum svdb_status {
+    SVDB_OK = 0,
+    SVDB_ERR_IMTQLB = 1,      /* SvdLibError::ImtqlbError  (src/error.rs:6) */
+    SVDB_ERR_STARTV = 2,      /* SvdLibError::StartvError  (src/error.rs:9) */
+    SVDB_ERR_STPONE = 3,      /* SvdLibError::StponeError  (src/error.rs:12) */
+    SVDB_ERR_IMTQL2 = 4,      /* SvdLibError::Imtql2Error  (src/error.rs:15) */
+    SVDB_ERR_LAS2 = 5,        /* SvdLibError::Las2Error    (src/error.rs:18) */
+    SVDB_ERR_SHAPE = 6,       /* the crate panics: assert! on shapes / bounds */
+    SVDB_ERR_CUDA = 7,        /* a CUDA runtime call failed */
+    SVDB_ERR_TIMEOUT = 8,     /* a device-side wait hit its iteration limit */
+    SVDB_ERR_UNSUPPORTED = 9, /* the crate has todo!() here, or an option not provided */
+    SVDB_ERR_ARG = 10,        /* null pointer, bad enum value */
+    SVDB_ERR_OOM = 11         /* device allocation failed */
+} svdb_status;
+
+/* Arithmetic of the sparse products.  SVDB_F64 is the drop-in (the crate's
+ * f64 path).  SVDB_MIXED stores matrix values in FP32 (SpMV accumulates in
+ * FP64; SpMM and Gram products in FP32), while the Lanczos scalars,
+ * reorthogonalisation, tridiagonal solves and the second CholeskyQR pass stay
+ * FP64. */
+typedef enum svdb_precision { SVDB_F64 = 0, SVDB_MIXED = 1 } svdb_precision;
+
+/* Which LAS2 restatement runs.  SVDB_LANCZOS follows lanczos::svd_las2 as
+ * written (src/lanczos/mod.rs:104-1406); SVDB_LEGACY follows legacy::svdLAS2
+ * (src/legacy.rs:569-2016, SVDLIBC semantics). */
+typedef enum svdb_las2_algorithm { SVDB_LANCZOS = 0, SVDB_LEGACY = 1 } svdb_las2_algorithm;
+
+/* PowerIterationNormalizer (src/randomized/mod.rs:14-19). */
+typedef enum svdb_normalizer { SVDB_NORM_QR = 0, SVDB_NORM_LU = 1, SVDB_NORM_NONE = 2 } svdb_normalizer;
+
+/* Opaque device-resident sparse operator: the SMat<T> trait object
+ * (src/utils.rs:22-33).  Holds A in CSR and in CSC (= CSR of A^T) in HBM. */
+typedef struct svdb_matrix svdb_matrix;
+
+/* Diagnostics<T> (src/utils.rs:67-79). */
+typedef struct svdb_diagnostics {
+    uint64_t non_zero;
+    uint64_t dimensions;
+    uint64_t iterations;
+    int32_t transposed;
+    uint64_t lanczos_steps;
+    uint64_t ritz_values_stabilized;
+    uint64_t significant_values;
+    uint64_t singular_values;
+    double end_interval[2];
+    double kappa;
+    uint32_t random_seed;
+} svdb_diagnostics;
+
+/* Producer of an svdb_rec; decides svdb_rec_recompose's formula. */
+typedef enum svdb_rec_origin { SVDB_REC_LANCZOS = 0, SVDB_REC_LEGACY = 1, SVDB_REC_RANDOMIZED = 2 } svdb_rec_origin;
+
+/* SvdRec<T> (src/utils.rs:44-50).  u is u_rows x u_cols row-major: d x m for
+ * LAS2 (src/lanczos/mod.rs:172), m x d for randomized_svd
+ * (src/randomized/mod.rs:175-184), as the crate returns them.  When the call
+ * asked for device results (svdb_options.result_on_device), u/s/vt are device
+ * pointers. */
+typedef struct svdb_rec {
+    uint64_t d;
+    uint64_t u_rows, u_cols;
+    double* u;
+    double* s;
+    uint64_t vt_rows, vt_cols;
+    double* vt;
+    svdb_diagnostics diagnostics;
+    int32_t on_device;
+    int32_t origin;           /* svdb_rec_origin: which entry point produced it */
+    /* Per-phase device times of the call in milliseconds (CUDA events);
+     * the verbose timers of randomized_svd (src/randomized/mod.rs:39-166). */
+    double time_ms_total;
+    double time_ms_spmv;
+    double time_ms_ortho;
+    double time_ms_tridiag;
+    double time_ms_ritvec;
+} svdb_rec;
+
+/* Internals of one LAS2 run, filled when svdb_options.trace is set: the
+ * tridiagonal T (alf: steps+1 values, bet: steps+2 values) and the Ritz values
+ * and bounds of the last lanso analysis (steps+1 values each), copied into
+ * caller arrays of `cap` doubles (truncated to cap). */
+typedef struct svdb_trace {
+    double* alf;
+    double* bet;
+    double* ritz;
+    double* bnd;
+    uint64_t cap;
+    uint64_t steps;      /* out: j of lanso */
+    uint64_t purges;     /* out: number of purge sweeps that ran */
+    int32_t sparsity_branch; /* out: 0 <= 0.9 < 1 <= 0.99 < 2 <= 0.999 < 3 */
+    int32_t lanczos_blocks;  /* out: cooperative grid size used */
+} svdb_trace;
+
+/* Options beyond the crate's arguments.  svdb_options_default fills the
+ * drop-in behaviour (f64, lanczos::*, results on the host). */
+typedef struct svdb_options {
+    int32_t precision;        /* svdb_precision */
+    int32_t algorithm;        /* svdb_las2_algorithm */
+    int32_t result_on_device; /* 1: leave u/s/vt in HBM */
+    int32_t verbose;          /* randomized_svd's verbose flag */
+    const double* omega;      /* randomized: explicit Omega (ncols x l row-major, host) or NULL */
+    void* stream;             /* cudaStream_t to run on, or NULL for the handle's stream */
+    svdb_trace* trace;        /* LAS2: optional run internals, or NULL */
+} svdb_options;
+
+void svdb_options_default(svdb_options* opts);
+
+/* ---- matrices (nalgebra_sparse storage the crate takes by reference) ---- */
+
+/* CsrMatrix<f64>: indptr[nrows+1], indices[nnz] (usize), values[nnz].
+ * Replaces `impl SMat<T> for CsrMatrix<T>` (src/lanczos/mod.rs:1506-1655). */
+int svdb_matrix_create_csr(uint64_t nrows, uint64_t ncols, uint64_t nnz, const uint64_t* indptr,
+                           const uint64_t* indices, const double* values, svdb_matrix** out);
+/* CscMatrix<f64>: colptr[ncols+1], row indices[nnz].
+ * Replaces `impl SMat<T> for CscMatrix<T>` (src/lanczos/mod.rs:1415-1504). */
+int svdb_matrix_create_csc(uint64_t nrows, uint64_t ncols, uint64_t nnz, const uint64_t* colptr,
+                           const uint64_t* rowidx, const double* values, svdb_matrix** out);
+/* CooMatrix<f64>: triplets in push order; duplicates are kept and summed by
+ * the products, as the crate's triplet loop does.
+ * Replaces `impl SMat<T> for CooMatrix<T>` (src/lanczos/mod.rs:1657-1740). */
+int svdb_matrix_create_coo(uint64_t nrows, uint64_t ncols, uint64_t nnz, const uint64_t* rows,
+                           const uint64_t* cols, const double* values, svdb_matrix** out);
+/* CSR whose arrays are already in device memory (int64 indptr, int32 column
+ * indices); the library copies them.  Same contract as svdb_matrix_create_csr. */
+int svdb_matrix_create_csr_device(uint64_t nrows, uint64_t ncols, uint64_t nnz, const int64_t* d_indptr,
+                                  const int32_t* d_indices, const double* d_values, svdb_matrix** out);
+void svdb_matrix_destroy(svdb_matrix* a);
+/* SMat::nrows / ncols / nnz (src/utils.rs:23-25). */
+uint64_t svdb_matrix_nrows(const svdb_matrix* a);
+uint64_t svdb_matrix_ncols(const svdb_matrix* a);
+uint64_t svdb_matrix_nnz(const svdb_matrix* a);
+
+/* ---- MaskedCSRMatrix (src/lanczos/masked.rs) ---- */
+
+/* MaskedCSRMatrix::new (masked.rs:21-46): mask_len must equal ncols
+ * (the crate's assert_eq!, masked.rs:22-26 -> SVDB_ERR_SHAPE).  The view is
+ * built on the device and is independent of later changes to `csr`; `csr`
+ * must outlive it (the crate's 'a lifetime). */
+int svdb_masked_new(const svdb_matrix* csr, const uint8_t* column_mask, uint64_t mask_len, svdb_matrix** out);
+/* MaskedCSRMatrix::with_columns (masked.rs:48-55): duplicates and order are
+ * ignored; an index >= ncols returns SVDB_ERR_SHAPE ("Column index out of
+ * bounds", masked.rs:51). */
+int svdb_masked_with_columns(const svdb_matrix* csr, const uint64_t* columns, uint64_t ncolumns,
+                             svdb_matrix** out);
+/* masked_to_original[ncols(masked)] (ascending) and original_to_masked[ncols(parent)]
+ * with -1 for None (masked.rs:15-17, 32-38); bit-exact. */
+int svdb_masked_maps(const svdb_matrix* masked, int64_t* masked_to_original, int64_t* original_to_masked);
+/* MaskedCSRMatrix::uses_all_columns (masked.rs:57-59); 1 / 0, -1 if not a masked view. */
+int svdb_masked_uses_all_columns(const svdb_matrix* masked);
+
+/* ---- SMat operator entry points (host buffers) ---- */
+
+/* SMat::svd_opa (src/utils.rs:26): y = A x, or A^T x when transposed. */
+int svdb_opa(const svdb_matrix* a, const double* x, double* y, int transposed);
+/* svd_opb (src/lanczos/mod.rs:311-319): y = A^T (A x), or A (A^T x) when transposed. */
+int svdb_opb(const svdb_matrix* a, const double* x, double* y, int transposed);
+/* SMat::multiply_with_dense (masked.rs:265-471): result = A X (X: ncols x l)
+ * or A^T X (X: nrows x l) when transpose_self.  The crate implements it only
+ * for MaskedCSRMatrix (todo!() for CSR/CSC/COO, src/lanczos/mod.rs:1629-1654);
+ * here it is defined for every handle.  The transposed product is the
+ * mathematical A^T X (masked.rs:388-393 indexes X as if row-major). */
+int svdb_multiply_with_dense(const svdb_matrix* a, const double* dense, uint64_t dense_cols, double* result,
+                             int transpose_self);
+/* SMat::multiply_transposed_by_dense (masked.rs:616-733): result (l x ncols) = Q^T A, Q: nrows x l. */
+int svdb_multiply_transposed_by_dense(const svdb_matrix* a, const double* q, uint64_t q_cols, double* result);
+
+/* multiply_with_dense on device buffers: d_result = A d_dense (transpose_self
+ * = 0, d_dense ncols x l) or A^T d_dense (nrows x l), row-major, enqueued on
+ * `stream` (cudaStream_t, NULL = the handle's stream) without synchronising.
+ * precision SVDB_F64: double operands; SVDB_MIXED: float operands and FP32
+ * matrix values. */
+int svdb_multiply_with_dense_device(const svdb_matrix* a, const void* d_dense, uint64_t dense_cols, void* d_result,
+                                    int transpose_self, int precision, void* stream);
+
+/* Number of kernels this library has launched in the process so far. */
+uint64_t svdb_kernel_launches(void);
+
+/* ---- LAS2 (src/lanczos/mod.rs) ---- */
+
+/* lanczos::svd_las2 (src/lanczos/mod.rs:104-189); opts may be NULL. */
+int svdb_las2(const svdb_matrix* a, uint64_t dimensions, uint64_t iterations, const double end_interval[2],
+              double kappa, uint32_t random_seed, const svdb_options* opts, svdb_rec* out);
+/* lanczos::svd (src/lanczos/mod.rs:27-36) */
+int svdb_svd(const svdb_matrix* a, svdb_rec* out);
+/* lanczos::svd_dim (src/lanczos/mod.rs:45-55) */
+int svdb_svd_dim(const svdb_matrix* a, uint64_t dimensions, svdb_rec* out);
+/* lanczos::svd_dim_seed (src/lanczos/mod.rs:65-86) */
+int svdb_svd_dim_seed(const svdb_matrix* a, uint64_t dimensions, uint32_t random_seed, svdb_rec* out);
+/* legacy::svdLAS2 (src/legacy.rs:569-654): the SVDLIBC semantics. */
+int svdb_legacy_svd_las2(const svdb_matrix* a, uint64_t dimensions, uint64_t iterations,
+                         const double end_interval[2], double kappa, uint32_t random_seed,
+                         const svdb_options* opts, svdb_rec* out);
+
+/* The LAS2 start vector on the current device: n draws of
+ * StdRng::from_seed([seed as u32 LE, 0, ...]).random_range(-1.0..1.0)
+ * (src/lanczos/mod.rs:598-605; rand 0.9 ChaCha12).  out: host array of n. */
+int svdb_start_vector(uint32_t seed, double* out, uint64_t n);
+
+/* The host-side argument handling of svd_las2 (src/lanczos/mod.rs:116-145):
+ * clamped dimensions / iterations, the transpose decision and the sparsity
+ * branch (0: <=0.9, 1: >0.9, 2: >0.99, 3: >0.999).  Needs no device. */
+int svdb_las2_plan(uint64_t nrows, uint64_t ncols, uint64_t nnz, uint64_t dimensions, uint64_t iterations,
+                   uint64_t* dimensions_out, uint64_t* iterations_out, int32_t* transposed_out,
+                   int32_t* sparsity_branch_out);
+
+/* ---- randomized SVD (src/randomized/mod.rs) ---- */
+
+/* randomized::randomized_svd (src/randomized/mod.rs:24-199).  has_seed = 0
+ * means seed None (the crate then seeds with 0, :304-307).  Omega is drawn on
+ * the device from a counter-based generator keyed by the seed, or taken from
+ * opts->omega.  mean_center = 1 returns SVDB_ERR_UNSUPPORTED. */
+int svdb_randomized_svd(const svdb_matrix* a, uint64_t target_rank, uint64_t n_oversamples,
+                        uint64_t n_power_iters, int normalizer, int mean_center, int has_seed, uint64_t seed,
+                        int verbose, const svdb_options* opts, svdb_rec* out);
+
+/* ---- results ---- */
+
+/* Frees u, s, vt (host or device) and zeroes the record. */
+void svdb_rec_free(svdb_rec* rec);
+/* SvdRec::recompose: out (u_rows x vt_cols, host) = u diag(s) vt as the crate
+ * writes it (src/lanczos/mod.rs:1408-1413), which needs u_cols == d
+ * (otherwise SVDB_ERR_SHAPE, where ndarray panics); for legacy records
+ * ut^T diag(s) vt (src/legacy.rs:2023-2028), out being u_cols x vt_cols. */
+int svdb_rec_recompose(const svdb_rec* rec, double* out);
+
+const char* svdb_last_error_message(void);
+/* Library version (major * 10000 + minor * 100 + patch). */
+int svdb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SVDB200_H */

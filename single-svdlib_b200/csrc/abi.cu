@@ -1,0 +1,379 @@
+// extern "C" entry points of libsvdb200 (include/svdb200.h).
+#include <atomic>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+
+#include "ops.cuh"
+#include "svdb_internal.h"
+
+namespace svdb {
+svdb_matrix* create_csr(uint64_t, uint64_t, uint64_t, const uint64_t*, const uint64_t*, const double*);
+svdb_matrix* create_csc(uint64_t, uint64_t, uint64_t, const uint64_t*, const uint64_t*, const double*);
+svdb_matrix* create_coo(uint64_t, uint64_t, uint64_t, const uint64_t*, const uint64_t*, const double*);
+svdb_matrix* create_csr_device(uint64_t, uint64_t, uint64_t, const int64_t*, const int32_t*, const double*);
+svdb_matrix* masked_new(const svdb_matrix*, const uint8_t*, uint64_t);
+void masked_maps(const svdb_matrix*, int64_t*, int64_t*);
+void destroy(svdb_matrix*);
+void las2(const svdb_matrix*, uint64_t, uint64_t, const double[2], double, uint32_t, bool, const svdb_options&,
+          svdb_rec*);
+int las2_plan(uint64_t, uint64_t, uint64_t, uint64_t, uint64_t, uint64_t*, uint64_t*, int32_t*, int32_t*);
+void randomized(const svdb_matrix*, uint64_t, uint64_t, uint64_t, int, int, int, uint64_t, int,
+                const svdb_options&, svdb_rec*);
+
+static thread_local std::string g_last_error;
+void set_last_error(const std::string& m) { g_last_error = m; }
+
+static std::atomic<uint64_t> g_launches{0};
+void count_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+// Runs `f`, mapping exceptions to status codes and the thread's last error.
+template <typename F>
+static int guarded(F&& f) {
+    try {
+        f();
+        return SVDB_OK;
+    } catch (Error& e) {
+        g_last_error = e.what();
+        return e.code;
+    } catch (std::bad_alloc&) {
+        g_last_error = "host allocation failed";
+        return SVDB_ERR_OOM;
+    } catch (std::exception& e) {
+        g_last_error = e.what();
+        return SVDB_ERR_ARG;
+    }
+}
+
+struct DeviceGuard {  // runs a call on the handle's device
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) SVDB_CUDA(cudaSetDevice(dev));
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+static svdb_options opts_or_default(const svdb_options* o) {
+    svdb_options d;
+    svdb_options_default(&d);
+    return o ? *o : d;
+}
+
+static void check_handle(const svdb_matrix* a) {
+    if (!a) throw Error(SVDB_ERR_ARG, "null matrix handle");
+}
+
+}  // namespace svdb
+
+using namespace svdb;
+
+extern "C" {
+
+void svdb_options_default(svdb_options* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->precision = SVDB_F64;
+    o->algorithm = SVDB_LANCZOS;
+}
+
+const char* svdb_last_error_message(void) { return g_last_error.c_str(); }
+int svdb_version(void) { return 10009; }
+
+int svdb_matrix_create_csr(uint64_t nrows, uint64_t ncols, uint64_t nnz, const uint64_t* indptr,
+                           const uint64_t* indices, const double* values, svdb_matrix** out) {
+    return guarded([&] {
+        if (!out) throw Error(SVDB_ERR_ARG, "null out");
+        *out = create_csr(nrows, ncols, nnz, indptr, indices, values);
+    });
+}
+int svdb_matrix_create_csc(uint64_t nrows, uint64_t ncols, uint64_t nnz, const uint64_t* colptr,
+                           const uint64_t* rowidx, const double* values, svdb_matrix** out) {
+    return guarded([&] {
+        if (!out) throw Error(SVDB_ERR_ARG, "null out");
+        *out = create_csc(nrows, ncols, nnz, colptr, rowidx, values);
+    });
+}
+int svdb_matrix_create_coo(uint64_t nrows, uint64_t ncols, uint64_t nnz, const uint64_t* rows, const uint64_t* cols,
+                           const double* values, svdb_matrix** out) {
+    return guarded([&] {
+        if (!out) throw Error(SVDB_ERR_ARG, "null out");
+        *out = create_coo(nrows, ncols, nnz, rows, cols, values);
+    });
+}
+int svdb_matrix_create_csr_device(uint64_t nrows, uint64_t ncols, uint64_t nnz, const int64_t* d_indptr,
+                                  const int32_t* d_indices, const double* d_values, svdb_matrix** out) {
+    return guarded([&] {
+        if (!out || !d_indptr || (nnz && (!d_indices || !d_values))) throw Error(SVDB_ERR_ARG, "null argument");
+        *out = create_csr_device(nrows, ncols, nnz, d_indptr, d_indices, d_values);
+    });
+}
+void svdb_matrix_destroy(svdb_matrix* a) {
+    if (!a) return;
+    guarded([&] {
+        DeviceGuard g(a->device);
+        destroy(a);
+    });
+}
+uint64_t svdb_matrix_nrows(const svdb_matrix* a) { return a ? a->nrows : 0; }
+uint64_t svdb_matrix_ncols(const svdb_matrix* a) { return a ? a->ncols : 0; }
+uint64_t svdb_matrix_nnz(const svdb_matrix* a) { return a ? a->nnz : 0; }
+
+int svdb_masked_new(const svdb_matrix* csr, const uint8_t* column_mask, uint64_t mask_len, svdb_matrix** out) {
+    return guarded([&] {
+        check_handle(csr);
+        if (!out) throw Error(SVDB_ERR_ARG, "null out");
+        DeviceGuard g(csr->device);
+        *out = masked_new(csr, column_mask, mask_len);
+    });
+}
+int svdb_masked_with_columns(const svdb_matrix* csr, const uint64_t* columns, uint64_t ncolumns,
+                             svdb_matrix** out) {
+    return guarded([&] {
+        check_handle(csr);
+        if (!out || (ncolumns && !columns)) throw Error(SVDB_ERR_ARG, "null argument");
+        std::vector<uint8_t> mask((size_t)csr->ncols, 0);  // masked.rs:48-55
+        for (uint64_t k = 0; k < ncolumns; ++k) {
+            if (columns[k] >= (uint64_t)csr->ncols) throw Error(SVDB_ERR_SHAPE, "Column index out of bounds");
+            mask[columns[k]] = 1;
+        }
+        DeviceGuard g(csr->device);
+        *out = masked_new(csr, mask.data(), mask.size());
+    });
+}
+int svdb_masked_maps(const svdb_matrix* m, int64_t* m2o, int64_t* o2m) {
+    return guarded([&] {
+        check_handle(m);
+        if (!m2o || !o2m) throw Error(SVDB_ERR_ARG, "null argument");
+        DeviceGuard g(m->device);
+        masked_maps(m, m2o, o2m);
+    });
+}
+int svdb_masked_uses_all_columns(const svdb_matrix* m) {
+    if (!m || m->kind != KIND_MASKED) return -1;
+    return m->all_columns ? 1 : 0;
+}
+
+int svdb_opa(const svdb_matrix* a, const double* x, double* y, int transposed) {
+    return guarded([&] {
+        check_handle(a);
+        if (!x || !y) throw Error(SVDB_ERR_ARG, "null argument");
+        svdb_matrix* am = const_cast<svdb_matrix*>(a);
+        std::lock_guard<std::mutex> lk(am->mu);
+        DeviceGuard g(a->device);
+        cudaStream_t s = a->stream;
+        const DevCompressed& op = transposed ? csc_of(a) : csr_of(a);
+        DevBuf<double> dx(std::max<int64_t>(op.nminor, 1), s), dy(std::max<int64_t>(op.nmajor, 1), s);
+        SVDB_CUDA(cudaMemcpyAsync(dx.p, x, op.nminor * 8, cudaMemcpyHostToDevice, s));
+        spmv(op, false, dx.p, dy.p, s);
+        SVDB_CUDA(cudaMemcpyAsync(y, dy.p, op.nmajor * 8, cudaMemcpyDeviceToHost, s));
+        SVDB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+int svdb_opb(const svdb_matrix* a, const double* x, double* y, int transposed) {
+    return guarded([&] {
+        check_handle(a);
+        if (!x || !y) throw Error(SVDB_ERR_ARG, "null argument");
+        svdb_matrix* am = const_cast<svdb_matrix*>(a);
+        std::lock_guard<std::mutex> lk(am->mu);
+        DeviceGuard g(a->device);
+        cudaStream_t s = a->stream;
+        const DevCompressed& o1 = transposed ? csc_of(a) : csr_of(a);
+        const DevCompressed& o2 = transposed ? csr_of(a) : csc_of(a);
+        DevBuf<double> dx(std::max<int64_t>(o1.nminor, 1), s), dt(std::max<int64_t>(o1.nmajor, 1), s),
+            dy(std::max<int64_t>(o2.nmajor, 1), s);
+        SVDB_CUDA(cudaMemcpyAsync(dx.p, x, o1.nminor * 8, cudaMemcpyHostToDevice, s));
+        spmv(o1, false, dx.p, dt.p, s);
+        spmv(o2, false, dt.p, dy.p, s);
+        SVDB_CUDA(cudaMemcpyAsync(y, dy.p, o2.nmajor * 8, cudaMemcpyDeviceToHost, s));
+        SVDB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+int svdb_multiply_with_dense(const svdb_matrix* a, const double* dense, uint64_t l, double* result,
+                             int transpose_self) {
+    return guarded([&] {
+        check_handle(a);
+        if (!dense || !result) throw Error(SVDB_ERR_ARG, "null argument");
+        svdb_matrix* am = const_cast<svdb_matrix*>(a);
+        std::lock_guard<std::mutex> lk(am->mu);
+        DeviceGuard g(a->device);
+        cudaStream_t s = a->stream;
+        const DevCompressed& op = transpose_self ? csc_of(a) : csr_of(a);
+        DevBuf<double> dx(std::max<int64_t>(op.nminor * l, 1), s), dy(std::max<int64_t>(op.nmajor * l, 1), s);
+        SVDB_CUDA(cudaMemcpyAsync(dx.p, dense, op.nminor * l * 8, cudaMemcpyHostToDevice, s));
+        spmm_dev<double>(op, false, dx.p, (int)l, dy.p, s);
+        SVDB_CUDA(cudaMemcpyAsync(result, dy.p, op.nmajor * l * 8, cudaMemcpyDeviceToHost, s));
+        SVDB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+int svdb_multiply_with_dense_device(const svdb_matrix* a, const void* d_dense, uint64_t l, void* d_result,
+                                    int transpose_self, int precision, void* stream) {
+    return guarded([&] {
+        check_handle(a);
+        if (!d_dense || !d_result) throw Error(SVDB_ERR_ARG, "null argument");
+        if (precision != SVDB_F64 && precision != SVDB_MIXED) throw Error(SVDB_ERR_ARG, "bad precision");
+        DeviceGuard g(a->device);
+        cudaStream_t s = stream ? (cudaStream_t)stream : a->stream;
+        const DevCompressed& op = transpose_self ? csc_of(a) : csr_of(a);
+        if (precision == SVDB_F64) {
+            spmm_dev<double>(op, false, (const double*)d_dense, (int)l, (double*)d_result, s);
+        } else {
+            if (!op.val32.p) {
+                svdb_matrix* am = const_cast<svdb_matrix*>(a);
+                std::lock_guard<std::mutex> lk(am->mu);
+                ensure_fp32(a);
+                SVDB_CUDA(cudaStreamSynchronize(a->stream));
+            }
+            spmm_dev<float>(op, true, (const float*)d_dense, (int)l, (float*)d_result, s);
+        }
+    });
+}
+
+uint64_t svdb_kernel_launches(void) { return g_launches.load(); }
+
+int svdb_multiply_transposed_by_dense(const svdb_matrix* a, const double* q, uint64_t l, double* result) {
+    return guarded([&] {
+        check_handle(a);
+        if (!q || !result) throw Error(SVDB_ERR_ARG, "null argument");
+        svdb_matrix* am = const_cast<svdb_matrix*>(a);
+        std::lock_guard<std::mutex> lk(am->mu);
+        DeviceGuard g(a->device);
+        cudaStream_t s = a->stream;
+        const DevCompressed& op = csc_of(a);  // (Q^T A)^T = A^T Q
+        DevBuf<double> dq(std::max<int64_t>(op.nminor * l, 1), s), dz(std::max<int64_t>(op.nmajor * l, 1), s),
+            dr(std::max<int64_t>(op.nmajor * l, 1), s);
+        SVDB_CUDA(cudaMemcpyAsync(dq.p, q, op.nminor * l * 8, cudaMemcpyHostToDevice, s));
+        spmm_dev<double>(op, false, dq.p, (int)l, dz.p, s);
+        transpose_dense<double>(dz.p, dr.p, op.nmajor, (int64_t)l, s);
+        SVDB_CUDA(cudaMemcpyAsync(result, dr.p, op.nmajor * l * 8, cudaMemcpyDeviceToHost, s));
+        SVDB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+static int las2_common(const svdb_matrix* a, uint64_t dimensions, uint64_t iterations, const double end_interval[2],
+                       double kappa, uint32_t seed, const svdb_options* opts, svdb_rec* out, int force_legacy) {
+    return guarded([&] {
+        check_handle(a);
+        if (!out) throw Error(SVDB_ERR_ARG, "null out");
+        const double ei_default[2] = {-1.0e-30, 1.0e-30};
+        const double* ei = end_interval ? end_interval : ei_default;
+        svdb_options o = opts_or_default(opts);
+        bool legacy = force_legacy || o.algorithm == SVDB_LEGACY;
+        svdb_matrix* am = const_cast<svdb_matrix*>(a);
+        std::lock_guard<std::mutex> lk(am->mu);
+        DeviceGuard g(a->device);
+        las2(a, dimensions, iterations, ei, kappa, seed, legacy, o, out);
+    });
+}
+
+int svdb_las2(const svdb_matrix* a, uint64_t dimensions, uint64_t iterations, const double end_interval[2],
+              double kappa, uint32_t random_seed, const svdb_options* opts, svdb_rec* out) {
+    return las2_common(a, dimensions, iterations, end_interval, kappa, random_seed, opts, out, 0);
+}
+int svdb_svd(const svdb_matrix* a, svdb_rec* out) {
+    return las2_common(a, 0, 0, nullptr, 1.0e-6, 0, nullptr, out, 0);
+}
+int svdb_svd_dim(const svdb_matrix* a, uint64_t dimensions, svdb_rec* out) {
+    return las2_common(a, dimensions, 0, nullptr, 1.0e-6, 0, nullptr, out, 0);
+}
+int svdb_svd_dim_seed(const svdb_matrix* a, uint64_t dimensions, uint32_t random_seed, svdb_rec* out) {
+    return las2_common(a, dimensions, 0, nullptr, 1.0e-6, random_seed, nullptr, out, 0);
+}
+int svdb_legacy_svd_las2(const svdb_matrix* a, uint64_t dimensions, uint64_t iterations,
+                         const double end_interval[2], double kappa, uint32_t random_seed,
+                         const svdb_options* opts, svdb_rec* out) {
+    return las2_common(a, dimensions, iterations, end_interval, kappa, random_seed, opts, out, 1);
+}
+
+int svdb_start_vector(uint32_t seed, double* out, uint64_t n) {
+    return guarded([&] {
+        if (!out && n) throw Error(SVDB_ERR_ARG, "null out");
+        cudaStream_t s = nullptr;
+        SVDB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        try {
+            DevBuf<double> w(std::max<uint64_t>(n, 1), s);
+            start_vector(seed, w.p, (int64_t)n, s);
+            if (n) SVDB_CUDA(cudaMemcpyAsync(out, w.p, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+            SVDB_CUDA(cudaStreamSynchronize(s));
+        } catch (...) {
+            cudaStreamDestroy(s);
+            throw;
+        }
+        cudaStreamDestroy(s);
+    });
+}
+
+int svdb_las2_plan(uint64_t nrows, uint64_t ncols, uint64_t nnz, uint64_t dimensions, uint64_t iterations,
+                   uint64_t* dimensions_out, uint64_t* iterations_out, int32_t* transposed_out,
+                   int32_t* sparsity_branch_out) {
+    return guarded([&] {
+        las2_plan(nrows, ncols, nnz, dimensions, iterations, dimensions_out, iterations_out, transposed_out,
+                  sparsity_branch_out);
+    });
+}
+
+int svdb_randomized_svd(const svdb_matrix* a, uint64_t target_rank, uint64_t n_oversamples, uint64_t n_power_iters,
+                        int normalizer, int mean_center, int has_seed, uint64_t seed, int verbose,
+                        const svdb_options* opts, svdb_rec* out) {
+    return guarded([&] {
+        check_handle(a);
+        if (!out) throw Error(SVDB_ERR_ARG, "null out");
+        if (normalizer < 0 || normalizer > 2) throw Error(SVDB_ERR_ARG, "bad normalizer");
+        svdb_options o = opts_or_default(opts);
+        svdb_matrix* am = const_cast<svdb_matrix*>(a);
+        std::lock_guard<std::mutex> lk(am->mu);
+        DeviceGuard g(a->device);
+        randomized(a, target_rank, n_oversamples, n_power_iters, normalizer, mean_center, has_seed, seed, verbose,
+                   o, out);
+    });
+}
+
+void svdb_rec_free(svdb_rec* r) {
+    if (!r) return;
+    if (r->on_device) {
+        cudaFree(r->u);
+        cudaFree(r->s);
+        cudaFree(r->vt);
+    } else {
+        free(r->u);
+        free(r->s);
+        free(r->vt);
+    }
+    std::memset(r, 0, sizeof(*r));
+}
+
+int svdb_rec_recompose(const svdb_rec* r, double* out) {
+    return guarded([&] {
+        if (!r || !out) throw Error(SVDB_ERR_ARG, "null argument");
+        if (r->on_device) throw Error(SVDB_ERR_UNSUPPORTED, "recompose of a device-resident record");
+        const uint64_t n = r->vt_cols, d = r->d;
+        if (r->origin == SVDB_REC_LEGACY) {  // ut.t() . diag(s) . vt
+            const uint64_t m = r->u_cols;
+            for (uint64_t i = 0; i < m; ++i)
+                for (uint64_t j = 0; j < n; ++j) {
+                    double acc = 0.0;
+                    for (uint64_t k = 0; k < d; ++k) acc += r->u[k * m + i] * r->s[k] * r->vt[k * n + j];
+                    out[i * n + j] = acc;
+                }
+            return;
+        }
+        // u . diag(s) . vt exactly as written; ndarray requires u_cols == len(s)
+        if (r->u_cols != d)
+            throw Error(SVDB_ERR_SHAPE, "ndarray: inputs " + std::to_string(r->u_rows) + " x " +
+                                            std::to_string(r->u_cols) + " and " + std::to_string(d) + " x " +
+                                            std::to_string(d) + " are not compatible for matrix multiplication");
+        const uint64_t m = r->u_rows;
+        for (uint64_t i = 0; i < m; ++i)
+            for (uint64_t j = 0; j < n; ++j) {
+                double acc = 0.0;
+                for (uint64_t k = 0; k < d; ++k) acc += r->u[i * d + k] * r->s[k] * r->vt[k * n + j];
+                out[i * n + j] = acc;
+            }
+    });
+}
+
+}  // extern "C"

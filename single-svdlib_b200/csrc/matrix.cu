@@ -1,0 +1,515 @@
+// Sparse operator handles in HBM: upload + validation, CSR <-> CSC transpose,
+// COO ingestion, and the MaskedCSRMatrix column remap / compaction.
+//
+// Layout: every handle keeps A twice, as CSR (rows of A) and as CSC (rows of
+// A^T), so both products of SMat::svd_opa (src/utils.rs:26) are row gathers
+// with coalesced index/value streams and no atomics.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cstring>
+
+#include "device_common.cuh"
+#include "svdb_internal.h"
+
+namespace svdb {
+
+const DeviceProps& device_props() {
+    static thread_local int cached_dev = -1;
+    static thread_local DeviceProps props;
+    int dev = 0;
+    SVDB_CUDA(cudaGetDevice(&dev));
+    if (dev != cached_dev) {
+        cudaDeviceProp p;
+        SVDB_CUDA(cudaGetDeviceProperties(&p, dev));
+        props.sms = p.multiProcessorCount;
+        props.coop = p.cooperativeLaunch;
+        props.l2 = p.l2CacheSize;
+        cached_dev = dev;
+    }
+    return props;
+}
+
+// ------------------------------------------------------------------ kernels
+__global__ void k_check_convert_ptr(const uint64_t* in, int64_t* out, int64_t nmajor, uint64_t nnz, int* bad) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (; i <= nmajor; i += stride) {
+        uint64_t v = in[i];
+        out[i] = (int64_t)v;
+        if (i == 0 && v != 0) atomicOr(bad, 1);
+        if (i == nmajor && v != nnz) atomicOr(bad, 2);
+        if (i < nmajor && in[i + 1] < v) atomicOr(bad, 4);
+    }
+}
+
+__global__ void k_check_convert_idx(const uint64_t* in, int32_t* out, uint64_t nnz, uint64_t bound, int* bad) {
+    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (; i < nnz; i += stride) {
+        uint64_t v = in[i];
+        if (v >= bound) { atomicOr(bad, 8); v = 0; }
+        out[i] = (int32_t)v;
+    }
+}
+
+// row id of every entry: binary search of the offsets
+__global__ void k_expand_major(const int64_t* ptr, int64_t nmajor, int64_t nnz, int32_t* major_of) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (; k < nnz; k += stride) {
+        int64_t lo = 0, hi = nmajor;  // find last r with ptr[r] <= k
+        while (hi - lo > 1) {
+            int64_t mid = (lo + hi) >> 1;
+            if (ptr[mid] <= k) lo = mid; else hi = mid;
+        }
+        major_of[k] = (int32_t)lo;
+    }
+}
+
+template <typename IT>
+__global__ void k_iota(IT* v, int64_t n) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (; k < n; k += stride) v[k] = (IT)k;
+}
+
+template <typename IT>
+__global__ void k_gather_transpose(const IT* perm, const int32_t* major_of, const double* val, int32_t* out_idx,
+                                   double* out_val, int64_t nnz) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (; k < nnz; k += stride) {
+        IT p = perm[k];
+        out_idx[k] = major_of[p];
+        out_val[k] = val[p];
+    }
+}
+
+// out_ptr[c] = first position with key >= c (keys sorted ascending), c in [0, nminor]
+__global__ void k_offsets_from_sorted(const int32_t* keys, int64_t nnz, int64_t nminor, int64_t* out_ptr) {
+    int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (; c <= nminor; c += stride) {
+        int64_t lo = 0, hi = nnz;
+        while (lo < hi) {
+            int64_t mid = (lo + hi) >> 1;
+            if ((int64_t)keys[mid] < c) lo = mid + 1; else hi = mid;
+        }
+        out_ptr[c] = lo;
+    }
+}
+
+__global__ void k_to_f32(const double* in, float* out, int64_t n) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (; k < n; k += stride) out[k] = (float)in[k];
+}
+
+static int grid_for(int64_t n, int threads = 256) {
+    int64_t b = (n + threads - 1) / threads;
+    int64_t cap = (int64_t)device_props().sms * 32;
+    return (int)std::max<int64_t>(1, std::min(b, cap));
+}
+
+static int bits_for(int64_t n) {
+    int b = 1;
+    while (b < 31 && (int64_t(1) << b) < n) ++b;
+    return b;
+}
+
+// Stable sort of entry positions by minor index: the transpose keeps majors
+// ascending inside every minor slice (CSR rows ascending inside each column).
+template <typename IT>
+static void transpose_impl(const DevCompressed& in, DevCompressed& out, cudaStream_t s) {
+    const int64_t nnz = in.nnz;
+    out.nmajor = in.nminor;
+    out.nminor = in.nmajor;
+    out.nnz = nnz;
+    out.ptr.alloc(out.nmajor + 1, s);
+    out.idx.alloc(std::max<int64_t>(nnz, 1), s);
+    out.val.alloc(std::max<int64_t>(nnz, 1), s);
+    if (nnz == 0) {
+        SVDB_CUDA(cudaMemsetAsync(out.ptr.p, 0, (out.nmajor + 1) * sizeof(int64_t), s));
+        return;
+    }
+    DevBuf<int32_t> major_of(nnz, s), keys_out(nnz, s);
+    DevBuf<IT> vals_in(nnz, s), vals_out(nnz, s);
+    k_expand_major<<<grid_for(nnz), 256, 0, s>>>(in.ptr.p, in.nmajor, nnz, major_of.p);
+    k_iota<IT><<<grid_for(nnz), 256, 0, s>>>(vals_in.p, nnz);
+    SVDB_CHECK_LAUNCH_N(2);
+    size_t tmp_bytes = 0;
+    int end_bit = bits_for(std::max<int64_t>(in.nminor, 2));
+    SVDB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, in.idx.p, keys_out.p, vals_in.p, vals_out.p,
+                                              nnz, 0, end_bit, s));
+    DevBuf<uint8_t> tmp(std::max<size_t>(tmp_bytes, 1), s);
+    SVDB_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tmp_bytes, in.idx.p, keys_out.p, vals_in.p, vals_out.p, nnz,
+                                              0, end_bit, s));
+    k_gather_transpose<IT><<<grid_for(nnz), 256, 0, s>>>(vals_out.p, major_of.p, in.val.p, out.idx.p, out.val.p,
+                                                         nnz);
+    k_offsets_from_sorted<<<grid_for(out.nmajor + 1), 256, 0, s>>>(keys_out.p, nnz, out.nmajor, out.ptr.p);
+    SVDB_CHECK_LAUNCH_N(2);
+}
+
+void transpose(const DevCompressed& in, DevCompressed& out, cudaStream_t s) {
+    if (in.nnz <= INT32_MAX) transpose_impl<int32_t>(in, out, s);
+    else transpose_impl<int64_t>(in, out, s);
+}
+
+void ensure_fp32(const svdb_matrix* a) {
+    for (const DevCompressed* c : {&csr_of(a), &csc_of(a)}) {
+        DevCompressed* m = const_cast<DevCompressed*>(c);
+        if (m->val32.p || m->nnz == 0) continue;
+        m->val32.alloc(m->nnz, a->stream);
+        k_to_f32<<<grid_for(m->nnz), 256, 0, a->stream>>>(m->val.p, m->val32.p, m->nnz);
+        SVDB_CHECK_LAUNCH();
+    }
+}
+
+const DevCompressed& csr_of(const svdb_matrix* a) {
+    if (a->kind == KIND_MASKED && a->all_columns) return a->parent->csr;
+    return a->csr;
+}
+const DevCompressed& csc_of(const svdb_matrix* a) {
+    if (a->kind == KIND_MASKED && a->all_columns) return a->parent->csc;
+    return a->csc;
+}
+
+// Upload a compressed structure given with usize offsets / indices.
+static void upload_compressed(DevCompressed& c, int64_t nmajor, int64_t nminor, uint64_t nnz, const uint64_t* ptr,
+                              const uint64_t* idx, const double* val, cudaStream_t s) {
+    if (!ptr || (nnz && (!idx || !val))) throw Error(SVDB_ERR_ARG, "null array");
+    if (nminor > INT32_MAX) throw Error(SVDB_ERR_UNSUPPORTED, "minor dimension above 2^31-1");
+    c.nmajor = nmajor;
+    c.nminor = nminor;
+    c.nnz = (int64_t)nnz;
+    DevBuf<uint64_t> tptr(nmajor + 1, s), tidx(std::max<uint64_t>(nnz, 1), s);
+    DevBuf<int> bad(1, s);
+    c.ptr.alloc(nmajor + 1, s);
+    c.idx.alloc(std::max<uint64_t>(nnz, 1), s);
+    c.val.alloc(std::max<uint64_t>(nnz, 1), s);
+    SVDB_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), s));
+    SVDB_CUDA(cudaMemcpyAsync(tptr.p, ptr, (nmajor + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+    if (nnz) {
+        SVDB_CUDA(cudaMemcpyAsync(tidx.p, idx, nnz * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+        SVDB_CUDA(cudaMemcpyAsync(c.val.p, val, nnz * sizeof(double), cudaMemcpyHostToDevice, s));
+    }
+    k_check_convert_ptr<<<grid_for(nmajor + 1), 256, 0, s>>>(tptr.p, c.ptr.p, nmajor, nnz, bad.p);
+    if (nnz) k_check_convert_idx<<<grid_for(nnz), 256, 0, s>>>(tidx.p, c.idx.p, nnz, (uint64_t)nminor, bad.p);
+    SVDB_CHECK_LAUNCH_N(nnz ? 2 : 1);
+    int hbad = 0;
+    SVDB_CUDA(cudaMemcpyAsync(&hbad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    SVDB_CUDA(cudaStreamSynchronize(s));
+    if (hbad) {
+        std::string m = "invalid compressed sparse input:";
+        if (hbad & 1) m += " offsets[0] != 0;";
+        if (hbad & 2) m += " offsets[last] != nnz;";
+        if (hbad & 4) m += " offsets not monotone;";
+        if (hbad & 8) m += " index out of bounds;";
+        throw Error(SVDB_ERR_SHAPE, m);
+    }
+}
+
+static svdb_matrix* new_handle() {
+    svdb_matrix* a = new svdb_matrix();
+    SVDB_CUDA(cudaGetDevice(&a->device));
+    SVDB_CUDA(cudaStreamCreateWithFlags(&a->stream, cudaStreamNonBlocking));
+    return a;
+}
+
+svdb_matrix* create_csr(uint64_t nrows, uint64_t ncols, uint64_t nnz, const uint64_t* indptr,
+                        const uint64_t* indices, const double* values) {
+    svdb_matrix* a = new_handle();
+    try {
+        a->kind = KIND_CSR;
+        a->nrows = nrows; a->ncols = ncols; a->nnz = nnz;
+        upload_compressed(a->csr, nrows, ncols, nnz, indptr, indices, values, a->stream);
+        transpose(a->csr, a->csc, a->stream);
+        SVDB_CUDA(cudaStreamSynchronize(a->stream));
+    } catch (...) {
+        cudaStreamSynchronize(a->stream);
+        delete a;
+        throw;
+    }
+    return a;
+}
+
+svdb_matrix* create_csc(uint64_t nrows, uint64_t ncols, uint64_t nnz, const uint64_t* colptr,
+                        const uint64_t* rowidx, const double* values) {
+    svdb_matrix* a = new_handle();
+    try {
+        a->kind = KIND_CSC;
+        a->nrows = nrows; a->ncols = ncols; a->nnz = nnz;
+        if (nrows > INT32_MAX) throw Error(SVDB_ERR_UNSUPPORTED, "nrows above 2^31-1");
+        upload_compressed(a->csc, ncols, nrows, nnz, colptr, rowidx, values, a->stream);
+        transpose(a->csc, a->csr, a->stream);
+        SVDB_CUDA(cudaStreamSynchronize(a->stream));
+    } catch (...) {
+        cudaStreamSynchronize(a->stream);
+        delete a;
+        throw;
+    }
+    return a;
+}
+
+// COO: entries stay in push order inside each row (stable sort by row), and
+// duplicates remain separate entries, as the crate's triplet loops use them.
+svdb_matrix* create_coo(uint64_t nrows, uint64_t ncols, uint64_t nnz, const uint64_t* rows, const uint64_t* cols,
+                        const double* values) {
+    svdb_matrix* a = new_handle();
+    try {
+        a->kind = KIND_COO;
+        a->nrows = nrows; a->ncols = ncols; a->nnz = nnz;
+        if (nrows > INT32_MAX || ncols > INT32_MAX) throw Error(SVDB_ERR_UNSUPPORTED, "dimension above 2^31-1");
+        cudaStream_t s = a->stream;
+        // Treat (row ids, col ids) as a "CSC-like" structure keyed by row:
+        // sort entry positions by row, stable.
+        DevCompressed tmp;
+        tmp.nmajor = 1; tmp.nminor = nrows; tmp.nnz = nnz;
+        DevBuf<uint64_t> tr(std::max<uint64_t>(nnz, 1), s), tc(std::max<uint64_t>(nnz, 1), s);
+        DevBuf<int32_t> r32(std::max<uint64_t>(nnz, 1), s), c32(std::max<uint64_t>(nnz, 1), s);
+        DevBuf<double> v(std::max<uint64_t>(nnz, 1), s);
+        DevBuf<int> bad(1, s);
+        SVDB_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), s));
+        if (nnz) {
+            if (!rows || !cols || !values) throw Error(SVDB_ERR_ARG, "null array");
+            SVDB_CUDA(cudaMemcpyAsync(tr.p, rows, nnz * 8, cudaMemcpyHostToDevice, s));
+            SVDB_CUDA(cudaMemcpyAsync(tc.p, cols, nnz * 8, cudaMemcpyHostToDevice, s));
+            SVDB_CUDA(cudaMemcpyAsync(v.p, values, nnz * 8, cudaMemcpyHostToDevice, s));
+            k_check_convert_idx<<<grid_for(nnz), 256, 0, s>>>(tr.p, r32.p, nnz, nrows, bad.p);
+            k_check_convert_idx<<<grid_for(nnz), 256, 0, s>>>(tc.p, c32.p, nnz, ncols, bad.p);
+            SVDB_CHECK_LAUNCH_N(2);
+        }
+        int hbad = 0;
+        SVDB_CUDA(cudaMemcpyAsync(&hbad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+        SVDB_CUDA(cudaStreamSynchronize(s));
+        if (hbad) throw Error(SVDB_ERR_SHAPE, "COO index out of bounds");
+        a->csr.nmajor = nrows; a->csr.nminor = ncols; a->csr.nnz = nnz;
+        a->csr.ptr.alloc(nrows + 1, s);
+        a->csr.idx.alloc(std::max<uint64_t>(nnz, 1), s);
+        a->csr.val.alloc(std::max<uint64_t>(nnz, 1), s);
+        if (nnz == 0) {
+            SVDB_CUDA(cudaMemsetAsync(a->csr.ptr.p, 0, (nrows + 1) * 8, s));
+        } else {
+            DevBuf<int32_t> keys_out(nnz, s);
+            DevBuf<int64_t> pin(nnz, s), pout(nnz, s);
+            k_iota<int64_t><<<grid_for(nnz), 256, 0, s>>>(pin.p, nnz);
+            size_t tb = 0;
+            int eb = bits_for(std::max<int64_t>(nrows, 2));
+            SVDB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, r32.p, keys_out.p, pin.p, pout.p, nnz, 0, eb, s));
+            DevBuf<uint8_t> t(std::max<size_t>(tb, 1), s);
+            SVDB_CUDA(cub::DeviceRadixSort::SortPairs(t.p, tb, r32.p, keys_out.p, pin.p, pout.p, nnz, 0, eb, s));
+            k_gather_transpose<int64_t><<<grid_for(nnz), 256, 0, s>>>(pout.p, c32.p, v.p, a->csr.idx.p,
+                                                                      a->csr.val.p, nnz);
+            k_offsets_from_sorted<<<grid_for(nrows + 1), 256, 0, s>>>(keys_out.p, nnz, nrows, a->csr.ptr.p);
+            SVDB_CHECK_LAUNCH_N(3);
+        }
+        transpose(a->csr, a->csc, s);
+        SVDB_CUDA(cudaStreamSynchronize(s));
+    } catch (...) {
+        cudaStreamSynchronize(a->stream);
+        delete a;
+        throw;
+    }
+    return a;
+}
+
+__global__ void k_copy_i64(const int64_t* in, int64_t* out, int64_t n, int64_t bound, int* bad, int check_mono,
+                           int64_t nnz) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (; i < n; i += stride) {
+        int64_t v = in[i];
+        out[i] = v;
+        if (check_mono) {
+            if (i == 0 && v != 0) atomicOr(bad, 1);
+            if (i == n - 1 && v != nnz) atomicOr(bad, 2);
+            if (i + 1 < n && in[i + 1] < v) atomicOr(bad, 4);
+        }
+    }
+}
+__global__ void k_copy_i32_checked(const int32_t* in, int32_t* out, int64_t n, int64_t bound, int* bad) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (; i < n; i += stride) {
+        int32_t v = in[i];
+        if (v < 0 || v >= bound) { atomicOr(bad, 8); v = 0; }
+        out[i] = v;
+    }
+}
+
+svdb_matrix* create_csr_device(uint64_t nrows, uint64_t ncols, uint64_t nnz, const int64_t* d_indptr,
+                               const int32_t* d_indices, const double* d_values) {
+    svdb_matrix* a = new_handle();
+    try {
+        if (ncols > INT32_MAX) throw Error(SVDB_ERR_UNSUPPORTED, "ncols above 2^31-1");
+        cudaStream_t s = a->stream;
+        a->kind = KIND_CSR;
+        a->nrows = nrows; a->ncols = ncols; a->nnz = nnz;
+        DevCompressed& c = a->csr;
+        c.nmajor = nrows; c.nminor = ncols; c.nnz = nnz;
+        c.ptr.alloc(nrows + 1, s);
+        c.idx.alloc(std::max<uint64_t>(nnz, 1), s);
+        c.val.alloc(std::max<uint64_t>(nnz, 1), s);
+        DevBuf<int> bad(1, s);
+        SVDB_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), s));
+        k_copy_i64<<<grid_for(nrows + 1), 256, 0, s>>>(d_indptr, c.ptr.p, nrows + 1, 0, bad.p, 1, nnz);
+        if (nnz) {
+            k_copy_i32_checked<<<grid_for(nnz), 256, 0, s>>>(d_indices, c.idx.p, nnz, ncols, bad.p);
+            SVDB_CUDA(cudaMemcpyAsync(c.val.p, d_values, nnz * 8, cudaMemcpyDeviceToDevice, s));
+        }
+        SVDB_CHECK_LAUNCH_N(nnz ? 2 : 1);
+        int hbad = 0;
+        SVDB_CUDA(cudaMemcpyAsync(&hbad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+        SVDB_CUDA(cudaStreamSynchronize(s));
+        if (hbad) throw Error(SVDB_ERR_SHAPE, "invalid compressed sparse input");
+        transpose(a->csr, a->csc, s);
+        SVDB_CUDA(cudaStreamSynchronize(s));
+    } catch (...) {
+        cudaStreamSynchronize(a->stream);
+        delete a;
+        throw;
+    }
+    return a;
+}
+
+// ----------------------------------------------------------- masked view --
+// original_to_masked[c] = rank of c among included columns (-1 = None),
+// masked_to_original[rank] = c; the ranks come from an exclusive scan of the
+// mask, so masked column j is the j-th included column in ascending order
+// (masked.rs:32-38).
+__global__ void k_mask_maps(const uint8_t* mask, const int64_t* scan, int64_t n, int64_t* o2m, int64_t* m2o) {
+    int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (; c < n; c += stride) {
+        if (mask[c]) { o2m[c] = scan[c]; m2o[scan[c]] = c; }
+        else o2m[c] = -1;
+    }
+}
+
+__global__ void k_mask_to_i64(const uint8_t* mask, int64_t* out, int64_t n) {
+    int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (; c < n; c += stride) out[c] = mask[c] ? 1 : 0;
+}
+
+__global__ void k_mask_flags(const int32_t* idx, const uint8_t* mask, int64_t nnz, int64_t* flags) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (; k < nnz; k += stride) flags[k] = mask[idx[k]] ? 1 : 0;
+}
+
+// Kept entries keep their order (scan positions); columns are remapped.
+__global__ void k_mask_compact(const int32_t* idx, const double* val, const int64_t* pos, const int64_t* o2m,
+                               int64_t nnz, int32_t* out_idx, double* out_val) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (; k < nnz; k += stride) {
+        int64_t mc = o2m[idx[k]];
+        if (mc >= 0) {
+            int64_t p = pos[k];
+            out_idx[p] = (int32_t)mc;
+            out_val[p] = val[k];
+        }
+    }
+}
+
+__global__ void k_mask_rowptr(const int64_t* ptr, const int64_t* pos, int64_t nrows, int64_t* out_ptr) {
+    int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (; r <= nrows; r += stride) out_ptr[r] = pos[ptr[r]];
+}
+
+svdb_matrix* masked_new(const svdb_matrix* parent, const uint8_t* hmask, uint64_t mask_len) {
+    if (!parent || !hmask) throw Error(SVDB_ERR_ARG, "null argument");
+    if (parent->kind == KIND_MASKED) throw Error(SVDB_ERR_ARG, "MaskedCSRMatrix borrows a CsrMatrix, not a view");
+    if ((int64_t)mask_len != parent->ncols)
+        throw Error(SVDB_ERR_SHAPE, "Column mask must have the same length as the number of columns in the matrix");
+    svdb_matrix* a = new_handle();
+    try {
+        cudaStream_t s = a->stream;
+        // The parent may be in use on its own stream; order after it.
+        SVDB_CUDA(cudaStreamSynchronize(parent->stream));
+        a->kind = KIND_MASKED;
+        a->parent = parent;
+        a->nrows = parent->nrows;
+        const int64_t n = parent->ncols;
+        const DevCompressed& P = parent->csr;
+        const int64_t nnz = P.nnz;
+        DevBuf<uint8_t> mask(std::max<int64_t>(n, 1), s);
+        DevBuf<int64_t> mask64(n + 1, s), scan(n + 1, s);
+        a->o2m.alloc(std::max<int64_t>(n, 1), s);
+        a->m2o.alloc(std::max<int64_t>(n, 1), s);
+        if (n) SVDB_CUDA(cudaMemcpyAsync(mask.p, hmask, n, cudaMemcpyHostToDevice, s));
+        // exclusive scan of the mask (as int64, one trailing zero) -> ranks;
+        // the last element is the masked column count
+        DevBuf<uint8_t> mask_pad(n + 1, s);
+        SVDB_CUDA(cudaMemsetAsync(mask_pad.p, 0, n + 1, s));
+        if (n) SVDB_CUDA(cudaMemcpyAsync(mask_pad.p, mask.p, n, cudaMemcpyDeviceToDevice, s));
+        k_mask_to_i64<<<grid_for(n + 1), 256, 0, s>>>(mask_pad.p, mask64.p, n + 1);
+        size_t tb = 0;
+        SVDB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, mask64.p, scan.p, n + 1, s));
+        DevBuf<uint8_t> tmp(std::max<size_t>(tb, 1), s);
+        SVDB_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, tb, mask64.p, scan.p, n + 1, s));
+        k_mask_maps<<<grid_for(std::max<int64_t>(n, 1)), 256, 0, s>>>(mask_pad.p, scan.p, n, a->o2m.p, a->m2o.p);
+        SVDB_CHECK_LAUNCH_N(2);
+        int64_t nm = 0;
+        SVDB_CUDA(cudaMemcpyAsync(&nm, scan.p + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        SVDB_CUDA(cudaStreamSynchronize(s));
+        a->ncols = nm;
+        bool all = (nm == n);
+        a->all_columns = all;
+        if (all) {
+            a->nnz = nnz;  // uses_all_columns: the view is the parent operator
+            return a;
+        }
+        // Compaction: flags -> exclusive scan -> scatter, order preserved.
+        DevBuf<int64_t> flags(nnz + 1, s), pos(nnz + 1, s);
+        SVDB_CUDA(cudaMemsetAsync(flags.p, 0, (nnz + 1) * sizeof(int64_t), s));
+        if (nnz) k_mask_flags<<<grid_for(nnz), 256, 0, s>>>(P.idx.p, mask_pad.p, nnz, flags.p);
+        size_t tb2 = 0;
+        SVDB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb2, flags.p, pos.p, nnz + 1, s));
+        DevBuf<uint8_t> tmp2(std::max<size_t>(tb2, 1), s);
+        SVDB_CUDA(cub::DeviceScan::ExclusiveSum(tmp2.p, tb2, flags.p, pos.p, nnz + 1, s));
+        int64_t mnnz = 0;
+        SVDB_CUDA(cudaMemcpyAsync(&mnnz, pos.p + nnz, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        SVDB_CUDA(cudaStreamSynchronize(s));
+        a->nnz = mnnz;
+        DevCompressed& C = a->csr;
+        C.nmajor = parent->nrows; C.nminor = nm; C.nnz = mnnz;
+        C.ptr.alloc(C.nmajor + 1, s);
+        C.idx.alloc(std::max<int64_t>(mnnz, 1), s);
+        C.val.alloc(std::max<int64_t>(mnnz, 1), s);
+        if (nnz) k_mask_compact<<<grid_for(nnz), 256, 0, s>>>(P.idx.p, P.val.p, pos.p, a->o2m.p, nnz, C.idx.p,
+                                                              C.val.p);
+        k_mask_rowptr<<<grid_for(C.nmajor + 1), 256, 0, s>>>(P.ptr.p, pos.p, C.nmajor, C.ptr.p);
+        SVDB_CHECK_LAUNCH_N(nnz ? 3 : 1);
+        transpose(a->csr, a->csc, s);
+        SVDB_CUDA(cudaStreamSynchronize(s));
+    } catch (...) {
+        cudaStreamSynchronize(a->stream);
+        delete a;
+        throw;
+    }
+    return a;
+}
+
+void masked_maps(const svdb_matrix* a, int64_t* m2o, int64_t* o2m) {
+    if (a->kind != KIND_MASKED) throw Error(SVDB_ERR_ARG, "not a MaskedCSRMatrix handle");
+    if (a->ncols) SVDB_CUDA(cudaMemcpyAsync(m2o, a->m2o.p, a->ncols * 8, cudaMemcpyDeviceToHost, a->stream));
+    if (a->parent->ncols)
+        SVDB_CUDA(cudaMemcpyAsync(o2m, a->o2m.p, a->parent->ncols * 8, cudaMemcpyDeviceToHost, a->stream));
+    SVDB_CUDA(cudaStreamSynchronize(a->stream));
+}
+
+void destroy(svdb_matrix* a) {
+    if (!a) return;
+    cudaStreamSynchronize(a->stream);
+    // buffers free themselves on a->stream
+    cudaStream_t s = a->stream;
+    delete a;
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+}
+
+}  // namespace svdb

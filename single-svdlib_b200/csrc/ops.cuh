@@ -1,0 +1,30 @@
+// Host-side launchers of the standalone device operators (ops.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "svdb_internal.h"
+
+namespace svdb {
+
+// lanes per row for a row gather with `avg` entries per row (power of two, 2..32)
+int group_for(double avg);
+
+// Y (nmajor x l) = M X with X (nminor x l), row-major; values FP32 when fp32
+// and the FP32 copy exists; accumulation in T.
+template <typename T>
+void spmm_dev(const DevCompressed& m, bool fp32, const T* X, int l, T* Y, cudaStream_t s);
+
+void datx(double a, const double* x, double* y, int64_t n, cudaStream_t s);  // y = a * x
+
+void gemv_t(const double* Q, int64_t n, int64_t i0, int64_t cnt, const double* x, double* t, double* scratch,
+            int64_t scratch_cap, cudaStream_t s);
+
+template <typename T>
+void transpose_dense(const T* in, T* out, int64_t rows, int64_t cols, cudaStream_t s);
+
+void transpose(const DevCompressed& in, DevCompressed& out, cudaStream_t s);
+
+}  // namespace svdb

@@ -1,0 +1,601 @@
+// randomized_svd (src/randomized/mod.rs:24-199) on the device.
+//
+//   Y = A Omega; q x [Z = A^T Y, normalise Z; Y = A Z, normalise Y];
+//   Q = qr(Y).q; B^T = A^T Q; SVD(B); U = Q U_B.
+//
+// nalgebra's Householder qr().q() (third-party) is replaced by CholeskyQR2:
+// the Gram X^T X in FP64, a one-block Cholesky, X R^-1, twice; if a Cholesky
+// pivot breaks down the pass is redone with a shift (shifted CholeskyQR3).
+// The column spaces are those of Householder QR; column signs may differ.
+// nalgebra's svd(B) is replaced by: QR of B^T = Q_b R (CholeskyQR2), then a
+// one-sided Jacobi SVD of the small R in one block, so that
+// B = V_R S (Q_b U_R)^T, singular values in descending order.
+//
+// SVDB_MIXED runs the sparse products in FP32 (values, dense operands and
+// accumulation); the Gram products, Cholesky and the second CholeskyQR pass
+// stay FP64.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "device_common.cuh"
+#include "ops.cuh"
+#include "svdb_internal.h"
+
+namespace svdb {
+
+static int nb(int64_t work, int threads, int per_sm = 16) {
+    int64_t b = (work + threads - 1) / threads;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(b, (int64_t)device_props().sms * per_sm));
+}
+
+// --------------------------------------------------------------- Omega ----
+// N(0,1) entries from a counter-based generator: splitmix64 (Steele, Lea and
+// Flood 2014) of (seed, index) gives two uniforms, Box-Muller gives the
+// normal.  rand_distr's ziggurat stream is not reproduced.
+__device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+template <typename T>
+__global__ void k_omega(uint64_t seed, int64_t total, T* __restrict__ out) {
+    const uint64_t key = splitmix64(seed ^ 0x5DEECE66Dull);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint64_t a = splitmix64(key + 2 * (uint64_t)i), b = splitmix64(key + 2 * (uint64_t)i + 1);
+        const double u1 = ((double)(a >> 11) + 0.5) * (1.0 / 9007199254740992.0);  // (0,1)
+        const double u2 = (double)(b >> 11) * (1.0 / 9007199254740992.0);          // [0,1)
+        out[i] = (T)(sqrt(-2.0 * log(u1)) * cospi(2.0 * u2));
+    }
+}
+
+// ---------------------------------------------------------------- Gram ----
+// G (c x c) = X^T X for X (rows x c) row-major.  Blocks take row chunks
+// (staged through shared memory); a 16 x 16 thread grid holds an NC x NC
+// register tile of G per thread (entries (ty + 16 i, tx + 16 j)).  G[a][b]
+// and G[b][a] see the same products in the same order, so G is exactly
+// symmetric.  Block partials are reduced in block order.
+constexpr int kGramRows = 32;
+template <typename T, int NC>
+__global__ void __launch_bounds__(256) k_gram_part(const T* __restrict__ X, int64_t rows, int c, int64_t chunk,
+                                                   double* __restrict__ part) {
+    extern __shared__ double xs[];  // kGramRows x c
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const int64_t r0 = blockIdx.x * chunk, r1 = std::min<int64_t>(rows, r0 + chunk);
+    double acc[NC][NC];
+#pragma unroll
+    for (int i = 0; i < NC; ++i)
+#pragma unroll
+        for (int j = 0; j < NC; ++j) acc[i][j] = 0.0;
+    for (int64_t rb = r0; rb < r1; rb += kGramRows) {
+        const int nr = (int)std::min<int64_t>(kGramRows, r1 - rb);
+        __syncthreads();
+        for (int t = threadIdx.x; t < nr * c; t += blockDim.x) xs[t] = (double)X[(rb + t / c) * c + t % c];
+        __syncthreads();
+        for (int r = 0; r < nr; ++r) {
+            double xa[NC], xb[NC];
+#pragma unroll
+            for (int i = 0; i < NC; ++i) {
+                const int a = ty + 16 * i, b = tx + 16 * i;
+                xa[i] = a < c ? xs[r * c + a] : 0.0;
+                xb[i] = b < c ? xs[r * c + b] : 0.0;
+            }
+#pragma unroll
+            for (int i = 0; i < NC; ++i)
+#pragma unroll
+                for (int j = 0; j < NC; ++j) acc[i][j] = fma(xa[i], xb[j], acc[i][j]);
+        }
+    }
+    double* out = part + (int64_t)blockIdx.x * c * c;
+#pragma unroll
+    for (int i = 0; i < NC; ++i)
+#pragma unroll
+        for (int j = 0; j < NC; ++j) {
+            const int a = ty + 16 * i, b = tx + 16 * j;
+            if (a < c && b < c) out[a * c + b] = acc[i][j];
+        }
+}
+__global__ void k_gram_reduce(const double* __restrict__ part, int nblocks, int c, double shift,
+                              double* __restrict__ G) {
+    const int cc = c * c;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < cc; p += gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int b = 0; b < nblocks; ++b) s += part[(int64_t)b * cc + p];
+        if (p / c == p % c) s += shift;
+        G[p] = s;
+    }
+}
+
+// ------------------------------------------------------ small dense ops ----
+// In-place upper Cholesky G = R^T R in one block; R overwrites the upper
+// triangle (lower set to 0).  status = 1 on a non-positive pivot.
+__global__ void k_cholesky(double* __restrict__ G, int c, int* __restrict__ status) {
+    __shared__ double piv;
+    for (int k = 0; k < c; ++k) {
+        if (threadIdx.x == 0) {
+            double d = G[k * c + k];
+            piv = (d > 0.0 && isfinite(d)) ? sqrt(d) : -1.0;
+            if (piv < 0.0) *status = 1;
+            else G[k * c + k] = piv;
+        }
+        __syncthreads();
+        if (piv < 0.0) return;
+        for (int j = k + 1 + threadIdx.x; j < c; j += blockDim.x) G[k * c + j] /= piv;
+        __syncthreads();
+        // trailing update of the upper triangle: G[i][j] -= R[k][i] R[k][j], i <= j
+        const int rem = c - k - 1;
+        for (int t = threadIdx.x; t < rem * rem; t += blockDim.x) {
+            const int i = k + 1 + t / rem, j = k + 1 + t % rem;
+            if (i <= j) G[i * c + j] -= G[k * c + i] * G[k * c + j];
+        }
+        __syncthreads();
+    }
+    for (int t = threadIdx.x; t < c * c; t += blockDim.x)
+        if (t / c > t % c) G[t] = 0.0;
+}
+
+// Rinv (upper) = R^-1, one block, column by column (back substitution).
+__global__ void k_tri_inv(const double* __restrict__ R, int c, double* __restrict__ Ri) {
+    for (int t = threadIdx.x; t < c * c; t += blockDim.x) Ri[t] = 0.0;
+    __syncthreads();
+    // solve R x = e_j for each column j (independent: one thread per column)
+    for (int j = threadIdx.x; j < c; j += blockDim.x) {
+        for (int i = j; i >= 0; --i) {
+            double s = (i == j) ? 1.0 : 0.0;
+            for (int k = i + 1; k <= j; ++k) s -= R[i * c + k] * Ri[k * c + j];
+            Ri[i * c + j] = s / R[i * c + i];
+        }
+    }
+}
+
+// C (c x c) = A (c x c) B (c x c), one block
+__global__ void k_small_gemm(const double* __restrict__ A, const double* __restrict__ B, int c,
+                             double* __restrict__ C) {
+    for (int t = threadIdx.x; t < c * c; t += blockDim.x) {
+        const int i = t / c, j = t % c;
+        double s = 0.0;
+        for (int k = 0; k < c; ++k) s = fma(A[i * c + k], B[k * c + j], s);
+        C[t] = s;
+    }
+}
+
+// Out (rows x cout) = X (rows x c) S (c x ldS, first cout columns); S in shared memory tiles.
+template <typename TI, typename TO>
+__global__ void __launch_bounds__(256) k_right_mul(const TI* __restrict__ X, int64_t rows, int c,
+                                                   const double* __restrict__ S, int lds, int cout,
+                                                   TO* __restrict__ Out) {
+    extern __shared__ double ss[];  // c x cout
+    for (int t = threadIdx.x; t < c * cout; t += blockDim.x) ss[t] = S[(t / cout) * lds + t % cout];
+    __syncthreads();
+    const int64_t total = rows * cout;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = t / cout;
+        const int j = (int)(t % cout);
+        const TI* xr = X + r * c;
+        double s = 0.0;
+        for (int k = 0; k < c; ++k) s = fma((double)xr[k], ss[k * cout + j], s);
+        Out[t] = (TO)s;
+    }
+}
+
+// normalize_columns (mod.rs:239-293): scale columns with norm > 1e-10
+template <typename T>
+__global__ void k_colnorm(T* __restrict__ X, int64_t rows, int c) {
+    __shared__ double sh[32];
+    __shared__ double scale;
+    const int j = blockIdx.x;
+    double acc = 0.0;
+    for (int64_t r = threadIdx.x; r < rows; r += blockDim.x) {
+        const double v = (double)X[r * c + j];
+        acc = fma(v, v, acc);
+    }
+    const double nrm = sqrt(block_sum(acc, sh));
+    if (threadIdx.x == 0) scale = nrm > 1e-10 ? 1.0 / nrm : 1.0;
+    __syncthreads();
+    if (nrm > 1e-10)
+        for (int64_t r = threadIdx.x; r < rows; r += blockDim.x) X[r * c + j] = (T)((double)X[r * c + j] * scale);
+}
+
+// One-sided Jacobi SVD of R (c x c, row-major) in one block: W = R V with
+// orthogonal columns, sigma_j = |W_j|, U_j = W_j / sigma_j.  Round-robin pair
+// ordering, one warp per pair.  Outputs sorted by descending sigma:
+// U (c x c), V (c x c), sig (c).  status = 2 if the sweep limit is reached.
+__global__ void __launch_bounds__(1024) k_jacobi_svd(const double* __restrict__ R, int c, double* __restrict__ U,
+                                                     double* __restrict__ V, double* __restrict__ sig,
+                                                     int* __restrict__ status) {
+    extern __shared__ double sm[];  // W (c x cp) | Vs (c x cp) | norms (cp) ; column-major
+    const int cp = c + (c & 1);     // even number of columns (zero padding column)
+    double* W = sm;
+    double* Vs = sm + (size_t)c * cp;
+    double* nr = Vs + (size_t)cp * cp;
+    __shared__ int s_rot;
+    for (int t = threadIdx.x; t < c * cp; t += blockDim.x) {
+        const int i = t % c, j = t / c;
+        W[j * c + i] = (j < c) ? R[i * c + j] : 0.0;
+    }
+    for (int t = threadIdx.x; t < cp * cp; t += blockDim.x) Vs[t] = ((t % cp) == (t / cp)) ? 1.0 : 0.0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int half = cp / 2;
+    const double tol = 2.220446049250313e-16 * (double)(c > 4 ? c : 4);
+    int sweep = 0;
+    for (; sweep < 60; ++sweep) {
+        if (threadIdx.x == 0) s_rot = 0;
+        __syncthreads();
+        for (int round = 0; round < cp - 1; ++round) {
+            for (int pr = warp; pr < half; pr += nwarps) {
+                // round-robin: position 0 fixed, others rotate
+                int a_pos = pr, b_pos = cp - 1 - pr;
+                auto at = [&](int pos) { return pos == 0 ? 0 : 1 + (pos - 1 + round) % (cp - 1); };
+                int p = at(a_pos), q = at(b_pos);
+                if (p > q) { int t = p; p = q; q = t; }
+                double al = 0, be = 0, ga = 0;
+                for (int i = lane; i < c; i += 32) {
+                    const double x = W[p * c + i], y = W[q * c + i];
+                    al = fma(x, x, al);
+                    be = fma(y, y, be);
+                    ga = fma(x, y, ga);
+                }
+                al = warp_sum(al);
+                be = warp_sum(be);
+                ga = warp_sum(ga);
+                if (ga != 0.0 && fabs(ga) > tol * sqrt(al * be)) {
+                    const double zeta = (be - al) / (2.0 * ga);
+                    const double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+                    const double cs = 1.0 / sqrt(1.0 + t * t), sn = cs * t;
+                    for (int i = lane; i < c; i += 32) {
+                        const double x = W[p * c + i], y = W[q * c + i];
+                        W[p * c + i] = cs * x - sn * y;
+                        W[q * c + i] = sn * x + cs * y;
+                    }
+                    for (int i = lane; i < cp; i += 32) {
+                        const double x = Vs[p * cp + i], y = Vs[q * cp + i];
+                        Vs[p * cp + i] = cs * x - sn * y;
+                        Vs[q * cp + i] = sn * x + cs * y;
+                    }
+                    if (lane == 0) s_rot = 1;
+                }
+            }
+            __syncthreads();
+        }
+        if (!s_rot) break;
+        __syncthreads();
+    }
+    if (sweep == 60 && threadIdx.x == 0) *status = 2;
+    for (int j = warp; j < cp; j += nwarps) {
+        double s = 0.0;
+        for (int i = lane; i < c; i += 32) s = fma(W[j * c + i], W[j * c + i], s);
+        s = warp_sum(s);
+        if (lane == 0) nr[j] = sqrt(s);
+    }
+    __syncthreads();
+    // rank of each column by descending norm (ties by index) -> output position
+    for (int j = threadIdx.x; j < c; j += blockDim.x) {
+        int pos = 0;
+        for (int k = 0; k < c; ++k)
+            if (nr[k] > nr[j] || (nr[k] == nr[j] && k < j)) ++pos;
+        sig[pos] = nr[j];
+        for (int i = 0; i < c; ++i) {
+            U[i * c + pos] = nr[j] > 0.0 ? W[j * c + i] / nr[j] : (i == pos ? 1.0 : 0.0);
+            V[i * c + pos] = Vs[j * cp + i];
+        }
+    }
+}
+
+template <typename T>
+__global__ void k_convert(const T* __restrict__ in, double* __restrict__ out, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = (double)in[i];
+}
+__global__ void k_to_float(const double* __restrict__ in, float* __restrict__ out, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = (float)in[i];
+}
+// copy the first `cout` columns of X (rows x c) into Out (rows x cout)
+__global__ void k_take_cols(const double* __restrict__ X, int64_t rows, int c, int cout, double* __restrict__ Out) {
+    const int64_t total = rows * cout;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x)
+        Out[t] = X[(t / cout) * c + t % cout];
+}
+
+// ------------------------------------------------------ host helpers ----
+struct RandCtx {
+    cudaStream_t s;
+    DevBuf<double> part, G, Rinv, R1, R2, Rtmp;
+    DevBuf<int> status;
+    int64_t part_cap = 0;
+};
+
+static void gram(RandCtx& cx, const double* X, int64_t rows, int c, double shift, double* G) {
+    if (c > 128) throw Error(SVDB_ERR_UNSUPPORTED, "randomized_svd: more than 128 sample columns");
+    const int sms = device_props().sms;
+    int64_t chunk = std::max<int64_t>(kGramRows * 4, (rows + sms * 2 - 1) / (sms * 2));
+    int nblk = (int)std::max<int64_t>(1, (rows + chunk - 1) / chunk);
+    if ((int64_t)nblk * c * c > cx.part_cap) {
+        cx.part_cap = (int64_t)nblk * c * c;
+        cx.part.alloc(cx.part_cap, cx.s);
+    }
+    const size_t smem = kGramRows * c * sizeof(double);
+    const int nc = (c + 15) / 16;
+    switch (nc) {
+        case 1: k_gram_part<double, 1><<<nblk, 256, smem, cx.s>>>(X, rows, c, chunk, cx.part.p); break;
+        case 2: k_gram_part<double, 2><<<nblk, 256, smem, cx.s>>>(X, rows, c, chunk, cx.part.p); break;
+        case 3: k_gram_part<double, 3><<<nblk, 256, smem, cx.s>>>(X, rows, c, chunk, cx.part.p); break;
+        case 4: k_gram_part<double, 4><<<nblk, 256, smem, cx.s>>>(X, rows, c, chunk, cx.part.p); break;
+        case 5: k_gram_part<double, 5><<<nblk, 256, smem, cx.s>>>(X, rows, c, chunk, cx.part.p); break;
+        case 6: k_gram_part<double, 6><<<nblk, 256, smem, cx.s>>>(X, rows, c, chunk, cx.part.p); break;
+        case 7: k_gram_part<double, 7><<<nblk, 256, smem, cx.s>>>(X, rows, c, chunk, cx.part.p); break;
+        default: k_gram_part<double, 8><<<nblk, 256, smem, cx.s>>>(X, rows, c, chunk, cx.part.p); break;
+    }
+    k_gram_reduce<<<nb((int64_t)c * c, 128), 128, 0, cx.s>>>(cx.part.p, nblk, c, shift, G);
+    SVDB_CHECK_LAUNCH_N(2);
+}
+
+static void right_mul(const double* X, int64_t rows, int c, const double* S, int lds, int cout, double* Out,
+                      cudaStream_t s) {
+    size_t smem = (size_t)c * cout * sizeof(double);
+    if (smem > 200 * 1024) throw Error(SVDB_ERR_UNSUPPORTED, "dense factor wider than the shared-memory tile");
+    if (smem > 48 * 1024)
+        SVDB_CUDA(cudaFuncSetAttribute(k_right_mul<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
+    k_right_mul<double, double><<<nb(rows * cout, 256), 256, smem, s>>>(X, rows, c, S, lds, cout, Out);
+    SVDB_CHECK_LAUNCH();
+}
+
+// One CholeskyQR pass on X (rows x c) in place; R (c x c) returned. false on breakdown.
+static bool cqr_pass(RandCtx& cx, double* X, double* Xtmp, int64_t rows, int c, double shift, double* R) {
+    gram(cx, X, rows, c, shift, R);
+    SVDB_CUDA(cudaMemsetAsync(cx.status.p, 0, sizeof(int), cx.s));
+    k_cholesky<<<1, 256, 0, cx.s>>>(R, c, cx.status.p);
+    SVDB_CHECK_LAUNCH();
+    int st = 0;
+    SVDB_CUDA(cudaMemcpyAsync(&st, cx.status.p, sizeof(int), cudaMemcpyDeviceToHost, cx.s));
+    SVDB_CUDA(cudaStreamSynchronize(cx.s));
+    if (st) return false;
+    k_tri_inv<<<1, 128, 0, cx.s>>>(R, c, cx.Rinv.p);
+    SVDB_CHECK_LAUNCH();
+    right_mul(X, rows, c, cx.Rinv.p, c, c, Xtmp, cx.s);
+    SVDB_CUDA(cudaMemcpyAsync(X, Xtmp, rows * c * sizeof(double), cudaMemcpyDeviceToDevice, cx.s));
+    return true;
+}
+
+// Thin Q of X (rows x c, rows >= c) in place, R (c x c) = R_last ... R_first.
+static void cholesky_qr(RandCtx& cx, double* X, int64_t rows, int c, double* Rout) {
+    DevBuf<double> Xtmp(rows * c, cx.s);
+    bool ok1 = cqr_pass(cx, X, Xtmp.p, rows, c, 0.0, cx.R1.p);
+    if (!ok1) {
+        // shifted CholeskyQR: shift = 11 (rows c + c(c+1)) u ||X||_F^2
+        gram(cx, X, rows, c, 0.0, cx.G.p);
+        std::vector<double> g((size_t)c * c);
+        SVDB_CUDA(cudaMemcpyAsync(g.data(), cx.G.p, g.size() * 8, cudaMemcpyDeviceToHost, cx.s));
+        SVDB_CUDA(cudaStreamSynchronize(cx.s));
+        double fro2 = 0.0;
+        for (int i = 0; i < c; ++i) fro2 += g[(size_t)i * c + i];
+        double shift = 11.0 * ((double)rows * c + (double)c * (c + 1)) * 1.1102230246251565e-16 * fro2;
+        if (!(shift > 0.0)) shift = 1e-300;
+        if (!cqr_pass(cx, X, Xtmp.p, rows, c, shift, cx.R1.p))
+            throw Error(SVDB_ERR_LAS2, "randomized_svd: shifted CholeskyQR broke down");
+    }
+    if (!cqr_pass(cx, X, Xtmp.p, rows, c, 0.0, cx.R2.p)) {
+        if (!cqr_pass(cx, X, Xtmp.p, rows, c, 1e-14, cx.R2.p))
+            throw Error(SVDB_ERR_LAS2, "randomized_svd: CholeskyQR broke down");
+    }
+    // a third pass after a shifted first one restores orthogonality
+    if (!ok1) {
+        k_small_gemm<<<1, 256, 0, cx.s>>>(cx.R2.p, cx.R1.p, c, cx.Rtmp.p);
+        SVDB_CHECK_LAUNCH();
+        SVDB_CUDA(cudaMemcpyAsync(cx.R1.p, cx.Rtmp.p, (size_t)c * c * 8, cudaMemcpyDeviceToDevice, cx.s));
+        if (!cqr_pass(cx, X, Xtmp.p, rows, c, 0.0, cx.R2.p))
+            throw Error(SVDB_ERR_LAS2, "randomized_svd: CholeskyQR broke down");
+    }
+    if (Rout) k_small_gemm<<<1, 256, 0, cx.s>>>(cx.R2.p, cx.R1.p, c, Rout);
+    SVDB_CHECK_LAUNCH_N(Rout ? 1 : 0);
+}
+
+// qr(X).q() for X (rows x c): returns the column count of Q; X is replaced by
+// Q (rows x k, k = min(rows, c)) stored with row stride k.
+static int thin_q(RandCtx& cx, DevBuf<double>& X, int64_t rows, int c) {
+    if (rows >= c) {
+        cholesky_qr(cx, X.p, rows, c, nullptr);
+        return c;
+    }
+    // wide: Q spans R^rows; take the leading rows x rows block's Q
+    const int k = (int)rows;
+    DevBuf<double> Xk((int64_t)rows * k, cx.s);
+    k_take_cols<<<nb(rows * k, 256), 256, 0, cx.s>>>(X.p, rows, c, k, Xk.p);
+    SVDB_CHECK_LAUNCH();
+    cholesky_qr(cx, Xk.p, rows, k, nullptr);
+    X = std::move(Xk);
+    return k;
+}
+
+static double ms_since(std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+void randomized(const svdb_matrix* A, uint64_t target_rank, uint64_t n_oversamples, uint64_t n_power_iters,
+                int normalizer, int mean_center, int has_seed, uint64_t seed, int verbose, const svdb_options& o,
+                svdb_rec* rec) {
+    if (mean_center) throw Error(SVDB_ERR_UNSUPPORTED, "randomized_svd: mean_center is not provided");
+    cudaStream_t s = o.stream ? (cudaStream_t)o.stream : A->stream;
+    const bool mixed = o.precision == SVDB_MIXED;
+    const int64_t m = A->nrows, n = A->ncols;
+    const int64_t rank = std::min<int64_t>((int64_t)target_rank, std::min(m, n));
+    int l = (int)(rank + (int64_t)n_oversamples);
+    if (l <= 0) throw Error(SVDB_ERR_SHAPE, "randomized_svd: zero sample columns");
+    const DevCompressed& Acsr = csr_of(A);
+    const DevCompressed& Acsc = csc_of(A);
+    if (mixed) ensure_fp32(A);
+    auto t0 = std::chrono::steady_clock::now();
+    cudaEvent_t e0, e1;
+    SVDB_CUDA(cudaEventCreate(&e0));
+    SVDB_CUDA(cudaEventCreate(&e1));
+    SVDB_CUDA(cudaEventRecord(e0, s));
+    float spmm_ms = 0.f;
+
+    RandCtx cx;
+    cx.s = s;
+    const int cmax = l;
+    cx.G.alloc((size_t)cmax * cmax, s);
+    cx.Rinv.alloc((size_t)cmax * cmax, s);
+    cx.R1.alloc((size_t)cmax * cmax, s);
+    cx.R2.alloc((size_t)cmax * cmax, s);
+    cx.Rtmp.alloc((size_t)cmax * cmax, s);
+    cx.status.alloc(1, s);
+
+    // Omega (n x l)
+    DevBuf<double> Om(std::max<int64_t>(n * l, 1), s);
+    if (o.omega) SVDB_CUDA(cudaMemcpyAsync(Om.p, o.omega, n * l * 8, cudaMemcpyHostToDevice, s));
+    else k_omega<double><<<nb(n * l, 256), 256, 0, s>>>(has_seed ? seed : 0, n * l, Om.p);
+    SVDB_CHECK_LAUNCH();
+
+    // Sparse products: FP64 operands, or FP32 copies under SVDB_MIXED.
+    DevBuf<float> f_in, f_out;
+    auto spmm = [&](const DevCompressed& M, const double* X, int c, double* Y) {
+        cudaEvent_t a, b;
+        SVDB_CUDA(cudaEventCreate(&a));
+        SVDB_CUDA(cudaEventCreate(&b));
+        SVDB_CUDA(cudaEventRecord(a, s));
+        if (!mixed) {
+            spmm_dev<double>(M, false, X, c, Y, s);
+        } else {
+            if ((int64_t)f_in.n < M.nminor * c) f_in.alloc(M.nminor * c, s);
+            if ((int64_t)f_out.n < M.nmajor * c) f_out.alloc(M.nmajor * c, s);
+            k_to_float<<<nb(M.nminor * c, 256), 256, 0, s>>>(X, f_in.p, M.nminor * c);
+            spmm_dev<float>(M, true, f_in.p, c, f_out.p, s);
+            k_convert<float><<<nb(M.nmajor * c, 256), 256, 0, s>>>(f_out.p, Y, M.nmajor * c);
+            SVDB_CHECK_LAUNCH_N(2);
+        }
+        SVDB_CUDA(cudaEventRecord(b, s));
+        SVDB_CUDA(cudaEventSynchronize(b));
+        float t = 0.f;
+        cudaEventElapsedTime(&t, a, b);
+        spmm_ms += t;
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+    };
+    auto normalize = [&](DevBuf<double>& X, int64_t rows, int c) -> int {
+        if (normalizer == SVDB_NORM_QR) return thin_q(cx, X, rows, c);
+        if (normalizer == SVDB_NORM_LU) {
+            k_colnorm<double><<<c, 256, 0, s>>>(X.p, rows, c);
+            SVDB_CHECK_LAUNCH();
+        }
+        return c;
+    };
+
+    if (verbose) printf("SVD | Randomized | Multiplying m with omega matrix....\n");
+    DevBuf<double> Y(std::max<int64_t>(m * l, 1), s);
+    spmm(Acsr, Om.p, l, Y.p);
+    int c = l;
+    if (verbose) printf("SVD | Randomized | Multiplication done, took: %.3f ms of total running time\n", ms_since(t0));
+    if (verbose) printf("SVD | Randomized | Starting power iterations....\n");
+    for (uint64_t it = 0; it < n_power_iters; ++it) {
+        if (verbose)
+            printf("SVD | Randomized | Running power-iteration: %llu, current time: %.3f ms\n",
+                   (unsigned long long)it, ms_since(t0));
+        DevBuf<double> Z(std::max<int64_t>(n * c, 1), s);
+        spmm(Acsc, Y.p, c, Z.p);
+        c = normalize(Z, n, c);
+        DevBuf<double> Y2(std::max<int64_t>(m * c, 1), s);
+        spmm(Acsr, Z.p, c, Y2.p);
+        Y = std::move(Y2);
+        c = normalize(Y, m, c);
+        if (verbose)
+            printf("SVD | Randomized | Power Iteration Normalization Backward-Step %.3f ms\n", ms_since(t0));
+    }
+    if (verbose) printf("SVD | Randomized | Running QR-Normalization after Power-Iterations %.3f ms\n", ms_since(t0));
+    c = thin_q(cx, Y, m, c);  // Q = qr(y).q()
+    // B^T = A^T Q (n x c)
+    DevBuf<double> Bt(std::max<int64_t>(n * c, 1), s);
+    spmm(Acsc, Y.p, c, Bt.p);
+    if (verbose) printf("SVD | Randomized | Transposed Matrix Multiplication %.3f ms\n", ms_since(t0));
+
+    // SVD(B), B = Bt^T (c x n).  r = min(c, n).
+    const int r = (int)std::min<int64_t>(c, n);
+    DevBuf<double> UB((size_t)c * r, s), sig(r, s), VtB((size_t)r * n, s);
+    {
+        DevBuf<double> Ur((size_t)r * r, s), Vr((size_t)r * r, s), R((size_t)r * r, s);
+        SVDB_CUDA(cudaMemsetAsync(cx.status.p, 0, sizeof(int), s));
+        const size_t smem = ((size_t)r * (r + 1) + (size_t)(r + 1) * (r + 1) + (r + 1)) * sizeof(double);
+        if (smem > 220 * 1024) throw Error(SVDB_ERR_UNSUPPORTED, "randomized_svd: sample width above the Jacobi tile");
+        SVDB_CUDA(cudaFuncSetAttribute(k_jacobi_svd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        if (n >= c) {
+            // B^T = Q_b R;  R = U_J S V_J^T  ->  B = V_J S (Q_b U_J)^T
+            cholesky_qr(cx, Bt.p, n, c, R.p);
+            k_jacobi_svd<<<1, 1024, smem, s>>>(R.p, r, Ur.p, Vr.p, sig.p, cx.status.p);
+            // U_B = V_J (c x r); V_B = Q_b U_J (n x r)
+            SVDB_CUDA(cudaMemcpyAsync(UB.p, Vr.p, (size_t)r * r * 8, cudaMemcpyDeviceToDevice, s));
+            DevBuf<double> VB((size_t)n * r, s);
+            right_mul(Bt.p, n, c, Ur.p, r, r, VB.p, s);
+            transpose_dense<double>(VB.p, VtB.p, n, r, s);
+        } else {
+            // B (c x n) is tall: B = Q_b R (R: n x n), R = U_J S V_J^T -> B = (Q_b U_J) S V_J^T
+            DevBuf<double> B((size_t)c * n, s);
+            transpose_dense<double>(Bt.p, B.p, n, c, s);
+            cholesky_qr(cx, B.p, c, (int)n, R.p);
+            k_jacobi_svd<<<1, 1024, smem, s>>>(R.p, r, Ur.p, Vr.p, sig.p, cx.status.p);
+            right_mul(B.p, c, (int)n, Ur.p, r, r, UB.p, s);
+            transpose_dense<double>(Vr.p, VtB.p, r, r, s);
+        }
+        SVDB_CHECK_LAUNCH();
+    }
+    if (verbose) printf("SVD | Randomized | Running Singular Value Decomposition, took %.3f ms\n", ms_since(t0));
+    // U = Q U_B (m x r), truncated to actual_rank columns
+    const int64_t actual = std::min<int64_t>((int64_t)target_rank, r);
+    DevBuf<double> U(std::max<int64_t>(m * actual, 1), s), Vt(std::max<int64_t>(actual * n, 1), s),
+        S(std::max<int64_t>(actual, 1), s);
+    if (actual > 0) {
+        right_mul(Y.p, m, c, UB.p, r, (int)actual, U.p, s);
+        SVDB_CUDA(cudaMemcpyAsync(Vt.p, VtB.p, actual * n * 8, cudaMemcpyDeviceToDevice, s));
+        SVDB_CUDA(cudaMemcpyAsync(S.p, sig.p, actual * 8, cudaMemcpyDeviceToDevice, s));
+    }
+    SVDB_CUDA(cudaEventRecord(e1, s));
+    SVDB_CUDA(cudaStreamSynchronize(s));
+    float tot = 0.f;
+    cudaEventElapsedTime(&tot, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+
+    std::memset(rec, 0, sizeof(*rec));
+    rec->d = actual;
+    rec->u_rows = m; rec->u_cols = actual;
+    rec->vt_rows = actual; rec->vt_cols = n;
+    if (o.result_on_device) {
+        rec->u = U.detach(); rec->s = S.detach(); rec->vt = Vt.detach();
+        rec->on_device = 1;
+    } else {
+        rec->u = (double*)malloc(std::max<int64_t>(m * actual, 1) * 8);
+        rec->s = (double*)malloc(std::max<int64_t>(actual, 1) * 8);
+        rec->vt = (double*)malloc(std::max<int64_t>(actual * n, 1) * 8);
+        if (actual) {
+            SVDB_CUDA(cudaMemcpyAsync(rec->u, U.p, m * actual * 8, cudaMemcpyDeviceToHost, s));
+            SVDB_CUDA(cudaMemcpyAsync(rec->s, S.p, actual * 8, cudaMemcpyDeviceToHost, s));
+            SVDB_CUDA(cudaMemcpyAsync(rec->vt, Vt.p, actual * n * 8, cudaMemcpyDeviceToHost, s));
+        }
+        SVDB_CUDA(cudaStreamSynchronize(s));
+    }
+    rec->origin = SVDB_REC_RANDOMIZED;
+    // create_diagnostics (mod.rs:214-237)
+    svdb_diagnostics& dg = rec->diagnostics;
+    dg.non_zero = A->nnz;
+    dg.dimensions = target_rank;
+    dg.iterations = n_power_iters;
+    dg.transposed = 0;
+    dg.lanczos_steps = 0;
+    dg.ritz_values_stabilized = actual;
+    dg.significant_values = actual;
+    dg.singular_values = actual;
+    dg.end_interval[0] = -1e-30;
+    dg.end_interval[1] = 1e-30;
+    dg.kappa = 1e-6;
+    dg.random_seed = (uint32_t)(has_seed ? seed : 0);
+    rec->time_ms_total = tot;
+    rec->time_ms_spmv = spmm_ms;
+    rec->time_ms_ortho = tot - spmm_ms;
+}
+
+}  // namespace svdb

@@ -1,0 +1,138 @@
+// Internal declarations shared by the CUDA sources of libsvdb200.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/svdb200.h"
+
+namespace svdb {
+
+// ---------------------------------------------------------------- errors ----
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void set_last_error(const std::string& msg);
+
+#define SVDB_CUDA(call)                                                                        \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            throw ::svdb::Error(e_ == cudaErrorMemoryAllocation ? SVDB_ERR_OOM : SVDB_ERR_CUDA, \
+                                std::string(#call) + ": " + cudaGetErrorString(e_));            \
+    } while (0)
+
+// Every kernel launch site is followed by SVDB_CHECK_LAUNCH(n), n being the
+// number of kernels launched since the previous check; the count feeds
+// svdb_kernel_launches().
+void count_launches(uint64_t n);
+#define SVDB_CHECK_LAUNCH_N(n)             \
+    do {                                   \
+        ::svdb::count_launches(n);         \
+        SVDB_CUDA(cudaGetLastError());     \
+    } while (0)
+#define SVDB_CHECK_LAUNCH() SVDB_CHECK_LAUNCH_N(1)
+
+// --------------------------------------------------------- device memory ----
+// Owning device buffer, stream-ordered (cudaMallocAsync pool).
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    cudaStream_t s = nullptr;
+    DevBuf() {}
+    DevBuf(size_t count, cudaStream_t st) { alloc(count, st); }
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n), s(o.s) { o.p = nullptr; o.n = 0; }
+    DevBuf& operator=(DevBuf&& o) noexcept {
+        if (this != &o) { release(); p = o.p; n = o.n; s = o.s; o.p = nullptr; o.n = 0; }
+        return *this;
+    }
+    ~DevBuf() { release(); }
+    void alloc(size_t count, cudaStream_t st) {
+        release();
+        s = st;
+        n = count;
+        if (count) SVDB_CUDA(cudaMallocAsync((void**)&p, count * sizeof(T), st));
+    }
+    void release() {
+        if (p) cudaFreeAsync(p, s);
+        p = nullptr;
+        n = 0;
+    }
+    T* detach() { T* q = p; p = nullptr; n = 0; return q; }
+    size_t bytes() const { return n * sizeof(T); }
+};
+
+// ------------------------------------------------------------ matrices ------
+// A compressed sparse structure in HBM: `nmajor` rows of a CSR (or columns of
+// a CSC, i.e. rows of the transpose).  Column indices are int32 (minor
+// dimension < 2^31), offsets int64.
+struct DevCompressed {
+    int64_t nmajor = 0, nminor = 0, nnz = 0;
+    DevBuf<int64_t> ptr;
+    DevBuf<int32_t> idx;
+    DevBuf<double> val;
+    DevBuf<float> val32;  // FP32 copy of val, made on first mixed-precision use
+    double avg_per_major() const { return nmajor ? double(nnz) / double(nmajor) : 0.0; }
+};
+
+enum MatKind { KIND_CSR = 0, KIND_CSC = 1, KIND_COO = 2, KIND_MASKED = 3 };
+
+}  // namespace svdb
+
+struct svdb_matrix {
+    int kind = svdb::KIND_CSR;
+    int device = 0;
+    int64_t nrows = 0, ncols = 0;  // logical shape (masked: masked column count)
+    int64_t nnz = 0;               // SMat::nnz (masked: entries in the mask)
+    cudaStream_t stream = nullptr;
+    svdb::DevCompressed csr;  // A, rows
+    svdb::DevCompressed csc;  // A^T, rows = columns of A
+    // masked view data
+    const svdb_matrix* parent = nullptr;
+    bool all_columns = false;
+    svdb::DevBuf<int64_t> m2o, o2m;
+    std::mutex mu;  // serialises calls on one handle
+};
+
+namespace svdb {
+
+const DevCompressed& csr_of(const svdb_matrix* a);
+const DevCompressed& csc_of(const svdb_matrix* a);
+void ensure_fp32(const svdb_matrix* a);
+
+struct DeviceProps {
+    int sms = 148;
+    int coop = 1;
+    size_t l2 = 0;
+};
+const DeviceProps& device_props();
+
+// ------------------------------------------------------- kernel entries ----
+// y[r] = sum_k val[k] * x[idx[k]] over the rows of `m` (group-per-row).
+void spmv(const DevCompressed& m, bool fp32, const double* x, double* y, cudaStream_t s);
+
+// Reductions and BLAS-1 (deterministic two-level reductions).
+void dot(const double* x, const double* y, int64_t n, double* d_out, double* scratch, cudaStream_t s);
+double dot_host(const double* x, const double* y, int64_t n, double* scratch, cudaStream_t s);
+void axpy(double a, const double* x, double* y, int64_t n, cudaStream_t s);   // y += a*x (unfused mul then add)
+void scal(double a, double* x, int64_t n, cudaStream_t s);                    // x *= a
+void copy(const double* x, double* y, int64_t n, cudaStream_t s);
+size_t reduce_scratch_doubles();
+
+// Start vector: rand 0.9 StdRng::from_seed(seed bytes) + random_range(-1.0..1.0).
+void start_vector(uint32_t seed, double* w, int64_t n, cudaStream_t s);
+
+// y[e] = y[e] - t[i] * Q[i0+i][e], sequentially over i (the crate's axpy order)
+void gemv_sub(const double* Q, int64_t n, int64_t i0, int64_t cnt, const double* t, double* y, cudaStream_t s);
+
+}  // namespace svdb

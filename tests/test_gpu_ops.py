@@ -1,0 +1,76 @@
+"""SMat operator entry points on the GPU against the checker: svd_opa / svd_opb
+(src/lanczos/mod.rs:311-319, 1427-1700) for CSR, CSC, COO and masked views,
+and the dense products multiply_with_dense / multiply_transposed_by_dense
+(src/lanczos/masked.rs:265-733).  Tolerance 1e-13 relative to the largest
+entry (FMA and summation order differ)."""
+import numpy as np
+import pytest
+
+import matrices as M
+import oracle as O
+from gpu_util import oracle_args, upload
+
+pytestmark = pytest.mark.gpu
+
+
+def close(a, b, tol=1e-13):
+    scale = max(np.max(np.abs(b)), 1e-300)
+    np.testing.assert_allclose(a, b, rtol=0, atol=tol * scale)
+
+
+@pytest.mark.parametrize("kind", ["csr", "csc", "coo", "masked"])
+@pytest.mark.parametrize("shape", [(50, 30), (300, 700), (1000, 64)])
+def test_opa_opb(kind, shape):
+    A = M.uniform(shape[0], shape[1], 0.05, 7)
+    mask = (np.random.default_rng(2).random(shape[1]) < 0.7).astype(np.uint8) if kind == "masked" else None
+    h = upload(kind, A, mask)
+    ncols = int(mask.sum()) if mask is not None else shape[1]
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal(ncols)
+    y = rng.standard_normal(shape[0])
+    ka = "masked" if kind == "masked" else kind
+    OA = oracle_args(kind, A)
+    close(h.svd_opa(x), O.opa(ka, OA, x, False, mask=mask))
+    close(h.svd_opa(y, transposed=True), O.opa(ka, OA, y, True, mask=mask))
+    close(h.svd_opb(x), O.opa(ka, OA, O.opa(ka, OA, x, False, mask=mask), True, mask=mask))
+
+
+def test_power_law_rows():
+    # rows from 1 to 3000 entries exercise every group width of the row gather
+    rng = np.random.default_rng(11)
+    m, n = 4000, 5000
+    k = np.minimum((rng.pareto(1.2, m) * 5 + 1).astype(int), 3000)
+    import scipy.sparse as sp
+    rows = np.repeat(np.arange(m), k)
+    cols = np.concatenate([rng.choice(n, kk, replace=False) for kk in k])
+    S = sp.csr_matrix((rng.standard_normal(len(rows)), (rows, cols)), shape=(m, n))
+    A = M.from_scipy(S)
+    h = upload("csr", A)
+    x = rng.standard_normal(n)
+    close(h.svd_opa(x), S @ x, 1e-12)
+    y = rng.standard_normal(m)
+    close(h.svd_opa(y, transposed=True), S.T @ y, 1e-12)
+
+
+@pytest.mark.parametrize("l", [1, 7, 32, 60, 150])
+def test_dense_products(l):
+    A = M.uniform(400, 250, 0.04, 21)
+    mask = (np.random.default_rng(4).random(250) < 0.5).astype(np.uint8)
+    rng = np.random.default_rng(5)
+    for h, mk in [(upload("csr", A), np.ones(250, np.uint8)), (upload("masked", A, mask), mask)]:
+        nm = int(mk.sum())
+        X = rng.standard_normal((nm, l))
+        Y = rng.standard_normal((400, l))
+        close(h.multiply_with_dense(X), O.masked_dense(A, mk, "AX", X), 1e-12)
+        close(h.multiply_with_dense(Y, transpose_self=True), O.masked_dense(A, mk, "ATX", Y), 1e-12)
+        close(h.multiply_transposed_by_dense(Y), O.masked_dense(A, mk, "XTA", Y), 1e-12)
+
+
+def test_empty_rows_and_columns():
+    import scipy.sparse as sp
+    S = sp.csr_matrix(([1.0, 2.0, 3.0], ([0, 5, 5], [3, 3, 9])), shape=(8, 12))
+    A = M.from_scipy(S)
+    h = upload("csr", A)
+    x = np.arange(12.0)
+    close(h.svd_opa(x), S @ x)
+    close(h.svd_opa(np.ones(8), transposed=True), S.T @ np.ones(8))

@@ -1,0 +1,90 @@
+"""randomized_svd on the GPU against the checker with the same Omega
+(src/randomized/mod.rs:24-199).  QR is CholeskyQR2 here and Householder in the
+checker, so column signs may differ: singular values are compared directly
+(1e-10 relative, f64), singular vectors through principal angles (cosines
+within 1e-8 of 1 for the leading, well-separated ones)."""
+import numpy as np
+import pytest
+
+import matrices as M
+import oracle as O
+from gpu_util import subspace_cos, upload
+from single_svdlib import MaskedCSRMatrix, UnsupportedError, randomized
+from single_svdlib.randomized import PowerIterationNormalizer as PIN
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("norm", ["QR", "LU", "None"])
+@pytest.mark.parametrize("q", [0, 1, 3])
+def test_parity_with_checker(norm, q):
+    A = M.lowrank_plus_noise(400, 150, 12, 1e-2, 31, density=0.3)
+    l = 10 + 6
+    om = M.omega(150, l, 5)
+    ref = O.randomized(A, 10, 6, q, norm, omega=om)
+    got = randomized.randomized_svd(upload("csr", A), 10, 6, q, getattr(PIN, norm if norm != "None" else "None_"),
+                                    False, 7, False, omega=om)
+    assert got.d == ref["d"] == 10
+    assert got.u.shape == (400, 10) and got.vt.shape == (10, 150)
+    tol = 1e-10 if norm == "QR" else 1e-7
+    np.testing.assert_allclose(got.s, ref["s"], rtol=tol)
+    k = 5
+    assert np.all(subspace_cos(got.u[:, :k], ref["u"][:, :k]) > 1 - 1e-8)
+    assert np.all(subspace_cos(got.vt[:k].T, ref["vt"][:k].T) > 1 - 1e-8)
+
+
+def test_all_true_masked_and_diagnostics():
+    A = M.uniform(300, 90, 0.1, 41)
+    om = M.omega(90, 15, 1)
+    mv = MaskedCSRMatrix(upload("csr", A), np.ones(90, np.uint8))
+    got = randomized.randomized_svd(mv, 10, 5, 2, PIN.QR, False, 42, False, omega=om)
+    ref = O.randomized(A, 10, 5, 2, "QR", omega=om)
+    np.testing.assert_allclose(got.s, ref["s"], rtol=1e-10)
+    dg = got.diagnostics
+    assert (dg.non_zero, dg.dimensions, dg.iterations, dg.lanczos_steps, dg.random_seed) == (len(A["data"]), 10, 2,
+                                                                                              0, 42)
+    assert dg.significant_values == dg.singular_values == dg.ritz_values_stabilized == 10
+    # descending, positive (randomized/mod.rs:683-689)
+    assert np.all(np.diff(got.s) <= 0) and np.all(got.s > 0)
+    # recompose works on the m x d orientation
+    assert got.recompose().shape == (300, 90)
+
+
+def test_real_mask():
+    A = M.uniform(250, 120, 0.1, 43)
+    mask = (np.random.default_rng(2).random(120) < 0.5).astype(np.uint8)
+    nm = int(mask.sum())
+    om = M.omega(nm, 12, 3)
+    mv = MaskedCSRMatrix(upload("csr", A), mask)
+    got = randomized.randomized_svd(mv, 8, 4, 2, PIN.QR, False, 1, False, omega=om)
+    ref = O.randomized(A, 8, 4, 2, "QR", omega=om, mask=mask)
+    np.testing.assert_allclose(got.s, ref["s"], rtol=1e-10)
+
+
+def test_mixed_precision_error_is_stated():
+    A = M.lowrank_plus_noise(500, 200, 15, 1e-2, 51, density=0.2)
+    om = M.omega(200, 25, 2)
+    f64 = randomized.randomized_svd(upload("csr", A), 15, 10, 3, PIN.QR, False, 1, False, omega=om)
+    mix = randomized.randomized_svd(upload("csr", A), 15, 10, 3, PIN.QR, False, 1, False, omega=om,
+                                    precision="mixed")
+    rel = np.max(np.abs(mix.s - f64.s) / f64.s)
+    assert rel < 1e-5, rel
+
+
+def test_device_omega_is_seeded():
+    A = M.uniform(200, 80, 0.1, 44)
+    r1 = randomized.randomized_svd(upload("csr", A), 5, 5, 1, PIN.QR, False, 9, False)
+    r2 = randomized.randomized_svd(upload("csr", A), 5, 5, 1, PIN.QR, False, 9, False)
+    np.testing.assert_array_equal(r1.s, r2.s)
+    truth = np.linalg.svd(M.to_scipy(A).toarray(), compute_uv=False)[:5]
+    assert np.max(np.abs(r1.s - truth) / truth) < 0.3
+
+
+def test_small_wide_and_rank_edge_cases():
+    # l larger than ncols: Q has min(rows, l) columns (nalgebra's thin QR)
+    A = M.uniform(30, 8, 0.6, 45)
+    got = randomized.randomized_svd(upload("csr", A), 5, 10, 2, PIN.QR, False, 3, False)
+    truth = np.linalg.svd(M.to_scipy(A).toarray(), compute_uv=False)[:5]
+    np.testing.assert_allclose(got.s, truth, rtol=1e-8)
+    with pytest.raises(UnsupportedError):
+        randomized.randomized_svd(upload("csr", A), 3, 2, 1, PIN.QR, True, 3, False)
