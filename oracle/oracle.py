@@ -49,7 +49,8 @@ class _Las2Out(C.Structure):
 
 class _RandOut(C.Structure):
     _fields_ = [("d", C.c_uint64), ("m", C.c_uint64), ("n", C.c_uint64),
-                ("u", C.POINTER(C.c_double)), ("s", C.POINTER(C.c_double)), ("vt", C.POINTER(C.c_double))]
+                ("u", C.POINTER(C.c_double)), ("s", C.POINTER(C.c_double)), ("vt", C.POINTER(C.c_double)),
+                ("t_sparse", C.c_double), ("t_rows", C.c_double), ("t_fixed", C.c_double)]
 
 
 def build():
@@ -251,7 +252,8 @@ def randomized(A, target_rank, n_oversamples, n_power_iters, normalizer="QR", om
         res = {"d": d,
                "u": np.ctypeslib.as_array(out.u, (max(1, m * d),))[: m * d].reshape(m, d).copy(),
                "s": np.ctypeslib.as_array(out.s, (max(1, d),))[:d].copy(),
-               "vt": np.ctypeslib.as_array(out.vt, (max(1, d * n),))[: d * n].reshape(d, n).copy()}
+               "vt": np.ctypeslib.as_array(out.vt, (max(1, d * n),))[: d * n].reshape(d, n).copy(),
+               "times": {"sparse": out.t_sparse, "rows": out.t_rows, "fixed": out.t_fixed}}
     finally:
         lib().orc_rand_free(C.byref(out))
     return res

@@ -27,6 +27,7 @@
 //     switch reproducing the masked A^T*Y indexing of masked.rs:388-393.
 // ============================================================================
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdint>
 #include <cstdlib>
@@ -1405,11 +1406,19 @@ struct RandResult {
     std::vector<double> u;   // m x d row-major
     std::vector<double> s;   // d
     std::vector<double> vt;  // d x n row-major
+    // wall time by what it scales with: sparse products (nnz), work on
+    // m-row dense matrices (rows), work on n-row matrices and the small SVD (fixed)
+    double t_sparse = 0, t_rows = 0, t_fixed = 0;
 };
+
+static double wall() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
 
 // normalizer: 0 = QR, 1 = LU (column normalisation), 2 = None
 static RandResult randomized_svd(const MaskedOp& M, size_t target_rank, size_t n_oversamples, size_t n_power_iters,
                                  int normalizer, const double* omega_rowmajor, bool compat_d3) {
+    RandResult R;
     size_t m = M.nrows(), n = M.ncols();
     size_t rank = std::min(target_rank, std::min(m, n));
     size_t l = rank + n_oversamples;
@@ -1417,27 +1426,36 @@ static RandResult randomized_svd(const MaskedOp& M, size_t target_rank, size_t n
     for (size_t i = 0; i < n; ++i)
         for (size_t c = 0; c < l; ++c) omega(i, c) = omega_rowmajor[i * l + c];
     DMatrix y;
+    double t = wall();
+    auto lap = [&](double& acc) { double now = wall(); acc += now - t; t = now; };
     masked_multiply_with_dense(M, omega, y, false, compat_d3);
+    lap(R.t_sparse);
     if (n_power_iters > 0) {
         DMatrix z;
         for (size_t it = 0; it < n_power_iters; ++it) {
             masked_multiply_with_dense(M, y, z, true, compat_d3);
+            lap(R.t_sparse);
             if (normalizer == 0) z = thin_q(z);
             else if (normalizer == 1) normalize_columns(z);
+            lap(R.t_fixed);
             masked_multiply_with_dense(M, z, y, false, compat_d3);
+            lap(R.t_sparse);
             if (normalizer == 0) y = thin_q(y);
             else if (normalizer == 1) normalize_columns(y);
+            lap(R.t_rows);
         }
     }
     DMatrix Q = thin_q(y);
+    lap(R.t_rows);
     DMatrix B;
     masked_multiply_transposed_by_dense(M, Q, B);
+    lap(R.t_sparse);
     DMatrix Ub, Vt;
     std::vector<double> sig;
     jacobi_svd(B, Ub, sig, Vt);
+    lap(R.t_fixed);
     size_t r = sig.size();
     size_t actual = std::min(target_rank, r);
-    RandResult R;
     R.d = actual; R.m = m; R.n = n;
     R.u.assign(m * actual, 0.0);
     for (size_t i = 0; i < m; ++i)
@@ -1446,6 +1464,7 @@ static RandResult randomized_svd(const MaskedOp& M, size_t target_rank, size_t n
             for (size_t j = 0; j < Q.c; ++j) acc += Q(i, j) * Ub(j, k);
             R.u[i * actual + k] = acc;
         }
+    lap(R.t_rows);
     R.s.assign(sig.begin(), sig.begin() + actual);
     R.vt.assign(actual * n, 0.0);
     for (size_t k = 0; k < actual; ++k)
@@ -1677,6 +1696,7 @@ struct orc_rand_out {
     double* u;
     double* s;
     double* vt;
+    double t_sparse, t_rows, t_fixed;
 };
 void orc_rand_free(orc_rand_out* o) {
     std::free(o->u); std::free(o->s); std::free(o->vt);
@@ -1700,6 +1720,7 @@ int orc_randomized(uint64_t nrows, uint64_t ncols, uint64_t nnz, const uint64_t*
                                                 compat_d3 != 0);
         out->d = r.d; out->m = r.m; out->n = r.n;
         out->u = dup_vec(r.u); out->s = dup_vec(r.s); out->vt = dup_vec(r.vt);
+        out->t_sparse = r.t_sparse; out->t_rows = r.t_rows; out->t_fixed = r.t_fixed;
         return 0;
     } catch (std::exception& ex) { g_orc_err = ex.what(); return orc::E_PANIC; }
 }

@@ -156,14 +156,21 @@ void transpose(const DevCompressed& in, DevCompressed& out, cudaStream_t s) {
     else transpose_impl<int64_t>(in, out, s);
 }
 
+// The FP32 copies belong to the handle that owns the arrays (the parent of an
+// all-columns masked view), so they are allocated, filled and later freed on
+// that handle's stream, which lives as long as they do.
 void ensure_fp32(const svdb_matrix* a) {
+    const svdb_matrix* owner = (a->kind == KIND_MASKED && a->all_columns) ? a->parent : a;
+    bool launched = false;
     for (const DevCompressed* c : {&csr_of(a), &csc_of(a)}) {
         DevCompressed* m = const_cast<DevCompressed*>(c);
         if (m->val32.p || m->nnz == 0) continue;
-        m->val32.alloc(m->nnz, a->stream);
-        k_to_f32<<<grid_for(m->nnz), 256, 0, a->stream>>>(m->val.p, m->val32.p, m->nnz);
+        m->val32.alloc(m->nnz, owner->stream);
+        k_to_f32<<<grid_for(m->nnz), 256, 0, owner->stream>>>(m->val.p, m->val32.p, m->nnz);
         SVDB_CHECK_LAUNCH();
+        launched = true;
     }
+    if (launched) SVDB_CUDA(cudaStreamSynchronize(owner->stream));
 }
 
 const DevCompressed& csr_of(const svdb_matrix* a) {

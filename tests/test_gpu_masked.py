@@ -62,3 +62,17 @@ def test_large_masked_compaction():
     S = M.to_scipy(A)[:, m2o]
     x = np.random.default_rng(3).standard_normal(len(m2o))
     np.testing.assert_allclose(mv.svd_opa(x), S @ x, rtol=0, atol=1e-12 * np.abs(S @ x).max())
+
+
+def test_view_then_parent_teardown_after_mixed_precision():
+    # the FP32 copy made through an all-columns view belongs to the parent and must
+    # outlive the view's stream
+    from single_svdlib import randomized
+    from single_svdlib.randomized import PowerIterationNormalizer as PIN
+    A = M.uniform(300, 100, 0.1, 61)
+    parent = csr(A)
+    mv = MaskedCSRMatrix(parent, np.ones(100, np.uint8))
+    r = randomized.randomized_svd(mv, 5, 5, 1, PIN.QR, False, 1, False, precision="mixed")
+    assert r.d == 5
+    mv.close()
+    parent.close()
