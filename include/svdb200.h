@@ -201,6 +201,19 @@ int svdb_multiply_transposed_by_dense(const svdb_matrix* a, const double* q, uin
 int svdb_multiply_with_dense_device(const svdb_matrix* a, const void* d_dense, uint64_t dense_cols, void* d_result,
                                     int transpose_self, int precision, void* stream);
 
+/* svd_opb on device buffers without allocating: d_y = A^T (A d_x), or
+ * A (A^T d_x) when transposed, enqueued on `stream` (NULL = the handle's
+ * stream).  No counterpart in the reference: it serves callers that cannot
+ * allocate device memory where they apply the operator (their own allocator
+ * holds the GPU's memory, or an allocation's synchronisation is not
+ * acceptable there).  The intermediate vector lives in a fixed 2^20-double
+ * (8 MiB) device array that every GPU loading the library keeps until exit;
+ * a larger intermediate (rows of A, or columns when transposed) returns
+ * SVDB_ERR_UNSUPPORTED.  The array's address is looked up on the first call on
+ * each device, so make that call before any stream capture.  All calls share
+ * the array: calls that overlap on the GPU race and must be serialised. */
+int svdb_opb_device_noalloc(const svdb_matrix* a, const double* d_x, double* d_y, int transposed, void* stream);
+
 /* Number of kernels this library has launched in the process so far. */
 uint64_t svdb_kernel_launches(void);
 
