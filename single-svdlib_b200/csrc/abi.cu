@@ -205,7 +205,7 @@ int svdb_multiply_with_dense(const svdb_matrix* a, const double* dense, uint64_t
         const DevCompressed& op = transpose_self ? csc_of(a) : csr_of(a);
         DevBuf<double> dx(std::max<int64_t>(op.nminor * l, 1), s), dy(std::max<int64_t>(op.nmajor * l, 1), s);
         SVDB_CUDA(cudaMemcpyAsync(dx.p, dense, op.nminor * l * 8, cudaMemcpyHostToDevice, s));
-        spmm_dev<double>(op, false, dx.p, (int)l, dy.p, s);
+        spmm_dev<double, double>(op, false, dx.p, (int)l, dy.p, s);
         SVDB_CUDA(cudaMemcpyAsync(result, dy.p, op.nmajor * l * 8, cudaMemcpyDeviceToHost, s));
         SVDB_CUDA(cudaStreamSynchronize(s));
     });
@@ -220,7 +220,7 @@ int svdb_multiply_with_dense_device(const svdb_matrix* a, const void* d_dense, u
         cudaStream_t s = stream ? (cudaStream_t)stream : a->stream;
         const DevCompressed& op = transpose_self ? csc_of(a) : csr_of(a);
         if (precision == SVDB_F64) {
-            spmm_dev<double>(op, false, (const double*)d_dense, (int)l, (double*)d_result, s);
+            spmm_dev<double, double>(op, false, (const double*)d_dense, (int)l, (double*)d_result, s);
         } else {
             if (!op.val32.p) {
                 svdb_matrix* am = const_cast<svdb_matrix*>(a);
@@ -228,7 +228,7 @@ int svdb_multiply_with_dense_device(const svdb_matrix* a, const void* d_dense, u
                 ensure_fp32(a);
                 SVDB_CUDA(cudaStreamSynchronize(a->stream));
             }
-            spmm_dev<float>(op, true, (const float*)d_dense, (int)l, (float*)d_result, s);
+            spmm_dev<float, float>(op, true, (const float*)d_dense, (int)l, (float*)d_result, s);
         }
     });
 }
@@ -247,7 +247,7 @@ int svdb_multiply_transposed_by_dense(const svdb_matrix* a, const double* q, uin
         DevBuf<double> dq(std::max<int64_t>(op.nminor * l, 1), s), dz(std::max<int64_t>(op.nmajor * l, 1), s),
             dr(std::max<int64_t>(op.nmajor * l, 1), s);
         SVDB_CUDA(cudaMemcpyAsync(dq.p, q, op.nminor * l * 8, cudaMemcpyHostToDevice, s));
-        spmm_dev<double>(op, false, dq.p, (int)l, dz.p, s);
+        spmm_dev<double, double>(op, false, dq.p, (int)l, dz.p, s);
         transpose_dense<double>(dz.p, dr.p, op.nmajor, (int64_t)l, s);
         SVDB_CUDA(cudaMemcpyAsync(result, dr.p, op.nmajor * l * 8, cudaMemcpyDeviceToHost, s));
         SVDB_CUDA(cudaStreamSynchronize(s));

@@ -173,6 +173,12 @@ void ensure_fp32(const svdb_matrix* a) {
     if (launched) SVDB_CUDA(cudaStreamSynchronize(owner->stream));
 }
 
+// SpMM load-balancing plans for both orientations (spmm.cu)
+static void build_plans(svdb_matrix* a, cudaStream_t s) {
+    build_seg_plan(a->csr, s);
+    build_seg_plan(a->csc, s);
+}
+
 const DevCompressed& csr_of(const svdb_matrix* a) {
     if (a->kind == KIND_MASKED && a->all_columns) return a->parent->csr;
     return a->csr;
@@ -232,6 +238,7 @@ svdb_matrix* create_csr(uint64_t nrows, uint64_t ncols, uint64_t nnz, const uint
         a->nrows = nrows; a->ncols = ncols; a->nnz = nnz;
         upload_compressed(a->csr, nrows, ncols, nnz, indptr, indices, values, a->stream);
         transpose(a->csr, a->csc, a->stream);
+        build_plans(a, a->stream);
         SVDB_CUDA(cudaStreamSynchronize(a->stream));
     } catch (...) {
         cudaStreamSynchronize(a->stream);
@@ -250,6 +257,7 @@ svdb_matrix* create_csc(uint64_t nrows, uint64_t ncols, uint64_t nnz, const uint
         if (nrows > INT32_MAX) throw Error(SVDB_ERR_UNSUPPORTED, "nrows above 2^31-1");
         upload_compressed(a->csc, ncols, nrows, nnz, colptr, rowidx, values, a->stream);
         transpose(a->csc, a->csr, a->stream);
+        build_plans(a, a->stream);
         SVDB_CUDA(cudaStreamSynchronize(a->stream));
     } catch (...) {
         cudaStreamSynchronize(a->stream);
@@ -312,6 +320,7 @@ svdb_matrix* create_coo(uint64_t nrows, uint64_t ncols, uint64_t nnz, const uint
             SVDB_CHECK_LAUNCH_N(3);
         }
         transpose(a->csr, a->csc, s);
+        build_plans(a, s);
         SVDB_CUDA(cudaStreamSynchronize(s));
     } catch (...) {
         cudaStreamSynchronize(a->stream);
@@ -371,6 +380,7 @@ svdb_matrix* create_csr_device(uint64_t nrows, uint64_t ncols, uint64_t nnz, con
         SVDB_CUDA(cudaStreamSynchronize(s));
         if (hbad) throw Error(SVDB_ERR_SHAPE, "invalid compressed sparse input");
         transpose(a->csr, a->csc, s);
+        build_plans(a, s);
         SVDB_CUDA(cudaStreamSynchronize(s));
     } catch (...) {
         cudaStreamSynchronize(a->stream);
@@ -492,6 +502,7 @@ svdb_matrix* masked_new(const svdb_matrix* parent, const uint8_t* hmask, uint64_
         k_mask_rowptr<<<grid_for(C.nmajor + 1), 256, 0, s>>>(P.ptr.p, pos.p, C.nmajor, C.ptr.p);
         SVDB_CHECK_LAUNCH_N(nnz ? 3 : 1);
         transpose(a->csr, a->csc, s);
+        build_plans(a, s);
         SVDB_CUDA(cudaStreamSynchronize(s));
     } catch (...) {
         cudaStreamSynchronize(a->stream);

@@ -1,4 +1,4 @@
-// Standalone device operators: SpMV / SpMM row gathers, deterministic
+// Standalone device operators: SpMV row gathers, deterministic
 // reductions, element-wise BLAS-1 (src/lanczos/mod.rs:311-424), classical
 // Gram-Schmidt GEMV pairs for startv (mod.rs:624-628), the ChaCha12 start
 // vector (mod.rs:598-605) and dense transposes.
@@ -55,75 +55,6 @@ void spmv(const DevCompressed& m, bool fp32, const double* x, double* y, cudaStr
         k_spmv<double><<<blocks, threads, 0, s>>>(m.ptr.p, m.idx.p, m.val.p, m.nmajor, G, x, y);
     SVDB_CHECK_LAUNCH();
 }
-
-// --------------------------------------------------------------- SpMM ----
-// Y (rows x l) = M X, X (minor x l) row-major.  One warp per row; lane c owns
-// columns c, c+32, ... (NT chunks of 32); the row's (index, value) pairs are
-// loaded 32 at a time and broadcast with shuffles.
-template <typename VT, typename T, int NT>
-__global__ void __launch_bounds__(256) k_spmm(const int64_t* __restrict__ rp, const int32_t* __restrict__ ci,
-                                              const VT* __restrict__ v, int64_t rows, const T* __restrict__ X,
-                                              int l, int64_t ldx, T* __restrict__ Y, int64_t ldy) {
-    const int lane = threadIdx.x & 31;
-    const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t r = gwarp; r < rows; r += nwarps) {
-        T acc[NT];
-#pragma unroll
-        for (int t = 0; t < NT; ++t) acc[t] = T(0);
-        const int64_t s = rp[r], e = rp[r + 1];
-        for (int64_t k0 = s; k0 < e; k0 += 32) {
-            const int64_t k = k0 + lane;
-            int32_t myc = 0;
-            T myv = T(0);
-            if (k < e) { myc = ci[k]; myv = (T)v[k]; }
-            const int cnt = (int)((e - k0) < 32 ? (e - k0) : 32);
-            for (int q = 0; q < cnt; ++q) {
-                const int32_t c = __shfl_sync(0xffffffffu, myc, q);
-                const T vv = __shfl_sync(0xffffffffu, myv, q);
-                const T* xr = X + (int64_t)c * ldx;
-#pragma unroll
-                for (int t = 0; t < NT; ++t) {
-                    const int col = lane + 32 * t;
-                    if (col < l) acc[t] = fma(vv, __ldg(xr + col), acc[t]);
-                }
-            }
-        }
-        T* yr = Y + r * ldy;
-#pragma unroll
-        for (int t = 0; t < NT; ++t) {
-            const int col = lane + 32 * t;
-            if (col < l) yr[col] = acc[t];
-        }
-    }
-}
-
-template <typename VT, typename T>
-static void spmm_launch(const int64_t* rp, const int32_t* ci, const VT* v, int64_t rows, const T* X, int l, T* Y,
-                        cudaStream_t s) {
-    const int threads = 256;
-    const int blocks = blocks_for(rows * 32, threads, 16);
-    // wide right-hand sides are processed 128 columns at a time through strided views
-    for (int c0 = 0; c0 < l; c0 += 128) {
-        const int lc = std::min(128, l - c0);
-        const T* Xc = X + c0;
-        T* Yc = Y + c0;
-        if (lc <= 32) k_spmm<VT, T, 1><<<blocks, threads, 0, s>>>(rp, ci, v, rows, Xc, lc, l, Yc, l);
-        else if (lc <= 64) k_spmm<VT, T, 2><<<blocks, threads, 0, s>>>(rp, ci, v, rows, Xc, lc, l, Yc, l);
-        else if (lc <= 96) k_spmm<VT, T, 3><<<blocks, threads, 0, s>>>(rp, ci, v, rows, Xc, lc, l, Yc, l);
-        else k_spmm<VT, T, 4><<<blocks, threads, 0, s>>>(rp, ci, v, rows, Xc, lc, l, Yc, l);
-        SVDB_CHECK_LAUNCH();
-    }
-}
-
-template <typename T>
-void spmm_dev(const DevCompressed& m, bool fp32, const T* X, int l, T* Y, cudaStream_t s) {
-    if (m.nmajor == 0 || l == 0) return;
-    if (fp32 && m.val32.p) spmm_launch<float, T>(m.ptr.p, m.idx.p, m.val32.p, m.nmajor, X, l, Y, s);
-    else spmm_launch<double, T>(m.ptr.p, m.idx.p, m.val.p, m.nmajor, X, l, Y, s);
-}
-template void spmm_dev<double>(const DevCompressed&, bool, const double*, int, double*, cudaStream_t);
-template void spmm_dev<float>(const DevCompressed&, bool, const float*, int, float*, cudaStream_t);
 
 // --------------------------------------------------------- reductions ----
 constexpr int kRedBlocks = 256;

@@ -12,10 +12,11 @@ namespace svdb {
 // lanes per row for a row gather with `avg` entries per row (power of two, 2..32)
 int group_for(double avg);
 
-// Y (nmajor x l) = M X with X (nminor x l), row-major; values FP32 when fp32
-// and the FP32 copy exists; accumulation in T.
-template <typename T>
-void spmm_dev(const DevCompressed& m, bool fp32, const T* X, int l, T* Y, cudaStream_t s);
+// Y (nmajor x l) = M X with X (nminor x l), row-major (spmm.cu); values FP32
+// when fp32 and the FP32 copy exists; accumulation in FP64.
+// Instantiated for (double, double), (float, float) and (float, double).
+template <typename XT, typename OT>
+void spmm_dev(const DevCompressed& m, bool fp32, const XT* X, int l, OT* Y, cudaStream_t s);
 
 void datx(double a, const double* x, double* y, int64_t n, cudaStream_t s);  // y = a * x
 

@@ -11,9 +11,9 @@
 // one-sided Jacobi SVD of the small R in one block, so that
 // B = V_R S (Q_b U_R)^T, singular values in descending order.
 //
-// SVDB_MIXED runs the sparse products in FP32 (values, dense operands and
-// accumulation); the Gram products, Cholesky and the second CholeskyQR pass
-// stay FP64.
+// SVDB_MIXED runs the sparse products on FP32 matrix values and an FP32 copy
+// of the dense operand (half the gathered bytes) with FP64 sums; the Gram
+// products, Cholesky, both CholeskyQR passes and the small SVD stay FP64.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -286,11 +286,6 @@ __global__ void __launch_bounds__(1024) k_jacobi_svd(const double* __restrict__ 
     }
 }
 
-template <typename T>
-__global__ void k_convert(const T* __restrict__ in, double* __restrict__ out, int64_t n) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        out[i] = (double)in[i];
-}
 __global__ void k_to_float(const double* __restrict__ in, float* __restrict__ out, int64_t n) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         out[i] = (float)in[i];
@@ -453,22 +448,21 @@ void randomized(const svdb_matrix* A, uint64_t target_rank, uint64_t n_oversampl
     else k_omega<double><<<nb(n * l, 256), 256, 0, s>>>(has_seed ? seed : 0, n * l, Om.p);
     SVDB_CHECK_LAUNCH();
 
-    // Sparse products: FP64 operands, or FP32 copies under SVDB_MIXED.
-    DevBuf<float> f_in, f_out;
+    // Sparse products: FP64 operands, or under SVDB_MIXED FP32 values and an
+    // FP32 copy of the dense operand (half the gathered bytes), FP64 sums and output.
+    DevBuf<float> f_in;
     auto spmm = [&](const DevCompressed& M, const double* X, int c, double* Y) {
         cudaEvent_t a, b;
         SVDB_CUDA(cudaEventCreate(&a));
         SVDB_CUDA(cudaEventCreate(&b));
         SVDB_CUDA(cudaEventRecord(a, s));
         if (!mixed) {
-            spmm_dev<double>(M, false, X, c, Y, s);
+            spmm_dev<double, double>(M, false, X, c, Y, s);
         } else {
             if ((int64_t)f_in.n < M.nminor * c) f_in.alloc(M.nminor * c, s);
-            if ((int64_t)f_out.n < M.nmajor * c) f_out.alloc(M.nmajor * c, s);
             k_to_float<<<nb(M.nminor * c, 256), 256, 0, s>>>(X, f_in.p, M.nminor * c);
-            spmm_dev<float>(M, true, f_in.p, c, f_out.p, s);
-            k_convert<float><<<nb(M.nmajor * c, 256), 256, 0, s>>>(f_out.p, Y, M.nmajor * c);
-            SVDB_CHECK_LAUNCH_N(2);
+            SVDB_CHECK_LAUNCH();
+            spmm_dev<float, double>(M, true, f_in.p, c, Y, s);
         }
         SVDB_CUDA(cudaEventRecord(b, s));
         SVDB_CUDA(cudaEventSynchronize(b));

@@ -159,8 +159,8 @@ void sigma_and_u(const DevCompressed& op1, const DevCompressed& op2, bool fp32, 
     if (d == 0) return;
     DevBuf<double> V(n * d, s), Y(m * d, s), T(n * d, s), t(d, s), scale(d, s);
     transpose_dense<double>(Vt, V.p, d, n, s);       // V (n x d)
-    spmm_dev<double>(op1, fp32, V.p, (int)d, Y.p, s);  // Y = A v   (m x d)
-    spmm_dev<double>(op2, fp32, Y.p, (int)d, T.p, s);  // T = A^T A v (n x d)
+    spmm_dev<double, double>(op1, fp32, V.p, (int)d, Y.p, s);  // Y = A v   (m x d)
+    spmm_dev<double, double>(op2, fp32, Y.p, (int)d, T.p, s);  // T = A^T A v (n x d)
     k_col_dots<<<(unsigned)d, 256, 0, s>>>(Vt, T.p, n, d, t.p);
     k_sigma<<<(unsigned)((d + 127) / 128), 128, 0, s>>>(t.p, d, legacy, eps_a, S, scale.p);
     transpose_dense<double>(Y.p, Ut, m, d, s);       // Ut (d x m)

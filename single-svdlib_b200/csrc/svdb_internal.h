@@ -76,14 +76,32 @@ struct DevBuf {
 // A compressed sparse structure in HBM: `nmajor` rows of a CSR (or columns of
 // a CSC, i.e. rows of the transpose).  Column indices are int32 (minor
 // dimension < 2^31), offsets int64.
+// Load-balancing plan for the row gathers of SpMM: every row is cut into
+// segments of at most kSegNnz entries; seg_first[r] .. seg_first[r+1] are the
+// segments of row r; segment s covers entries [seg_beg[s], seg_end[s]) of row
+// seg_row[s], stored as -(row + 1) when the row has several segments; those
+// rows are listed in multi_rows and merged by a second, ordered pass.
+constexpr int64_t kSegNnz = 2048;
+struct SegPlan {
+    int64_t nseg = 0, nmulti = 0;
+    DevBuf<int64_t> seg_first;
+    DevBuf<int32_t> seg_row;
+    DevBuf<int64_t> seg_beg, seg_end;
+    DevBuf<int32_t> multi_rows;
+};
+
 struct DevCompressed {
     int64_t nmajor = 0, nminor = 0, nnz = 0;
     DevBuf<int64_t> ptr;
     DevBuf<int32_t> idx;
     DevBuf<double> val;
     DevBuf<float> val32;  // FP32 copy of val, made on first mixed-precision use
+    SegPlan plan;         // built when the handle is created
     double avg_per_major() const { return nmajor ? double(nnz) / double(nmajor) : 0.0; }
 };
+
+// Builds m.plan on stream s (called once per structure, at creation).
+void build_seg_plan(DevCompressed& m, cudaStream_t s);
 
 enum MatKind { KIND_CSR = 0, KIND_CSC = 1, KIND_COO = 2, KIND_MASKED = 3 };
 
