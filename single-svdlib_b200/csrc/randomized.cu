@@ -58,11 +58,14 @@ __global__ void k_omega(uint64_t seed, int64_t total, T* __restrict__ out) {
 // (staged through shared memory); a 16 x 16 thread grid holds an NC x NC
 // register tile of G per thread (entries (ty + 16 i, tx + 16 j)).  G[a][b]
 // and G[b][a] see the same products in the same order, so G is exactly
-// symmetric.  Block partials are reduced in block order.
+// symmetric.  Block partials are reduced in block order.  Every kernel of a
+// CholeskyQR pass takes `cond`: when it points to 0 the kernel returns at
+// once (the conditional third pass of shifted CholeskyQR).
 constexpr int kGramRows = 32;
 template <typename T, int NC>
 __global__ void __launch_bounds__(256) k_gram_part(const T* __restrict__ X, int64_t rows, int c, int64_t chunk,
-                                                   double* __restrict__ part) {
+                                                   double* __restrict__ part, const int* __restrict__ cond) {
+    if (cond && *cond == 0) return;
     extern __shared__ double xs[];  // kGramRows x c
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     const int64_t r0 = blockIdx.x * chunk, r1 = std::min<int64_t>(rows, r0 + chunk);
@@ -99,62 +102,109 @@ __global__ void __launch_bounds__(256) k_gram_part(const T* __restrict__ X, int6
             if (a < c && b < c) out[a * c + b] = acc[i][j];
         }
 }
-__global__ void k_gram_reduce(const double* __restrict__ part, int nblocks, int c, double shift,
-                              double* __restrict__ G) {
+// G[p] = sum over blocks of part[b][p]: four interleaved partial sums, fixed order
+__global__ void k_gram_reduce(const double* __restrict__ part, int nblocks, int c, double* __restrict__ G,
+                              const int* __restrict__ cond) {
+    if (cond && *cond == 0) return;
     const int cc = c * c;
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < cc; p += gridDim.x * blockDim.x) {
-        double s = 0.0;
-        for (int b = 0; b < nblocks; ++b) s += part[(int64_t)b * cc + p];
-        if (p / c == p % c) s += shift;
-        G[p] = s;
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        int b = 0;
+        for (; b + 4 <= nblocks; b += 4) {
+            s0 += part[(int64_t)b * cc + p];
+            s1 += part[(int64_t)(b + 1) * cc + p];
+            s2 += part[(int64_t)(b + 2) * cc + p];
+            s3 += part[(int64_t)(b + 3) * cc + p];
+        }
+        for (; b < nblocks; ++b) s0 += part[(int64_t)b * cc + p];
+        G[p] = (s0 + s1) + (s2 + s3);
     }
 }
 
 // ------------------------------------------------------ small dense ops ----
-// In-place upper Cholesky G = R^T R in one block; R overwrites the upper
-// triangle (lower set to 0).  status = 1 on a non-positive pivot.
-__global__ void k_cholesky(double* __restrict__ G, int c, int* __restrict__ status) {
-    __shared__ double piv;
-    for (int k = 0; k < c; ++k) {
-        if (threadIdx.x == 0) {
-            double d = G[k * c + k];
-            piv = (d > 0.0 && isfinite(d)) ? sqrt(d) : -1.0;
-            if (piv < 0.0) *status = 1;
-            else G[k * c + k] = piv;
+// One block: G = R^T R (upper R) in shared memory, then R^-1.  A non-positive
+// pivot restarts the factorisation on G + shift I with shift =
+// shift_scale * trace(G) (shifted CholeskyQR); that sets bit 1 of *flags and
+// *shifted (which enables the third pass).  A second breakdown sets bit 2 and
+// leaves R = R^-1 = I.  R and R^-1 are written to global memory.
+__global__ void __launch_bounds__(1024) k_chol_inv(const double* __restrict__ G, int c, double shift_scale,
+                                                   double* __restrict__ R, double* __restrict__ Ri,
+                                                   int* __restrict__ flags, int* __restrict__ shifted,
+                                                   const int* __restrict__ cond, int ri_in_smem) {
+    if (cond && *cond == 0) return;
+    extern __shared__ double sm[];  // R work (c*c) | R^-1 (c*c) when ri_in_smem
+    __shared__ int s_fail;
+    __shared__ double s_shift;
+    const int cc = c * c;
+    double* ri = ri_in_smem ? sm + cc : Ri;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        for (int t = threadIdx.x; t < cc; t += blockDim.x)
+            sm[t] = G[t] + ((attempt == 1 && t / c == t % c) ? s_shift : 0.0);
+        if (threadIdx.x == 0) s_fail = 0;
+        __syncthreads();
+        for (int k = 0; k < c; ++k) {
+            if (threadIdx.x == 0) {
+                const double d = sm[k * c + k];
+                if (d > 0.0 && isfinite(d)) sm[k * c + k] = sqrt(d);
+                else s_fail = 1;
+            }
+            __syncthreads();
+            if (s_fail) break;
+            const double piv = sm[k * c + k];
+            for (int j = k + 1 + threadIdx.x; j < c; j += blockDim.x) sm[k * c + j] /= piv;
+            __syncthreads();
+            const int rem = c - k - 1;
+            for (int t = threadIdx.x; t < rem * rem; t += blockDim.x) {
+                const int i = k + 1 + t / rem, j = k + 1 + t % rem;
+                if (i <= j) sm[i * c + j] -= sm[k * c + i] * sm[k * c + j];
+            }
+            __syncthreads();
         }
-        __syncthreads();
-        if (piv < 0.0) return;
-        for (int j = k + 1 + threadIdx.x; j < c; j += blockDim.x) G[k * c + j] /= piv;
-        __syncthreads();
-        // trailing update of the upper triangle: G[i][j] -= R[k][i] R[k][j], i <= j
-        const int rem = c - k - 1;
-        for (int t = threadIdx.x; t < rem * rem; t += blockDim.x) {
-            const int i = k + 1 + t / rem, j = k + 1 + t % rem;
-            if (i <= j) G[i * c + j] -= G[k * c + i] * G[k * c + j];
+        if (!s_fail) break;
+        if (attempt == 0) {
+            if (threadIdx.x == 0) {
+                double tr = 0.0;
+                for (int i = 0; i < c; ++i) tr += G[i * c + i];
+                s_shift = shift_scale * tr > 0.0 ? shift_scale * tr : 1e-300;
+                atomicOr(flags, 1);
+                *shifted = 1;
+            }
+            __syncthreads();
         }
-        __syncthreads();
     }
-    for (int t = threadIdx.x; t < c * c; t += blockDim.x)
-        if (t / c > t % c) G[t] = 0.0;
-}
-
-// Rinv (upper) = R^-1, one block, column by column (back substitution).
-__global__ void k_tri_inv(const double* __restrict__ R, int c, double* __restrict__ Ri) {
-    for (int t = threadIdx.x; t < c * c; t += blockDim.x) Ri[t] = 0.0;
+    if (s_fail) {
+        if (threadIdx.x == 0) atomicOr(flags, 2);
+        for (int t = threadIdx.x; t < cc; t += blockDim.x) {
+            const double v = (t / c == t % c) ? 1.0 : 0.0;
+            R[t] = v;
+            Ri[t] = v;
+        }
+        return;
+    }
+    for (int t = threadIdx.x; t < cc; t += blockDim.x) {
+        if (t / c > t % c) sm[t] = 0.0;
+        ri[t] = 0.0;
+    }
     __syncthreads();
-    // solve R x = e_j for each column j (independent: one thread per column)
+    for (int t = threadIdx.x; t < cc; t += blockDim.x) R[t] = sm[t];
+    // R^-1 column j by back substitution (one thread per column)
     for (int j = threadIdx.x; j < c; j += blockDim.x) {
         for (int i = j; i >= 0; --i) {
             double s = (i == j) ? 1.0 : 0.0;
-            for (int k = i + 1; k <= j; ++k) s -= R[i * c + k] * Ri[k * c + j];
-            Ri[i * c + j] = s / R[i * c + i];
+            for (int k = i + 1; k <= j; ++k) s -= sm[i * c + k] * ri[k * c + j];
+            ri[i * c + j] = s / sm[i * c + i];
         }
+    }
+    if (ri_in_smem) {
+        __syncthreads();
+        for (int t = threadIdx.x; t < cc; t += blockDim.x) Ri[t] = ri[t];
     }
 }
 
 // C (c x c) = A (c x c) B (c x c), one block
 __global__ void k_small_gemm(const double* __restrict__ A, const double* __restrict__ B, int c,
-                             double* __restrict__ C) {
+                             double* __restrict__ C, const int* __restrict__ cond) {
+    if (cond && *cond == 0) return;
     for (int t = threadIdx.x; t < c * c; t += blockDim.x) {
         const int i = t / c, j = t % c;
         double s = 0.0;
@@ -163,26 +213,40 @@ __global__ void k_small_gemm(const double* __restrict__ A, const double* __restr
     }
 }
 
-// Out (rows x cout) = X (rows x c) S (c x ldS, first cout columns); S in shared memory tiles.
+// Out (rows x cout) = X (rows x c) S (c x lds, first cout columns).  S and a
+// 32-row tile of X are staged in shared memory.
+constexpr int kRmRows = 32;
 template <typename TI, typename TO>
 __global__ void __launch_bounds__(256) k_right_mul(const TI* __restrict__ X, int64_t rows, int c,
                                                    const double* __restrict__ S, int lds, int cout,
-                                                   TO* __restrict__ Out) {
-    extern __shared__ double ss[];  // c x cout
+                                                   TO* __restrict__ Out, const int* __restrict__ cond) {
+    if (cond && *cond == 0) return;
+    extern __shared__ double sm[];  // S: c*cout | X tile: kRmRows*c
+    double* ss = sm;
+    double* xs = sm + c * cout;
     for (int t = threadIdx.x; t < c * cout; t += blockDim.x) ss[t] = S[(t / cout) * lds + t % cout];
-    __syncthreads();
-    const int64_t total = rows * cout;
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t r = t / cout;
-        const int j = (int)(t % cout);
-        const TI* xr = X + r * c;
-        double s = 0.0;
-        for (int k = 0; k < c; ++k) s = fma((double)xr[k], ss[k * cout + j], s);
-        Out[t] = (TO)s;
+    for (int64_t r0 = (int64_t)blockIdx.x * kRmRows; r0 < rows; r0 += (int64_t)gridDim.x * kRmRows) {
+        const int nr = (int)std::min<int64_t>(kRmRows, rows - r0);
+        __syncthreads();
+        for (int t = threadIdx.x; t < nr * c; t += blockDim.x) xs[t] = (double)X[r0 * c + t];
+        __syncthreads();
+        for (int t = threadIdx.x; t < nr * cout; t += blockDim.x) {
+            const int rr = t / cout, j = t % cout;
+            const double* xr = xs + rr * c;
+            double s = 0.0;
+            for (int k = 0; k < c; ++k) s = fma(xr[k], ss[k * cout + j], s);
+            Out[(r0 + rr) * cout + j] = (TO)s;
+        }
     }
 }
 
-// normalize_columns (mod.rs:239-293): scale columns with norm > 1e-10
+__global__ void k_copy_cond(const double* __restrict__ src, double* __restrict__ dst, int64_t n,
+                            const int* __restrict__ cond) {
+    if (cond && *cond == 0) return;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        dst[i] = src[i];
+}
+
 template <typename T>
 __global__ void k_colnorm(T* __restrict__ X, int64_t rows, int c) {
     __shared__ double sh[32];
@@ -300,12 +364,13 @@ __global__ void k_take_cols(const double* __restrict__ X, int64_t rows, int c, i
 // ------------------------------------------------------ host helpers ----
 struct RandCtx {
     cudaStream_t s;
-    DevBuf<double> part, G, Rinv, R1, R2, Rtmp;
-    DevBuf<int> status;
+    int cmax = 0;
+    DevBuf<double> part, G, R1, R2, R3, Ri, Rtmp, T;
+    DevBuf<int> flags, shifted;
     int64_t part_cap = 0;
 };
 
-static void gram(RandCtx& cx, const double* X, int64_t rows, int c, double shift, double* G) {
+static void gram(RandCtx& cx, const double* X, int64_t rows, int c, double* G, const int* cond) {
     if (c > 128) throw Error(SVDB_ERR_UNSUPPORTED, "randomized_svd: more than 128 sample columns");
     const int sms = device_props().sms;
     int64_t chunk = std::max<int64_t>(kGramRows * 4, (rows + sms * 2 - 1) / (sms * 2));
@@ -317,78 +382,73 @@ static void gram(RandCtx& cx, const double* X, int64_t rows, int c, double shift
     const size_t smem = kGramRows * c * sizeof(double);
     const int nc = (c + 15) / 16;
     switch (nc) {
-        case 1: k_gram_part<double, 1><<<nblk, 256, smem, cx.s>>>(X, rows, c, chunk, cx.part.p); break;
-        case 2: k_gram_part<double, 2><<<nblk, 256, smem, cx.s>>>(X, rows, c, chunk, cx.part.p); break;
-        case 3: k_gram_part<double, 3><<<nblk, 256, smem, cx.s>>>(X, rows, c, chunk, cx.part.p); break;
-        case 4: k_gram_part<double, 4><<<nblk, 256, smem, cx.s>>>(X, rows, c, chunk, cx.part.p); break;
-        case 5: k_gram_part<double, 5><<<nblk, 256, smem, cx.s>>>(X, rows, c, chunk, cx.part.p); break;
-        case 6: k_gram_part<double, 6><<<nblk, 256, smem, cx.s>>>(X, rows, c, chunk, cx.part.p); break;
-        case 7: k_gram_part<double, 7><<<nblk, 256, smem, cx.s>>>(X, rows, c, chunk, cx.part.p); break;
-        default: k_gram_part<double, 8><<<nblk, 256, smem, cx.s>>>(X, rows, c, chunk, cx.part.p); break;
+        case 1: k_gram_part<double, 1><<<nblk, 256, smem, cx.s>>>(X, rows, c, chunk, cx.part.p, cond); break;
+        case 2: k_gram_part<double, 2><<<nblk, 256, smem, cx.s>>>(X, rows, c, chunk, cx.part.p, cond); break;
+        case 3: k_gram_part<double, 3><<<nblk, 256, smem, cx.s>>>(X, rows, c, chunk, cx.part.p, cond); break;
+        case 4: k_gram_part<double, 4><<<nblk, 256, smem, cx.s>>>(X, rows, c, chunk, cx.part.p, cond); break;
+        case 5: k_gram_part<double, 5><<<nblk, 256, smem, cx.s>>>(X, rows, c, chunk, cx.part.p, cond); break;
+        case 6: k_gram_part<double, 6><<<nblk, 256, smem, cx.s>>>(X, rows, c, chunk, cx.part.p, cond); break;
+        case 7: k_gram_part<double, 7><<<nblk, 256, smem, cx.s>>>(X, rows, c, chunk, cx.part.p, cond); break;
+        default: k_gram_part<double, 8><<<nblk, 256, smem, cx.s>>>(X, rows, c, chunk, cx.part.p, cond); break;
     }
-    k_gram_reduce<<<nb((int64_t)c * c, 128), 128, 0, cx.s>>>(cx.part.p, nblk, c, shift, G);
+    k_gram_reduce<<<nb((int64_t)c * c, 128), 128, 0, cx.s>>>(cx.part.p, nblk, c, G, cond);
     SVDB_CHECK_LAUNCH_N(2);
 }
 
 static void right_mul(const double* X, int64_t rows, int c, const double* S, int lds, int cout, double* Out,
-                      cudaStream_t s) {
-    size_t smem = (size_t)c * cout * sizeof(double);
+                      cudaStream_t s, const int* cond = nullptr) {
+    const size_t smem = ((size_t)c * cout + (size_t)kRmRows * c) * sizeof(double);
     if (smem > 200 * 1024) throw Error(SVDB_ERR_UNSUPPORTED, "dense factor wider than the shared-memory tile");
     if (smem > 48 * 1024)
         SVDB_CUDA(cudaFuncSetAttribute(k_right_mul<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem));
-    k_right_mul<double, double><<<nb(rows * cout, 256), 256, smem, s>>>(X, rows, c, S, lds, cout, Out);
+    const int blocks = (int)std::max<int64_t>(
+        1, std::min<int64_t>((rows + kRmRows - 1) / kRmRows, (int64_t)device_props().sms * 4));
+    k_right_mul<double, double><<<blocks, 256, smem, s>>>(X, rows, c, S, lds, cout, Out, cond);
     SVDB_CHECK_LAUNCH();
 }
 
-// One CholeskyQR pass on X (rows x c) in place; R (c x c) returned. false on breakdown.
-static bool cqr_pass(RandCtx& cx, double* X, double* Xtmp, int64_t rows, int c, double shift, double* R) {
-    gram(cx, X, rows, c, shift, R);
-    SVDB_CUDA(cudaMemsetAsync(cx.status.p, 0, sizeof(int), cx.s));
-    k_cholesky<<<1, 256, 0, cx.s>>>(R, c, cx.status.p);
+static void chol_inv(RandCtx& cx, const double* G, int c, int64_t rows, double* R, const int* cond) {
+    const bool two = 2 * (size_t)c * c * sizeof(double) <= 200 * 1024;
+    const size_t smem = (two ? 2 : 1) * (size_t)c * c * sizeof(double);
+    if (smem > 48 * 1024)
+        SVDB_CUDA(cudaFuncSetAttribute(k_chol_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // shifted CholeskyQR: shift = 11 (rows c + c (c + 1)) u ||X||_F^2, ||X||_F^2 = trace(G)
+    const double shift_scale = 11.0 * ((double)rows * c + (double)c * (c + 1)) * 1.1102230246251565e-16;
+    k_chol_inv<<<1, 1024, smem, cx.s>>>(G, c, shift_scale, R, cx.Ri.p, cx.flags.p, cx.shifted.p, cond, two);
     SVDB_CHECK_LAUNCH();
-    int st = 0;
-    SVDB_CUDA(cudaMemcpyAsync(&st, cx.status.p, sizeof(int), cudaMemcpyDeviceToHost, cx.s));
-    SVDB_CUDA(cudaStreamSynchronize(cx.s));
-    if (st) return false;
-    k_tri_inv<<<1, 128, 0, cx.s>>>(R, c, cx.Rinv.p);
-    SVDB_CHECK_LAUNCH();
-    right_mul(X, rows, c, cx.Rinv.p, c, c, Xtmp, cx.s);
-    SVDB_CUDA(cudaMemcpyAsync(X, Xtmp, rows * c * sizeof(double), cudaMemcpyDeviceToDevice, cx.s));
-    return true;
 }
 
-// Thin Q of X (rows x c, rows >= c) in place, R (c x c) = R_last ... R_first.
+// Thin Q of X (rows x c, rows >= c) in place; Rout (c x c) = R_last ... R_first
+// when requested.  CholeskyQR2; a pass whose Cholesky broke down is redone with
+// a shift and a third pass follows.  Nothing here waits for the device: the
+// third pass's kernels read the device flag and return when it is 0.
 static void cholesky_qr(RandCtx& cx, double* X, int64_t rows, int c, double* Rout) {
-    DevBuf<double> Xtmp(rows * c, cx.s);
-    bool ok1 = cqr_pass(cx, X, Xtmp.p, rows, c, 0.0, cx.R1.p);
-    if (!ok1) {
-        // shifted CholeskyQR: shift = 11 (rows c + c(c+1)) u ||X||_F^2
-        gram(cx, X, rows, c, 0.0, cx.G.p);
-        std::vector<double> g((size_t)c * c);
-        SVDB_CUDA(cudaMemcpyAsync(g.data(), cx.G.p, g.size() * 8, cudaMemcpyDeviceToHost, cx.s));
-        SVDB_CUDA(cudaStreamSynchronize(cx.s));
-        double fro2 = 0.0;
-        for (int i = 0; i < c; ++i) fro2 += g[(size_t)i * c + i];
-        double shift = 11.0 * ((double)rows * c + (double)c * (c + 1)) * 1.1102230246251565e-16 * fro2;
-        if (!(shift > 0.0)) shift = 1e-300;
-        if (!cqr_pass(cx, X, Xtmp.p, rows, c, shift, cx.R1.p))
-            throw Error(SVDB_ERR_LAS2, "randomized_svd: shifted CholeskyQR broke down");
+    cudaStream_t s = cx.s;
+    if ((int64_t)cx.T.n < rows * c) cx.T.alloc(rows * c, s);
+    double* T = cx.T.p;
+    SVDB_CUDA(cudaMemsetAsync(cx.shifted.p, 0, sizeof(int), s));
+    // pass 1: X -> T
+    gram(cx, X, rows, c, cx.G.p, nullptr);
+    chol_inv(cx, cx.G.p, c, rows, cx.R1.p, nullptr);
+    right_mul(X, rows, c, cx.Ri.p, c, c, T, s);
+    // pass 2: T -> X
+    gram(cx, T, rows, c, cx.G.p, nullptr);
+    chol_inv(cx, cx.G.p, c, rows, cx.R2.p, nullptr);
+    right_mul(T, rows, c, cx.Ri.p, c, c, X, s);
+    // pass 3 only after a shifted pass: X -> T -> X
+    const int* cond = cx.shifted.p;
+    gram(cx, X, rows, c, cx.G.p, cond);
+    chol_inv(cx, cx.G.p, c, rows, cx.R3.p, cond);
+    right_mul(X, rows, c, cx.Ri.p, c, c, T, s, cond);
+    k_copy_cond<<<nb(rows * c, 256), 256, 0, s>>>(T, X, rows * c, cond);
+    SVDB_CHECK_LAUNCH();
+    if (Rout) {
+        k_small_gemm<<<1, 256, 0, s>>>(cx.R2.p, cx.R1.p, c, Rout, nullptr);
+        k_small_gemm<<<1, 256, 0, s>>>(cx.R3.p, Rout, c, cx.Rtmp.p, cond);
+        k_copy_cond<<<1, 256, 0, s>>>(cx.Rtmp.p, Rout, (int64_t)c * c, cond);
+        SVDB_CHECK_LAUNCH_N(3);
     }
-    if (!cqr_pass(cx, X, Xtmp.p, rows, c, 0.0, cx.R2.p)) {
-        if (!cqr_pass(cx, X, Xtmp.p, rows, c, 1e-14, cx.R2.p))
-            throw Error(SVDB_ERR_LAS2, "randomized_svd: CholeskyQR broke down");
-    }
-    // a third pass after a shifted first one restores orthogonality
-    if (!ok1) {
-        k_small_gemm<<<1, 256, 0, cx.s>>>(cx.R2.p, cx.R1.p, c, cx.Rtmp.p);
-        SVDB_CHECK_LAUNCH();
-        SVDB_CUDA(cudaMemcpyAsync(cx.R1.p, cx.Rtmp.p, (size_t)c * c * 8, cudaMemcpyDeviceToDevice, cx.s));
-        if (!cqr_pass(cx, X, Xtmp.p, rows, c, 0.0, cx.R2.p))
-            throw Error(SVDB_ERR_LAS2, "randomized_svd: CholeskyQR broke down");
-    }
-    if (Rout) k_small_gemm<<<1, 256, 0, cx.s>>>(cx.R2.p, cx.R1.p, c, Rout);
-    SVDB_CHECK_LAUNCH_N(Rout ? 1 : 0);
 }
 
 // qr(X).q() for X (rows x c): returns the column count of Q; X is replaced by
@@ -435,12 +495,12 @@ void randomized(const svdb_matrix* A, uint64_t target_rank, uint64_t n_oversampl
     RandCtx cx;
     cx.s = s;
     const int cmax = l;
-    cx.G.alloc((size_t)cmax * cmax, s);
-    cx.Rinv.alloc((size_t)cmax * cmax, s);
-    cx.R1.alloc((size_t)cmax * cmax, s);
-    cx.R2.alloc((size_t)cmax * cmax, s);
-    cx.Rtmp.alloc((size_t)cmax * cmax, s);
-    cx.status.alloc(1, s);
+    for (DevBuf<double>* b : {&cx.G, &cx.R1, &cx.R2, &cx.R3, &cx.Ri, &cx.Rtmp}) b->alloc((size_t)cmax * cmax, s);
+    cx.flags.alloc(1, s);
+    cx.shifted.alloc(1, s);
+    DevBuf<int> jac_status(1, s);
+    SVDB_CUDA(cudaMemsetAsync(cx.flags.p, 0, sizeof(int), s));
+    SVDB_CUDA(cudaMemsetAsync(jac_status.p, 0, sizeof(int), s));
 
     // Omega (n x l)
     DevBuf<double> Om(std::max<int64_t>(n * l, 1), s);
@@ -451,6 +511,7 @@ void randomized(const svdb_matrix* A, uint64_t target_rank, uint64_t n_oversampl
     // Sparse products: FP64 operands, or under SVDB_MIXED FP32 values and an
     // FP32 copy of the dense operand (half the gathered bytes), FP64 sums and output.
     DevBuf<float> f_in;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> spmm_events;  // read once, at the end
     auto spmm = [&](const DevCompressed& M, const double* X, int c, double* Y) {
         cudaEvent_t a, b;
         SVDB_CUDA(cudaEventCreate(&a));
@@ -465,12 +526,7 @@ void randomized(const svdb_matrix* A, uint64_t target_rank, uint64_t n_oversampl
             spmm_dev<float, double>(M, true, f_in.p, c, Y, s);
         }
         SVDB_CUDA(cudaEventRecord(b, s));
-        SVDB_CUDA(cudaEventSynchronize(b));
-        float t = 0.f;
-        cudaEventElapsedTime(&t, a, b);
-        spmm_ms += t;
-        cudaEventDestroy(a);
-        cudaEventDestroy(b);
+        spmm_events.emplace_back(a, b);
     };
     auto normalize = [&](DevBuf<double>& X, int64_t rows, int c) -> int {
         if (normalizer == SVDB_NORM_QR) return thin_q(cx, X, rows, c);
@@ -513,14 +569,13 @@ void randomized(const svdb_matrix* A, uint64_t target_rank, uint64_t n_oversampl
     DevBuf<double> UB((size_t)c * r, s), sig(r, s), VtB((size_t)r * n, s);
     {
         DevBuf<double> Ur((size_t)r * r, s), Vr((size_t)r * r, s), R((size_t)r * r, s);
-        SVDB_CUDA(cudaMemsetAsync(cx.status.p, 0, sizeof(int), s));
         const size_t smem = ((size_t)r * (r + 1) + (size_t)(r + 1) * (r + 1) + (r + 1)) * sizeof(double);
         if (smem > 220 * 1024) throw Error(SVDB_ERR_UNSUPPORTED, "randomized_svd: sample width above the Jacobi tile");
         SVDB_CUDA(cudaFuncSetAttribute(k_jacobi_svd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         if (n >= c) {
             // B^T = Q_b R;  R = U_J S V_J^T  ->  B = V_J S (Q_b U_J)^T
             cholesky_qr(cx, Bt.p, n, c, R.p);
-            k_jacobi_svd<<<1, 1024, smem, s>>>(R.p, r, Ur.p, Vr.p, sig.p, cx.status.p);
+            k_jacobi_svd<<<1, 1024, smem, s>>>(R.p, r, Ur.p, Vr.p, sig.p, jac_status.p);
             // U_B = V_J (c x r); V_B = Q_b U_J (n x r)
             SVDB_CUDA(cudaMemcpyAsync(UB.p, Vr.p, (size_t)r * r * 8, cudaMemcpyDeviceToDevice, s));
             DevBuf<double> VB((size_t)n * r, s);
@@ -531,7 +586,7 @@ void randomized(const svdb_matrix* A, uint64_t target_rank, uint64_t n_oversampl
             DevBuf<double> B((size_t)c * n, s);
             transpose_dense<double>(Bt.p, B.p, n, c, s);
             cholesky_qr(cx, B.p, c, (int)n, R.p);
-            k_jacobi_svd<<<1, 1024, smem, s>>>(R.p, r, Ur.p, Vr.p, sig.p, cx.status.p);
+            k_jacobi_svd<<<1, 1024, smem, s>>>(R.p, r, Ur.p, Vr.p, sig.p, jac_status.p);
             right_mul(B.p, c, (int)n, Ur.p, r, r, UB.p, s);
             transpose_dense<double>(Vr.p, VtB.p, r, r, s);
         }
@@ -548,11 +603,21 @@ void randomized(const svdb_matrix* A, uint64_t target_rank, uint64_t n_oversampl
         SVDB_CUDA(cudaMemcpyAsync(S.p, sig.p, actual * 8, cudaMemcpyDeviceToDevice, s));
     }
     SVDB_CUDA(cudaEventRecord(e1, s));
+    int hflags = 0;
+    SVDB_CUDA(cudaMemcpyAsync(&hflags, cx.flags.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     SVDB_CUDA(cudaStreamSynchronize(s));
     float tot = 0.f;
     cudaEventElapsedTime(&tot, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    for (auto& ev : spmm_events) {
+        float t = 0.f;
+        cudaEventElapsedTime(&t, ev.first, ev.second);
+        spmm_ms += t;
+        cudaEventDestroy(ev.first);
+        cudaEventDestroy(ev.second);
+    }
+    if (hflags & 2) throw Error(SVDB_ERR_LAS2, "randomized_svd: CholeskyQR broke down even with a shift");
 
     std::memset(rec, 0, sizeof(*rec));
     rec->d = actual;

@@ -88,3 +88,16 @@ def test_small_wide_and_rank_edge_cases():
     np.testing.assert_allclose(got.s, truth, rtol=1e-8)
     with pytest.raises(UnsupportedError):
         randomized.randomized_svd(upload("csr", A), 3, 2, 1, PIN.QR, True, 3, False)
+
+
+def test_rank_deficient_input_takes_the_shifted_qr():
+    # rank 5 < l = 15: the Gram of Y is singular, so CholeskyQR needs its shift;
+    # the leading singular values must still be exact and the rest ~0
+    rng = np.random.default_rng(71)
+    Mx = (rng.standard_normal((200, 5)) * np.geomspace(10, 1, 5)) @ rng.standard_normal((5, 80))
+    A = M.dense(Mx)
+    got = randomized.randomized_svd(upload("csr", A), 10, 5, 2, PIN.QR, False, 5, False)
+    truth = np.linalg.svd(Mx, compute_uv=False)
+    np.testing.assert_allclose(got.s[:5], truth[:5], rtol=1e-9)
+    assert np.all(np.abs(got.s[5:]) < 1e-8 * truth[0])
+    assert np.all(np.isfinite(got.u)) and np.all(np.isfinite(got.vt))
