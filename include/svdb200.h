@@ -40,7 +40,8 @@ typedef enum svdb_status {
     SVDB_ERR_TIMEOUT = 8,     /* a device-side wait hit its iteration limit */
     SVDB_ERR_UNSUPPORTED = 9, /* the crate has todo!() here, or an option not provided */
     SVDB_ERR_ARG = 10,        /* null pointer, bad enum value */
-    SVDB_ERR_OOM = 11         /* device allocation failed */
+    SVDB_ERR_OOM = 11,        /* device allocation failed */
+    SVDB_ERR_NOCONV = 12      /* an iterative solve stopped above its tolerance */
 } svdb_status;
 
 /* Arithmetic of the sparse products.  SVDB_F64 is the drop-in (the crate's
@@ -254,6 +255,65 @@ int svdb_las2_plan(uint64_t nrows, uint64_t ncols, uint64_t nnz, uint64_t dimens
 int svdb_randomized_svd(const svdb_matrix* a, uint64_t target_rank, uint64_t n_oversamples,
                         uint64_t n_power_iters, int normalizer, int mean_center, int has_seed, uint64_t seed,
                         int verbose, const svdb_options* opts, svdb_rec* out);
+
+/* ---- adjoint of the truncated SVD (no reference counterpart) ---- */
+
+/* Options of svdb_svd_adjoint; svdb_adjoint_options_default gives FP64,
+ * host buffers, cg_tol 1e-12 and cg_max_iters 5000. */
+typedef struct svdb_adjoint_options {
+    int32_t precision;        /* SVDB_F64, or SVDB_MIXED: FP32 factors and sums in the SDDMM */
+    int32_t inputs_on_device; /* 1: u, s, v, g_u, g_s, g_v and grad_values are device pointers */
+    double cg_tol;            /* relative residual of the complement solves */
+    uint64_t cg_max_iters;
+    void* stream;             /* cudaStream_t, NULL = the handle's stream */
+    uint64_t cg_iterations;   /* out: block-CG iterations run */
+    double cg_residual;       /* out: largest relative residual at exit */
+    double time_ms_solve;     /* out: device time of everything before the SDDMM */
+    double time_ms_sddmm;     /* out: device time of the SDDMM */
+} svdb_adjoint_options;
+
+void svdb_adjoint_options_default(svdb_adjoint_options* opts);
+
+/* Gradient of L(U, s, V) with respect to A's stored values, where
+ * A V = U diag(s), A^T U = V diag(s) are the k leading singular triplets
+ * (u: nrows x k, v: ncols x k, row-major; s descending, s_k above the next
+ * singular value of A) and g_u, g_s, g_v = dL/dU, dL/ds, dL/dV (NULL = 0).
+ * The dense gradient is
+ *   U M V^T + Gamma V^T + U Delta^T,
+ *   M = diag(g_s) + (F o (U^T g_u - g_u^T U)) S + S (F o (V^T g_v - g_v^T V)),
+ *   F_ij = 1 / (s_j^2 - s_i^2) (i != j), 0 on the diagonal,
+ * and (Gamma, Delta) solve, column by column, the shifted systems of the
+ * residual operator A_perp = A - U S V^T that carry the complement
+ * projections (I - U U^T) g_u, (I - V V^T) g_v:
+ *   (s_i^2 I - A_perp^T A_perp) delta_i = s_i b_i + A_perp^T a_i,
+ *   gamma_i = (a_i + A_perp delta_i) / s_i,
+ * solved by block CG on the device.  The gradient is evaluated only at A's
+ * nonzeros, as an SDDMM of the rank-2k factors [U M + Gamma, U] and
+ * [V, Delta]: grad_values[e] = dL/dA(r_e, c_e) in the order the handle was
+ * created with (CSR entry order, or CSC entry order for CSC handles).  COO
+ * handles and masked views return SVDB_ERR_UNSUPPORTED; a CG that stops above
+ * cg_tol returns SVDB_ERR_NOCONV with grad_values filled. */
+int svdb_svd_adjoint(const svdb_matrix* a, uint64_t k, const double* u, const double* s, const double* v,
+                     const double* g_u, const double* g_s, const double* g_v, svdb_adjoint_options* opts,
+                     double* grad_values);
+
+/* SDDMM on the handle's pattern with device factors:
+ * d_out[e] = sum_t left[r_e][t] * right[c_e][t] (left: nrows x rank,
+ * right: ncols x rank, row-major), in the entry order of svdb_svd_adjoint.
+ * precision SVDB_F64: double factors and output; SVDB_MIXED: float. */
+int svdb_sddmm_device(const svdb_matrix* a, const void* d_left, const void* d_right, uint64_t rank, void* d_out,
+                      int precision, void* stream);
+
+/* svd_flip(u, v, u_based_decision) (src/randomized/mod.rs:332-438), in place
+ * on row-major arrays (u: u_rows x u_cols, v: v_rows x v_cols; either may be
+ * NULL).  u-based: column j of u is negated when its first entry of largest
+ * magnitude is negative, and so is row j of v (j < min(v_rows, u_cols)).
+ * v-based: row i of v by its largest entry, and column i of u
+ * (i < min(u_cols, v_rows)).  Both NULL, or the deciding matrix NULL, return
+ * SVDB_ERR_LAS2 as the crate's Las2Error.  on_device = 1: device pointers
+ * (the flip runs on the current device's default stream and synchronises). */
+int svdb_svd_flip(double* u, uint64_t u_rows, uint64_t u_cols, double* v, uint64_t v_rows, uint64_t v_cols,
+                  int u_based_decision, int on_device);
 
 /* ---- results ---- */
 

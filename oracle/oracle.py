@@ -257,3 +257,49 @@ def randomized(A, target_rank, n_oversamples, n_power_iters, normalizer="QR", om
     finally:
         lib().orc_rand_free(C.byref(out))
     return res
+
+
+# --------------------------------------------------------- numpy checkers ----
+def svd_flip(u=None, v=None, u_based_decision=True):
+    """svd_flip (src/randomized/mod.rs:332-438), restated in numpy on copies.
+
+    u-based: column j of u decides by its first entry of largest magnitude (a
+    strict > scan from max_abs = 0, :357-365); negative -> column j of u and
+    row j of v (j < min(v.rows, u.cols), :383-391) are negated.  v-based: row
+    i of v decides (:405-413); column i of u follows (:429-435).
+    """
+    if u is None and v is None:
+        raise OracleError(5, "Both u and v cannot be None")
+    u = None if u is None else np.array(u, dtype=np.float64, copy=True)
+    v = None if v is None else np.array(v, dtype=np.float64, copy=True)
+
+    def first_max(vec):
+        best, idx = 0.0, 0
+        for i, x in enumerate(vec):
+            if abs(x) > best:
+                best, idx = abs(x), i
+        return idx
+
+    if u_based_decision:
+        if u is None:
+            raise OracleError(5, "u cannot be None when u_based_decision is true")
+        signs = np.array([-1.0 if u[first_max(u[:, j]), j] < 0 else 1.0 for j in range(u.shape[1])])
+        u *= signs[None, :]
+        if v is not None:
+            t = min(v.shape[0], len(signs))
+            v[:t] *= signs[:t, None]
+    else:
+        if v is None:
+            raise OracleError(5, "v cannot be None when u_based_decision is false")
+        signs = np.array([-1.0 if v[i, first_max(v[i])] < 0 else 1.0 for i in range(v.shape[0])])
+        v *= signs[:, None]
+        if u is not None:
+            t = min(u.shape[1], len(signs))
+            u[:, :t] *= signs[None, :t]
+    return u, v
+
+
+def sddmm(A, left, right):
+    """out[e] = left[row(e)] . right[col(e)] for the CSR entries of A (numpy)."""
+    rows = np.repeat(np.arange(A["nrows"]), np.diff(A["indptr"]))
+    return np.einsum("ij,ij->i", left[rows], right[A["indices"]])

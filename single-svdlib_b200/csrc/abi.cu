@@ -20,6 +20,10 @@ void las2(const svdb_matrix*, uint64_t, uint64_t, const double[2], double, uint3
 int las2_plan(uint64_t, uint64_t, uint64_t, uint64_t, uint64_t, uint64_t*, uint64_t*, int32_t*, int32_t*);
 void randomized(const svdb_matrix*, uint64_t, uint64_t, uint64_t, int, int, int, uint64_t, int,
                 const svdb_options&, svdb_rec*);
+void svd_adjoint(const svdb_matrix*, int64_t, const double*, const double*, const double*, const double*,
+                 const double*, const double*, svdb_adjoint_options&, double*);
+void sddmm_device(const svdb_matrix*, const void*, const void*, int64_t, void*, int, cudaStream_t);
+void svd_flip(double*, int64_t, int64_t, double*, int64_t, int64_t, bool, bool);
 
 static thread_local std::string g_last_error;
 void set_last_error(const std::string& m) { g_last_error = m; }
@@ -373,6 +377,49 @@ int svdb_rec_recompose(const svdb_rec* r, double* out) {
                 for (uint64_t k = 0; k < d; ++k) acc += r->u[i * d + k] * r->s[k] * r->vt[k * n + j];
                 out[i * n + j] = acc;
             }
+    });
+}
+
+void svdb_adjoint_options_default(svdb_adjoint_options* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->precision = SVDB_F64;
+    o->cg_tol = 1e-12;
+    o->cg_max_iters = 5000;
+}
+
+int svdb_svd_adjoint(const svdb_matrix* a, uint64_t k, const double* u, const double* s, const double* v,
+                     const double* g_u, const double* g_s, const double* g_v, svdb_adjoint_options* opts,
+                     double* grad_values) {
+    return guarded([&] {
+        check_handle(a);
+        svdb_adjoint_options d;
+        svdb_adjoint_options_default(&d);
+        svdb_adjoint_options& o = opts ? *opts : d;
+        if (o.precision != SVDB_F64 && o.precision != SVDB_MIXED) throw Error(SVDB_ERR_ARG, "bad precision");
+        svdb_matrix* am = const_cast<svdb_matrix*>(a);
+        std::lock_guard<std::mutex> lk(am->mu);
+        DeviceGuard g(a->device);
+        svd_adjoint(a, (int64_t)k, u, s, v, g_u, g_s, g_v, o, grad_values);
+    });
+}
+
+int svdb_sddmm_device(const svdb_matrix* a, const void* d_left, const void* d_right, uint64_t rank, void* d_out,
+                      int precision, void* stream) {
+    return guarded([&] {
+        check_handle(a);
+        if (!d_left || !d_right || !d_out) throw Error(SVDB_ERR_ARG, "null argument");
+        if (precision != SVDB_F64 && precision != SVDB_MIXED) throw Error(SVDB_ERR_ARG, "bad precision");
+        DeviceGuard g(a->device);
+        sddmm_device(a, d_left, d_right, (int64_t)rank, d_out, precision, stream ? (cudaStream_t)stream : a->stream);
+    });
+}
+
+int svdb_svd_flip(double* u, uint64_t u_rows, uint64_t u_cols, double* v, uint64_t v_rows, uint64_t v_cols,
+                  int u_based_decision, int on_device) {
+    return guarded([&] {
+        svd_flip(u, (int64_t)u_rows, (int64_t)u_cols, v, (int64_t)v_rows, (int64_t)v_cols, u_based_decision != 0,
+                 on_device != 0);
     });
 }
 

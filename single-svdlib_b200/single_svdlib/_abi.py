@@ -21,7 +21,7 @@ SVDB_OK = 0
 STATUS_NAMES = {
     1: "ImtqlbError", 2: "StartvError", 3: "StponeError", 4: "Imtql2Error", 5: "Las2Error",
     6: "ShapeError", 7: "CudaError", 8: "TimeoutError", 9: "Unsupported", 10: "ArgumentError",
-    11: "OutOfMemory",
+    11: "OutOfMemory", 12: "NoConvergence",
 }
 PRECISION = {"f64": 0, "mixed": 1}
 ALGORITHM = {"lanczos": 0, "legacy": 1}
@@ -58,6 +58,12 @@ class svdb_options(C.Structure):
                 ("trace", C.POINTER(svdb_trace))]
 
 
+class svdb_adjoint_options(C.Structure):
+    _fields_ = [("precision", C.c_int32), ("inputs_on_device", C.c_int32), ("cg_tol", C.c_double),
+                ("cg_max_iters", C.c_uint64), ("stream", C.c_void_p), ("cg_iterations", C.c_uint64),
+                ("cg_residual", C.c_double), ("time_ms_solve", C.c_double), ("time_ms_sddmm", C.c_double)]
+
+
 # Every exported symbol with its prototype: (restype, argtypes).
 P = C.POINTER
 u64, i64, u32, i32, dbl, vp = C.c_uint64, C.c_int64, C.c_uint32, C.c_int32, C.c_double, C.c_void_p
@@ -91,6 +97,10 @@ SIGNATURES = {
     "svdb_las2_plan": (C.c_int, [u64, u64, u64, u64, u64, P(u64), P(u64), P(i32), P(i32)]),
     "svdb_randomized_svd": (C.c_int, [vp, u64, u64, u64, C.c_int, C.c_int, C.c_int, u64, C.c_int,
                                       P(svdb_options), P(svdb_rec)]),
+    "svdb_adjoint_options_default": (None, [P(svdb_adjoint_options)]),
+    "svdb_svd_adjoint": (C.c_int, [vp, u64, vp, vp, vp, vp, vp, vp, P(svdb_adjoint_options), vp]),
+    "svdb_sddmm_device": (C.c_int, [vp, vp, vp, u64, vp, C.c_int, vp]),
+    "svdb_svd_flip": (C.c_int, [vp, u64, u64, vp, u64, u64, C.c_int, C.c_int]),
     "svdb_rec_free": (None, [P(svdb_rec)]),
     "svdb_rec_recompose": (C.c_int, [P(svdb_rec), vp]),
     "svdb_last_error_message": (C.c_char_p, []),

@@ -63,8 +63,15 @@ class UnsupportedError(SvdLibError):
     kind = "Unsupported"
 
 
+class NoConvergenceError(SvdLibError):
+    """An iterative solve (the adjoint's block CG) stopped above its tolerance."""
+
+    kind = "NoConvergence"
+
+
 _ERR = {1: ImtqlbError, 2: StartvError, 3: StponeError, 4: Imtql2Error, 5: Las2Error, 6: ShapeError,
-        7: DeviceError, 8: DeviceError, 9: UnsupportedError, 10: ValueError, 11: DeviceError}
+        7: DeviceError, 8: DeviceError, 9: UnsupportedError, 10: ValueError, 11: DeviceError,
+        12: NoConvergenceError}
 
 
 def check(status: int):

@@ -40,3 +40,17 @@ def randomized_svd(m, target_rank, n_oversamples, n_power_iters, power_iteration
         return rec_from_c(r)
     finally:
         _abi.lib().svdb_rec_free(C.byref(r))
+
+
+def svd_flip(u=None, v=None, u_based_decision=True):
+    """randomized::svd_flip (mod.rs:332-438) on copies of u (m x k) and v (k x n); returns (u, v).
+
+    Runs on the GPU (svdb_svd_flip).  Missing inputs raise Las2Error as the crate does.
+    """
+    uu = None if u is None else np.array(u, dtype=np.float64, order="C", copy=True)
+    vv = None if v is None else np.array(v, dtype=np.float64, order="C", copy=True)
+    ur, uc = (0, 0) if uu is None else uu.shape
+    vr, vc = (0, 0) if vv is None else vv.shape
+    check(_abi.lib().svdb_svd_flip(None if uu is None else uu.ctypes.data, ur, uc,
+                                   None if vv is None else vv.ctypes.data, vr, vc, int(u_based_decision), 0))
+    return uu, vv
