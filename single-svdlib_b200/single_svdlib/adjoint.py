@@ -18,7 +18,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _abi
-from ._core import CscMatrix, CsrMatrix, check
+from ._core import check
 
 
 @dataclass
@@ -55,10 +55,9 @@ def svd_adjoint(a, u, s, v, g_u=None, g_s=None, g_v=None, precision="f64", cg_to
     """dL/dvalues of A (a CsrMatrix or CscMatrix handle), in the handle's entry order.
 
     u: m x k, s: k, v: n x k (the k leading triplets, s descending);
-    g_u, g_s, g_v: dL/du, dL/ds, dL/dv (None = 0).
+    g_u, g_s, g_v: dL/du, dL/ds, dL/dv (None = 0).  Other handle kinds raise
+    UnsupportedError from the library.
     """
-    if not isinstance(a, (CsrMatrix, CscMatrix)):
-        raise TypeError("svd_adjoint needs a CsrMatrix or CscMatrix")
     m, n = a.shape
     s = np.ascontiguousarray(s, dtype=np.float64).ravel()
     k = s.shape[0]
