@@ -2,7 +2,7 @@
 """Benchmark: time-to-k-triplets of randomized_svd on the 100,000 x 30,000
 count-like workload, FP32 (mixed) GPU path against the plain-f64 GPU path.
 
-    python bench.py --gpus N --steps K --warmup W [--impl reference] [--workload randomized|las2]
+    python bench.py --gpus N --steps K --warmup W [--impl reference] [--workload NAME]
 
 One JSON line on rank 0.  A step is one randomized_svd call (rank 50, 10
 oversamples, 3 power iterations, QR normaliser, seed 7) on an all-columns
@@ -13,6 +13,17 @@ upload and result download inside the timed region).  Several GPUs run
 independent replicas (weak scaling).  `--impl reference` times the CPU
 restatement of the crate's path (oracle/, all host threads) on a row sample
 of the same workload and scales it to the full matrix.
+
+Other workloads (--workload), one JSON line each with the same keys:
+  las2        LAS2 f64 on the 5,000 x 2,000 Poisson(20) CSR, dimensions 10,
+              seed 42 (SVDLIBC semantics; the as-written crate path ends in
+              Imtql2Error on this input, timed and reported beside it)
+  las2-large  LAS2 on a 1,000,000 x 200,000 CSR with ~200 M nnz (Zipf 1.85 row
+              lengths on [20, 20000], uniform columns, N(0,1) values plus a
+              planted rank-20 signal), dimensions 100: FP32-value SpMV with
+              FP64 recurrences against plain f64
+  adjoint     truncated-SVD adjoint on a 50,000 x 20,000 CSR, density 0.5 %,
+              N(0,1) values, k = 32: block-CG solve + SDDMM (FP32 throughput)
 """
 from __future__ import annotations
 
@@ -193,6 +204,483 @@ def cpu_reference(indptr, cols, vals, threads, sample_rows, omega):
     return full, measured, nnz_s
 
 
+# ------------------------------------------------------- other workloads --
+def _env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    return rank, world, local, threads
+
+
+def _gpu_setup(local, world):
+    import torch
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+    return torch
+
+
+def _timed(torch, stream, world, fn, k):
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    out = [fn() for _ in range(k)]
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    return e0.elapsed_time(e1) / k, out
+
+
+def _line(args, world, metric, value_s, dtype, config, **extra):
+    d = {"metric": metric, "value": value_s, "unit": "s", "n_gpus": world, "steps": args.steps,
+         "warmup": args.warmup, "ms_per_step": value_s * 1e3, "higher_is_better": False, "scaling": "weak",
+         "vs_baseline": None, "dtype": dtype, "data": "synthetic", "config": config}
+    d.update(extra)
+    print(json.dumps(d), flush=True)
+
+
+def _las2_call(L, C, check, _abi, options, handle, dims, iters, seed, legacy, precision, on_device, s=None,
+               kappa=1e-6):
+    o = options(precision=precision, algorithm="legacy" if legacy else "lanczos", result_on_device=on_device)
+    o.stream = s.cuda_stream if s is not None else None
+    r = _abi.svdb_rec()
+    ei = (C.c_double * 2)(-1e-30, 1e-30)
+    fn = L.svdb_legacy_svd_las2 if legacy else L.svdb_las2
+    st = fn(handle, dims, iters, ei, kappa, seed, C.byref(o), C.byref(r))
+    return st, r
+
+
+def _spmv_gbs(torch, L, check, handle, m, n, nnz, precision, stream, reps=20):
+    """Standalone SpMV (svdb_opa_device) of A and A^T: ms and algorithmic GB/s each."""
+    x = torch.randn(n, dtype=torch.float64, device="cuda")
+    xt = torch.randn(m, dtype=torch.float64, device="cuda")
+    y = torch.empty(m, dtype=torch.float64, device="cuda")
+    yt = torch.empty(n, dtype=torch.float64, device="cuda")
+    sv = 4 if precision == 1 else 8
+    out = {}
+    for name, xi, yo, tr, rows, cols in (("A_x", x, y, 0, m, n), ("At_x", xt, yt, 1, n, m)):
+        for _ in range(3):
+            check(L.svdb_opa_device(handle, xi.data_ptr(), yo.data_ptr(), tr, precision, stream.cuda_stream))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            check(L.svdb_opa_device(handle, xi.data_ptr(), yo.data_ptr(), tr, precision, stream.cuda_stream))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        b = nnz * (sv + 4) + (rows + 1) * 8 + cols * 8 + rows * 8
+        out[name] = {"ms": ms, "gbs": b / ms / 1e6, "bytes": b}
+    return out
+
+
+LAS2_WORKLOAD = ("LAS2 5000x2000 CSR, per row Poisson(20) distinct columns uniform in [0,2000), values U(0,1), "
+                 "dimensions 10, iterations 0, end_interval [-1e-30,1e-30], kappa 1e-6, seed 42")
+
+
+def run_las2(args):
+    """LAS2 f64 on the 5,000 x 2,000 Poisson(20) matrix (numpy PCG64 seed 42)."""
+    import matrices as Mx
+    rank, world, local, threads = _env()
+    A = Mx.poisson_rows(5000, 2000, 20, 42)
+    m, n, nnz = A["nrows"], A["ncols"], len(A["data"])
+    dims, seed = 10, 42
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        import oracle as O
+        O.set_threads(threads)
+        for _ in range(args.warmup):
+            O.las2("csr", A, dims, 0, seed=seed, legacy=True)
+        ts = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            O.las2("csr", A, dims, 0, seed=seed, legacy=True)
+            ts.append(time.perf_counter() - t0)
+        v = statistics.mean(ts)
+        cpu = {"value": v, "unit": "s", "cores": threads, "kind": "port",
+               "sample": "the whole workload (legacy::svdLAS2 restated in C++, OpenMP over the crate's Rayon loops)"}
+        _line(args, 1, "time-to-k-triplets (s), LAS2 k=10 f64", v, "f64", {"workload": LAS2_WORKLOAD, "nnz": nnz},
+              impl="reference", cpu_baseline=cpu,
+              e2e={"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+        return 0
+    torch = _gpu_setup(local, world)
+    from single_svdlib import _abi
+    from single_svdlib._core import check, options, rec_from_c
+    L = _abi.lib()
+    h_ip = torch.from_numpy(A["indptr"].astype(np.uint64).view(np.int64)).pin_memory()
+    h_ix = torch.from_numpy(A["indices"].astype(np.uint64).view(np.int64)).pin_memory()
+    h_v = torch.from_numpy(A["data"]).pin_memory()
+
+    def create():
+        h = C.c_void_p()
+        check(L.svdb_matrix_create_csr(m, n, nnz, h_ip.data_ptr(), h_ix.data_ptr(), h_v.data_ptr(), C.byref(h)))
+        return h
+
+    h = create()
+    stream = torch.cuda.Stream()
+
+    def solve(legacy, prec, on_device=1):
+        st, r = _las2_call(L, C, check, _abi, options, h, dims, 0, seed, legacy, prec, on_device, stream)
+        return st, r
+
+    stage("las2 warmup")
+    for _ in range(args.warmup):
+        for prec in ("f64", "mixed"):
+            st, r = solve(True, prec)
+            check(st)
+            L.svdb_rec_free(C.byref(r))
+    launches0 = L.svdb_kernel_launches()
+    with ClockSampler(local) as clk:
+        ms_f64, recs = _timed(torch, stream, world, lambda: solve(True, "f64"), args.steps)
+    launches = L.svdb_kernel_launches() - launches0
+    clocks = clk.summary()
+    steps_taken = None
+    for st, r in recs:
+        check(st)
+        steps_taken = int(r.diagnostics.lanczos_steps)
+        phases = {"lanczos_ms": r.time_ms_spmv, "tridiag_ms": r.time_ms_tridiag, "ritvec_ms": r.time_ms_ritvec,
+                  "device_total_ms": r.time_ms_total}
+        L.svdb_rec_free(C.byref(r))
+    ms_mixed, recs = _timed(torch, stream, world, lambda: solve(True, "mixed"), args.steps)
+    for st, r in recs:
+        L.svdb_rec_free(C.byref(r))
+    # the crate's own path as written: Imtql2Error after its full run on this input
+    ms_asw, recs = _timed(torch, stream, world, lambda: solve(False, "f64"), max(1, args.steps // 2))
+    asw_status = _abi.STATUS_NAMES.get(recs[0][0], "ok") if recs[0][0] else "ok"
+    for st, r in recs:
+        L.svdb_rec_free(C.byref(r))
+    sig = {}
+    for prec in ("f64", "mixed"):
+        st, r = solve(True, prec, 0)
+        check(st)
+        sig[prec] = rec_from_c(r).s
+        L.svdb_rec_free(C.byref(r))
+    sigma_err = float(np.max(np.abs(sig["mixed"] - sig["f64"]) / np.abs(sig["f64"])))
+    import oracle as O
+    ref = O.las2("csr", A, dims, 0, seed=seed, legacy=True)
+    sigma_err_oracle = float(np.max(np.abs(sig["f64"] - ref["s"]) / np.abs(ref["s"])))
+    # e2e: upload + solve + host result, every step
+    stage("las2 e2e")
+
+    def e2e():
+        hh = create()
+        st, r = _las2_call(L, C, check, _abi, options, hh, dims, 0, seed, True, "f64", 0)
+        check(st)
+        L.svdb_rec_free(C.byref(r))
+        L.svdb_matrix_destroy(hh)
+
+    e2e()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e()
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    spmv = _spmv_gbs(torch, L, check, h, m, n, nnz, 0, stream)
+    peak, peak_kind = peak_hbm()
+    per_step_us = ms_f64 * 1e3 / max(1, steps_taken)
+    step_bytes = spmv["A_x"]["bytes"] + spmv["At_x"]["bytes"]
+    ach = step_bytes / (per_step_us * 1e-6) / 1e9
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        O.set_threads(threads)
+        t0 = time.perf_counter()
+        O.las2("csr", A, dims, 0, seed=seed, legacy=True)
+        tc = time.perf_counter() - t0
+        cpu = {"value": tc, "unit": "s", "cores": threads, "kind": "port",
+               "sample": "the whole workload (legacy::svdLAS2 restated in C++, OpenMP over the crate's Rayon loops)"}
+    ms_f64, ms_mixed = max_over_ranks(ms_f64, world), max_over_ranks(ms_mixed, world)
+    if rank == 0:
+        _line(args, world, "time-to-k-triplets (s), LAS2 k=10 f64", ms_f64 / 1e3, "f64",
+              {"workload": LAS2_WORKLOAD, "nrows": m, "ncols": n, "nnz": nnz, "lanczos_steps": steps_taken,
+               "convention": "SVDLIBC (legacy::svdLAS2)", "parallelism": f"replicas x{world}",
+               "l2": "matrix (1.2 MB) stays in L2: latency-bound, timed back to back"},
+              mixed_value=ms_mixed / 1e3, mixed_speedup_vs_f64=ms_f64 / ms_mixed, sigma_rel_err_mixed_vs_f64=sigma_err,
+              sigma_rel_err_vs_oracle=sigma_err_oracle, phases=phases,
+              lanczos_as_written={"status": asw_status, "seconds": ms_asw / 1e3},
+              roofline={"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                        "traffic": None, "kernel": "k_lanczos_block (per step: A x and A^T x)",
+                        "peak_source": peak_kind, "us_per_lanczos_step": per_step_us, "spmv_standalone": spmv},
+              cpu_baseline=cpu,
+              e2e={"value": e2e_s, "unit": "s", "h2d_bytes_per_step": 8 * (m + 1) + 16 * nnz,
+                   "d2h_bytes_per_step": 8 * (dims * (m + n) + dims)},
+              gpu_launches=int(launches), clocks=clocks)
+    L.svdb_matrix_destroy(h)
+    return 0
+
+
+LARGE_M, LARGE_N, LARGE_DIMS = 1_000_000, 200_000, 100
+LARGE_WORKLOAD = ("LAS2 1000000x200000 CSR, row lengths Zipf(1.85) on [20,20000] (mean 203), columns uniform "
+                  "(duplicates merged), values N(0,1) plus sum_r s_r u_i v_j / density with unit u, v and s "
+                  "geometric 100..1 (r < 20), dimensions 100, SVDLIBC semantics, seed 42")
+
+
+def gen_large(torch, m, n, seed=3):
+    """Seeded 1M x 200k CSR on the device (torch CUDA generator): int64 indptr, int32 columns, f64 values."""
+    rng = np.random.default_rng(seed)
+    ks = np.arange(20, 20001)
+    p = ks.astype(np.float64) ** -1.85
+    p /= p.sum()
+    rowlen = torch.from_numpy(rng.choice(ks, size=m, p=p)).cuda()
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    nnz0 = int(rowlen.sum())
+    keys = torch.repeat_interleave(torch.arange(m, device="cuda", dtype=torch.int64), rowlen) * n
+    keys += torch.randint(0, n, (nnz0,), device="cuda", generator=g, dtype=torch.int64)
+    keys = torch.unique_consecutive(torch.sort(keys).values)
+    rows = keys // n
+    cols = (keys - rows * n).to(torch.int32)
+    del keys
+    nnz = rows.numel()
+    indptr = torch.zeros(m + 1, dtype=torch.int64, device="cuda")
+    indptr[1:] = torch.cumsum(torch.bincount(rows, minlength=m), 0)
+    vals = torch.randn(nnz, dtype=torch.float64, device="cuda", generator=g)
+    r = 20
+    u = torch.randn(m, r, dtype=torch.float64, device="cuda", generator=g)
+    v = torch.randn(n, r, dtype=torch.float64, device="cuda", generator=g)
+    u /= u.norm(dim=0)
+    v /= v.norm(dim=0)
+    sig = torch.logspace(2, 0, r, dtype=torch.float64, device="cuda") * (m * n / nnz)
+    for c0 in range(0, nnz, 1 << 23):
+        c1 = min(nnz, c0 + (1 << 23))
+        vals[c0:c1] += (u[rows[c0:c1]] * v[cols[c0:c1].long()] * sig).sum(1)
+    del rows, u, v
+    return indptr, cols, vals
+
+
+def run_las2_large(args):
+    rank, world, local, threads = _env()
+    if args.impl == "reference" and rank != 0:
+        return 0
+    torch = _gpu_setup(local, world)
+    from single_svdlib import _abi
+    from single_svdlib._core import check, options, rec_from_c
+    L = _abi.lib()
+    m, n, dims, seed = LARGE_M, LARGE_N, LARGE_DIMS, 42
+    if args.scale != 1.0:
+        m, n = int(m * args.scale), int(n * args.scale)
+    stage("las2-large generate")
+    indptr, cols, vals = gen_large(torch, m, n)
+    nnz = vals.numel()
+    if args.impl == "reference":
+        # the CPU restatement on the whole matrix, capped at a few Lanczos steps; the
+        # per-step time is scaled to the step count of a converged run (measured on
+        # the GPU, passed in with --las2-iterations, else 1000)
+        import oracle as O
+        A = {"nrows": m, "ncols": n, "indptr": indptr.cpu().numpy(), "indices": cols.cpu().numpy().astype(np.int64),
+             "data": vals.cpu().numpy()}
+        del indptr, cols, vals
+        O.set_threads(threads)
+        t0 = time.perf_counter()
+        r = O.las2("csr", A, 10, 12, seed=seed, legacy=True)
+        t = time.perf_counter() - t0
+        st = max(1, r["steps"] + 1)
+        target = args.las2_iterations or 1000
+        v = t / st * target
+        cpu = {"value": v, "unit": "s", "cores": threads, "kind": "port",
+               "sample": f"{st} Lanczos steps of legacy::svdLAS2 restated in C++ on the whole matrix ({t:.1f} s), "
+                         f"scaled per step to {target} steps (reorthogonalisation growth not included)"}
+        _line(args, 1, "time-to-k-triplets (s), LAS2 k=100", v, "f64", {"workload": LARGE_WORKLOAD, "nnz": nnz},
+              impl="reference", cpu_baseline=cpu,
+              e2e={"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+        return 0
+    h = C.c_void_p()
+    check(L.svdb_matrix_create_csr_device(m, n, nnz, indptr.data_ptr(), cols.data_ptr(), vals.data_ptr(),
+                                          C.byref(h)))
+    stream = torch.cuda.Stream()
+    iters = args.las2_iterations
+
+    def solve(prec, on_device=1):
+        return _las2_call(L, C, check, _abi, options, h, dims, iters, seed, True, prec, on_device, stream)
+
+    stage("las2-large warmup")
+    for _ in range(args.warmup):
+        st, r = solve("mixed")
+        check(st)
+        L.svdb_rec_free(C.byref(r))
+    launches0 = L.svdb_kernel_launches()
+    with ClockSampler(local) as clk:
+        ms_mixed, recs = _timed(torch, stream, world, lambda: solve("mixed"), args.steps)
+    launches = L.svdb_kernel_launches() - launches0
+    clocks = clk.summary()
+    for st, r in recs:
+        check(st)
+        steps_mixed = int(r.diagnostics.lanczos_steps)
+        d_mixed = int(r.d)
+        L.svdb_rec_free(C.byref(r))
+    stage("las2-large f64")
+    ms_f64, recs = _timed(torch, stream, world, lambda: solve("f64"), 1)
+    for st, r in recs:
+        check(st)
+        steps_f64 = int(r.diagnostics.lanczos_steps)
+        L.svdb_rec_free(C.byref(r))
+    sig = {}
+    for prec in ("f64", "mixed"):
+        st, r = solve(prec, 0)
+        check(st)
+        sig[prec] = rec_from_c(r).s
+        L.svdb_rec_free(C.byref(r))
+    k = min(len(sig["f64"]), len(sig["mixed"]))
+    sigma_err = float(np.max(np.abs(sig["mixed"][:k] - sig["f64"][:k]) / np.abs(sig["f64"][:k]))) if k else None
+    stage("las2-large spmv")
+    spmv_mixed = _spmv_gbs(torch, L, check, h, m, n, nnz, 1, stream)
+    spmv_f64 = _spmv_gbs(torch, L, check, h, m, n, nnz, 0, stream)
+    peak, peak_kind = peak_hbm()
+    dom = max(spmv_mixed.values(), key=lambda x: x["ms"])
+    # e2e: host CSR -> handle -> solve (mixed) -> host result
+    stage("las2-large e2e")
+    h_ip = indptr.cpu().pin_memory()
+    h_ix = cols.to(torch.int64).cpu().pin_memory()
+    h_v = vals.cpu().pin_memory()
+    del indptr, cols, vals
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    hh = C.c_void_p()
+    check(L.svdb_matrix_create_csr(m, n, nnz, h_ip.data_ptr(), h_ix.data_ptr(), h_v.data_ptr(), C.byref(hh)))
+    st, r = _las2_call(L, C, check, _abi, options, hh, dims, iters, seed, True, "mixed", 0)
+    check(st)
+    d2h = 8 * int(r.d) * (m + n + 1)
+    L.svdb_rec_free(C.byref(r))
+    L.svdb_matrix_destroy(hh)
+    e2e_s = time.perf_counter() - t0
+    ms_mixed, ms_f64 = max_over_ranks(ms_mixed, world), max_over_ranks(ms_f64, world)
+    if rank == 0:
+        _line(args, world, "time-to-k-triplets (s), LAS2 k=100, FP32-value SpMV + FP64 recurrences", ms_mixed / 1e3,
+              "f32", {"workload": LARGE_WORKLOAD, "nrows": m, "ncols": n, "nnz": nnz, "iterations_cap": iters,
+                      "lanczos_steps": steps_mixed, "triplets": d_mixed, "parallelism": f"replicas x{world}",
+                      "l2": "inputs larger than L2 (%.1f GB CSR + CSC)" % (nnz * 24 / 1e9)},
+              f64_value=ms_f64 / 1e3, f64_lanczos_steps=steps_f64, mixed_speedup_vs_f64=ms_f64 / ms_mixed,
+              sigma_rel_err_vs_f64=sigma_err,
+              roofline={"bound": "hbm", "achieved": dom["gbs"], "peak": peak, "unit": "GB/s",
+                        "frac": dom["gbs"] / peak, "traffic": None, "kernel": "k_spmv (FP32 values)",
+                        "peak_source": peak_kind, "spmv_mixed": spmv_mixed, "spmv_f64": spmv_f64,
+                        "us_per_lanczos_step_mixed": ms_mixed * 1e3 / max(1, steps_mixed)},
+              cpu_baseline=None,
+              e2e={"value": e2e_s, "unit": "s", "h2d_bytes_per_step": 8 * (m + 1) + 16 * nnz,
+                   "d2h_bytes_per_step": d2h},
+              gpu_launches=int(launches), clocks=clocks)
+    L.svdb_matrix_destroy(h)
+    return 0
+
+
+ADJ_M, ADJ_N, ADJ_K, ADJ_DENSITY = 50_000, 20_000, 32, 0.005
+ADJ_WORKLOAD = ("truncated-SVD adjoint, 50000x20000 CSR, density 0.5 % uniform pattern, values N(0,1), k 32, "
+                "upstream gradients N(0,1); forward LAS2 f64 (SVDLIBC semantics, kappa 1e-10); backward block CG "
+                "(tol 1e-10) + SDDMM of rank-2k factors")
+
+
+def run_adjoint(args):
+    rank, world, local, threads = _env()
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "the crate has no adjoint of the SVD"}), flush=True)
+        return 0
+    torch = _gpu_setup(local, world)
+    import scipy.sparse as sp
+
+    import matrices as Mx
+    from single_svdlib import _abi
+    from single_svdlib._core import check, options, rec_from_c
+    L = _abi.lib()
+    m, n, k = ADJ_M, ADJ_N, ADJ_K
+    rng = np.random.default_rng(5)
+    nnz0 = int(m * n * ADJ_DENSITY)
+    flat = np.unique(rng.integers(0, m * n, nnz0))
+    r_, c_ = np.divmod(flat, n)
+    A = Mx.from_scipy(sp.csr_matrix((rng.standard_normal(flat.size), (r_, c_)), shape=(m, n)))
+    nnz = len(A["data"])
+    ip64, ix64 = A["indptr"].astype(np.uint64), A["indices"].astype(np.uint64)  # alive across the calls
+    h = C.c_void_p()
+    check(L.svdb_matrix_create_csr(m, n, nnz, ip64.ctypes.data, ix64.ctypes.data, A["data"].ctypes.data, C.byref(h)))
+    stream = torch.cuda.Stream()
+    stage("adjoint forward")
+    t0 = time.perf_counter()
+    st, r = _las2_call(L, C, check, _abi, options, h, k + 8, 0, 42, True, "f64", 0, kappa=1e-10)
+    check(st)
+    rec = rec_from_c(r)
+    L.svdb_rec_free(C.byref(r))
+    fwd_s = time.perf_counter() - t0
+    U = np.ascontiguousarray(rec.u[:k].T)
+    S = np.ascontiguousarray(rec.s[:k])
+    V = np.ascontiguousarray(rec.vt[:k].T)
+    gU, gs, gV = rng.standard_normal((m, k)), rng.standard_normal(k), rng.standard_normal((n, k))
+    o = _abi.svdb_adjoint_options()
+    L.svdb_adjoint_options_default(C.byref(o))
+    o.cg_tol = 1e-10
+    o.cg_max_iters = 20000
+    grad = np.empty(nnz)
+
+    def adj():
+        st = L.svdb_svd_adjoint(h, k, U.ctypes.data, S.ctypes.data, V.ctypes.data, gU.ctypes.data, gs.ctypes.data,
+                                gV.ctypes.data, C.byref(o), grad.ctypes.data)
+        return st
+
+    stage("adjoint warmup")
+    for _ in range(args.warmup):
+        adj()
+    launches0 = L.svdb_kernel_launches()
+    with ClockSampler(local) as clk:
+        ms_adj, sts = _timed(torch, stream, world, adj, args.steps)
+    launches = L.svdb_kernel_launches() - launches0
+    clocks = clk.summary()
+    status = _abi.STATUS_NAMES.get(sts[-1], "ok") if sts[-1] else "ok"
+    info = {"cg_iterations": int(o.cg_iterations), "cg_residual": float(o.cg_residual),
+            "time_ms_solve": float(o.time_ms_solve), "time_ms_sddmm": float(o.time_ms_sddmm), "status": status}
+    # SDDMM throughput in FP32 on the rank-2k factors
+    rank2 = 2 * k
+    Lf = torch.randn(m, rank2, device="cuda", dtype=torch.float32)
+    Rf = torch.randn(n, rank2, device="cuda", dtype=torch.float32)
+    out = torch.empty(nnz, device="cuda", dtype=torch.float32)
+    for _ in range(3):
+        check(L.svdb_sddmm_device(h, Lf.data_ptr(), Rf.data_ptr(), rank2, out.data_ptr(), 1, stream.cuda_stream))
+    reps = 50
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        check(L.svdb_sddmm_device(h, Lf.data_ptr(), Rf.data_ptr(), rank2, out.data_ptr(), 1, stream.cuda_stream))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_sddmm = e0.elapsed_time(e1) / reps
+    sddmm_bytes = nnz * (4 + 4) + (m + 1) * 8 + (m + n) * rank2 * 4
+    peak, peak_kind = peak_hbm()
+    gbs = sddmm_bytes / ms_sddmm / 1e6
+    # finite-difference wall time: one central difference = two forward solves
+    t0 = time.perf_counter()
+    for sgn in (1.0, -1.0):
+        vals = A["data"].copy()
+        vals[0] += sgn * 1e-4
+        hh = C.c_void_p()
+        check(L.svdb_matrix_create_csr(m, n, nnz, ip64.ctypes.data, ix64.ctypes.data, vals.ctypes.data, C.byref(hh)))
+        st, r = _las2_call(L, C, check, _abi, options, hh, k + 8, 0, 42, True, "f64", 1, kappa=1e-10)
+        L.svdb_rec_free(C.byref(r))
+        L.svdb_matrix_destroy(hh)
+    fd_s = time.perf_counter() - t0
+    ms_adj = max_over_ranks(ms_adj, world)
+    if rank == 0:
+        _line(args, world, "adjoint wall time (s): block-CG complement solves + SDDMM, k=32", ms_adj / 1e3, "f64",
+              {"workload": ADJ_WORKLOAD, "nrows": m, "ncols": n, "nnz": nnz, "k": k,
+               "parallelism": f"replicas x{world}", "l2": "factors (19 MB FP32) in L2; pattern streamed"},
+              adjoint=info, forward_las2_s=fwd_s, fd_seconds_per_entry=fd_s,
+              sddmm_fp32={"ms": ms_sddmm, "nnz_per_s": nnz / (ms_sddmm * 1e-3), "bytes": sddmm_bytes},
+              roofline={"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+                        "traffic": None, "kernel": "k_sddmm<float> (rank 64)", "peak_source": peak_kind},
+              cpu_baseline=None,
+              e2e={"value": ms_adj / 1e3, "unit": "s", "h2d_bytes_per_step": 8 * (2 * (m + n) * k + k),
+                   "d2h_bytes_per_step": 8 * nnz},
+              gpu_launches=int(launches), clocks=clocks)
+    L.svdb_matrix_destroy(h)
+    return 0
+
+
+WORKLOADS = {"las2": run_las2, "las2-large": run_las2_large, "adjoint": run_adjoint}
+
+
 # ------------------------------------------------------------------- main --
 def main():
     ap = argparse.ArgumentParser()
@@ -203,8 +691,12 @@ def main():
     ap.add_argument("--cpu-sample-rows", type=int, default=20000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--scale", type=float, default=1.0, help="shrink both dimensions (smoke runs only)")
+    ap.add_argument("--workload", default="randomized", choices=["randomized", "las2", "las2-large", "adjoint"])
+    ap.add_argument("--las2-iterations", type=int, default=0, help="las2-large: Lanczos step cap (0 = the crate's)")
     args = ap.parse_args()
     faulthandler.enable()
+    if args.workload != "randomized":
+        return WORKLOADS[args.workload](args)
     global M_ROWS, N_COLS
     if args.scale != 1.0:
         M_ROWS, N_COLS = int(M_ROWS * args.scale), int(N_COLS * args.scale)

@@ -215,6 +215,18 @@ int svdb_multiply_with_dense_device(const svdb_matrix* a, const void* d_dense, u
  * the array: calls that overlap on the GPU race and must be serialised. */
 int svdb_opb_device_noalloc(const svdb_matrix* a, const double* d_x, double* d_y, int transposed, void* stream);
 
+/* svd_opa on device buffers: d_y = A d_x, or A^T d_x when transposed (double
+ * vectors), enqueued on `stream` (NULL = the handle's stream) without
+ * synchronising.  precision SVDB_MIXED reads the FP32 copy of the matrix
+ * values (made on first use) and still sums in FP64. */
+int svdb_opa_device(const svdb_matrix* a, const double* d_x, double* d_y, int transposed, int precision,
+                    void* stream);
+
+/* Device buffers come from the device's stream-ordered pool, which the
+ * library keeps cached between calls; this returns the cached memory of the
+ * current device to the driver (after a device synchronisation). */
+int svdb_release_cached_memory(void);
+
 /* Number of kernels this library has launched in the process so far. */
 uint64_t svdb_kernel_launches(void);
 

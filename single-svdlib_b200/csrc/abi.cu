@@ -24,6 +24,7 @@ void svd_adjoint(const svdb_matrix*, int64_t, const double*, const double*, cons
                  const double*, const double*, svdb_adjoint_options&, double*);
 void sddmm_device(const svdb_matrix*, const void*, const void*, int64_t, void*, int, cudaStream_t);
 void svd_flip(double*, int64_t, int64_t, double*, int64_t, int64_t, bool, bool);
+void release_cached_memory();
 
 static thread_local std::string g_last_error;
 void set_last_error(const std::string& m) { g_last_error = m; }
@@ -214,6 +215,23 @@ int svdb_multiply_with_dense(const svdb_matrix* a, const double* dense, uint64_t
         SVDB_CUDA(cudaStreamSynchronize(s));
     });
 }
+int svdb_opa_device(const svdb_matrix* a, const double* d_x, double* d_y, int transposed, int precision,
+                    void* stream) {
+    return guarded([&] {
+        check_handle(a);
+        if (!d_x || !d_y) throw Error(SVDB_ERR_ARG, "null argument");
+        if (precision != SVDB_F64 && precision != SVDB_MIXED) throw Error(SVDB_ERR_ARG, "bad precision");
+        DeviceGuard g(a->device);
+        const DevCompressed& op = transposed ? csc_of(a) : csr_of(a);
+        if (precision == SVDB_MIXED && !op.val32.p) {
+            svdb_matrix* am = const_cast<svdb_matrix*>(a);
+            std::lock_guard<std::mutex> lk(am->mu);
+            ensure_fp32(a);
+        }
+        spmv(op, precision == SVDB_MIXED, d_x, d_y, stream ? (cudaStream_t)stream : a->stream);
+    });
+}
+
 int svdb_multiply_with_dense_device(const svdb_matrix* a, const void* d_dense, uint64_t l, void* d_result,
                                     int transpose_self, int precision, void* stream) {
     return guarded([&] {
@@ -413,6 +431,10 @@ int svdb_sddmm_device(const svdb_matrix* a, const void* d_left, const void* d_ri
         DeviceGuard g(a->device);
         sddmm_device(a, d_left, d_right, (int64_t)rank, d_out, precision, stream ? (cudaStream_t)stream : a->stream);
     });
+}
+
+int svdb_release_cached_memory(void) {
+    return guarded([&] { release_cached_memory(); });
 }
 
 int svdb_svd_flip(double* u, uint64_t u_rows, uint64_t u_cols, double* v, uint64_t v_rows, uint64_t v_cols,

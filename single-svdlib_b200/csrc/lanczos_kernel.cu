@@ -11,6 +11,7 @@
 #include <cooperative_groups.h>
 
 #include "lanczos_kernel.cuh"
+#include "spmv.cuh"
 #include "svdb_internal.h"
 
 namespace svdb {
@@ -21,44 +22,42 @@ constexpr int kThreads = 512;
 
 __device__ __forceinline__ bool cmp_eq(double a, double b) { return fabs(b - a) < kEps; }
 
-// Row-gather SpMV over the rows of `op`, G lanes per row, rows dealt to warps
-// round-robin.  SCALE: x is read as x * rinv (the dscal of w3 folded in).
-// EPI: y = acc + (-rnm) * w2, and returns this thread's share of dot(y, w3).
-// Only the matrix arrays are read through the non-coherent path: the vectors
-// change between phases of the same launch.
+// Row-gather SpMV over the rows of `op`: rows of more than kSegNnz entries
+// (op.long_rows) one block each, the others through the length bins
+// (spmv_binned, spmv.cuh).  SCALE: x is read as x * rinv (the dscal
+// of w3 folded in).  EPI: y = acc + (-rnm) * w2, and returns this thread's
+// share of dot(y, w3).  Only the matrix arrays are read through the
+// non-coherent path: the vectors change between phases of the same launch.
 template <bool FP32, bool SCALE, bool EPI>
 __device__ __forceinline__ double spmv_rows(const LzOperand& op, const double* x, double rinv, double* y,
-                                            double neg_rnm, const double* w2, const double* w3) {
-    const int G = op.group;
-    const int lane = threadIdx.x & 31;
-    const int sub = lane & (G - 1);
-    const int rpw = 32 / G;
+                                            double neg_rnm, const double* w2, const double* w3, double* sh) {
+    auto xl = [&](int32_t c) {
+        double xv = x[c];
+        if (SCALE) xv = mul_rn(xv, rinv);
+        return xv;
+    };
+    double dotacc = 0.0;
+    auto finish = [&](int64_t r, double acc) {
+        if (EPI) {
+            const double w0 = add_rn(acc, mul_rn(neg_rnm, w2[r]));
+            y[r] = w0;
+            dotacc = fma(w0, w3[r], dotacc);
+        } else {
+            y[r] = acc;
+        }
+    };
+    for (int64_t i = blockIdx.x; i < op.nlong; i += gridDim.x) {
+        const int64_t r = __ldg(op.long_rows + i);
+        const int64_t s = __ldg(op.rp + r), e = __ldg(op.rp + r + 1);
+        double acc = FP32 ? row_dot(op.ci, op.vf, s, e, (int)threadIdx.x, (int)blockDim.x, xl)
+                          : row_dot(op.ci, op.v, s, e, (int)threadIdx.x, (int)blockDim.x, xl);
+        acc = block_sum(acc, sh);
+        if (threadIdx.x == 0) finish(r, acc);
+    }
     const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    double dotacc = 0.0;
-    for (int64_t base = gwarp * rpw; base < op.rows; base += nwarps * rpw) {
-        const int64_t r = base + lane / G;
-        double acc = 0.0;
-        if (r < op.rows) {
-            const int64_t s = __ldg(op.rp + r), e = __ldg(op.rp + r + 1);
-            for (int64_t k = s + sub; k < e; k += G) {
-                double xv = x[__ldg(op.ci + k)];
-                if (SCALE) xv = mul_rn(xv, rinv);
-                const double vv = FP32 ? (double)__ldg(op.vf + k) : __ldg(op.v + k);
-                acc = fma(vv, xv, acc);
-            }
-        }
-        for (int o = G >> 1; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (r < op.rows && sub == 0) {
-            if (EPI) {
-                const double w0 = add_rn(acc, mul_rn(neg_rnm, w2[r]));
-                y[r] = w0;
-                dotacc = fma(w0, w3[r], dotacc);
-            } else {
-                y[r] = acc;
-            }
-        }
-    }
+    if (FP32) spmv_binned(op.rp, op.ci, op.vf, op.bins, gwarp, nwarps, xl, finish);
+    else spmv_binned(op.rp, op.ci, op.v, op.bins, gwarp, nwarps, xl, finish);
     return dotacc;
 }
 
@@ -73,7 +72,7 @@ __device__ __forceinline__ bool grid_sum(double v, double* part, GridBarrier* ba
 }
 
 template <bool FP32>
-__global__ void __launch_bounds__(kThreads, 2) k_lanczos_block(LzArgs a) {
+__global__ void __launch_bounds__(kThreads, 2) k_lanczos_block(const __grid_constant__ LzArgs a) {
     __shared__ double sh[32];
     const int64_t n = a.n;
     const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -132,7 +131,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_lanczos_block(LzArgs a) {
             const double* w4 = WV(4);
             double* w1 = WV(1);
             double* w3s = WV(6);
-            spmv_rows<FP32, true, false>(a.op1, w3, rinv, a.temp, 0.0, nullptr, nullptr);
+            spmv_rows<FP32, true, false>(a.op1, w3, rinv, a.temp, 0.0, nullptr, nullptr, sh);
             for (int64_t e = tid; e < n; e += nth) {
                 w1[e] = mul_rn(rinv, w0[e]);
                 w3s[e] = mul_rn(w3[e], rinv);
@@ -149,7 +148,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_lanczos_block(LzArgs a) {
         // ---- phase 2: w0 = op2 temp - rnm w2; alf[j] = w0 . w3
         double alf_j;
         {
-            double part = spmv_rows<FP32, false, true>(a.op2, a.temp, 1.0, WV(0), -rnm, WV(2), WV(3));
+            double part = spmv_rows<FP32, false, true>(a.op2, a.temp, 1.0, WV(0), -rnm, WV(2), WV(3), sh);
             if (!grid_sum(part, a.part, a.bar, sh, alf_j)) return;
         }
 

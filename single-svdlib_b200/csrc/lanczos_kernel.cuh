@@ -4,6 +4,7 @@
 #include <cstdint>
 
 #include "device_common.cuh"
+#include "svdb_internal.h"
 
 namespace svdb {
 
@@ -26,7 +27,9 @@ struct LzOperand {
     const double* v;
     const float* vf;  // FP32 values (mixed precision) or null
     int64_t rows;
-    int group;        // lanes per row (power of two, <= 32)
+    const int32_t* long_rows;  // rows of more than kSegNnz entries, one block each
+    int64_t nlong;
+    SpmvBins bins;             // the other rows, by length
 };
 
 struct LzArgs {

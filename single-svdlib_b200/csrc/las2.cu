@@ -503,9 +503,9 @@ int64_t Las2Run::lanczos_step(int64_t first, int64_t last, int64_t& ll, bool& en
         LzArgs a;
         std::memset(&a, 0, sizeof a);
         a.op1 = {op1_->ptr.p, op1_->idx.p, op1_->val.p, fp32_ ? op1_->val32.p : nullptr, op1_->nmajor,
-                 group_for(op1_->avg_per_major())};
+                 op1_->plan.multi_rows.p, op1_->plan.nmulti, op1_->plan.bins};
         a.op2 = {op2_->ptr.p, op2_->idx.p, op2_->val.p, fp32_ ? op2_->val32.p : nullptr, op2_->nmajor,
-                 group_for(op2_->avg_per_major())};
+                 op2_->plan.multi_rows.p, op2_->plan.nmulti, op2_->plan.bins};
         a.n = n_;
         for (int k = 0; k < 7; ++k) a.W[k] = W_[k].p;
         a.temp = temp_.p;

@@ -223,9 +223,37 @@ static void upload_compressed(DevCompressed& c, int64_t nmajor, int64_t nminor, 
     }
 }
 
+// Device buffers come from the device's default stream-ordered pool.  With
+// its default release threshold of 0 the pool hands memory back to the driver
+// at every synchronisation, and the next call pays for fresh allocations;
+// the library keeps what it freed cached instead (svdb_release_cached_memory
+// trims it).
+static void keep_pool_cached(int dev) {
+    static std::mutex mu;
+    static bool done[64] = {};
+    std::lock_guard<std::mutex> lk(mu);
+    if (dev < 0 || dev >= 64 || done[dev]) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t thr = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    done[dev] = true;
+}
+
+void release_cached_memory() {
+    int dev = 0;
+    SVDB_CUDA(cudaGetDevice(&dev));
+    cudaMemPool_t pool;
+    SVDB_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
+    SVDB_CUDA(cudaDeviceSynchronize());
+    SVDB_CUDA(cudaMemPoolTrimTo(pool, 0));
+}
+
 static svdb_matrix* new_handle() {
     svdb_matrix* a = new svdb_matrix();
     SVDB_CUDA(cudaGetDevice(&a->device));
+    keep_pool_cached(a->device);
     SVDB_CUDA(cudaStreamCreateWithFlags(&a->stream, cudaStreamNonBlocking));
     return a;
 }

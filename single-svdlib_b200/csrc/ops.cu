@@ -6,6 +6,7 @@
 
 #include "device_common.cuh"
 #include "ops.cuh"
+#include "spmv.cuh"
 #include "svdb_internal.h"
 
 namespace svdb {
@@ -23,36 +24,52 @@ int group_for(double avg) {
 }
 
 // --------------------------------------------------------------- SpMV ----
+// One launch: every block first takes its share of the rows of more than
+// kSegNnz entries (one block per row, the plan's multi rows), then its warps
+// take the other rows through the length bins.  The grid is one wave of
+// resident blocks, so the two parts overlap and no partial wave trails.
 template <typename VT>
 __global__ void __launch_bounds__(256) k_spmv(const int64_t* __restrict__ rp, const int32_t* __restrict__ ci,
-                                              const VT* __restrict__ v, int64_t rows, int G,
+                                              const VT* __restrict__ v, const __grid_constant__ SpmvBins bins,
+                                              const int32_t* __restrict__ long_rows, int64_t nlong,
                                               const double* __restrict__ x, double* __restrict__ y) {
-    const int lane = threadIdx.x & 31;
-    const int sub = lane & (G - 1);
-    const int rpw = 32 / G;
+    __shared__ double sh[32];
+    auto xl = [&](int32_t c) { return __ldg(x + c); };
+    for (int64_t i = blockIdx.x; i < nlong; i += gridDim.x) {
+        const int64_t r = long_rows[i];
+        const double acc = row_dot(ci, v, rp[r], rp[r + 1], (int)threadIdx.x, (int)blockDim.x, xl);
+        const double tot = block_sum(acc, sh);
+        if (threadIdx.x == 0) y[r] = tot;
+    }
     const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t base = gwarp * rpw; base < rows; base += nwarps * rpw) {
-        const int64_t r = base + lane / G;
-        double acc = 0.0;
-        if (r < rows) {
-            const int64_t s = rp[r], e = rp[r + 1];
-            for (int64_t k = s + sub; k < e; k += G) acc = fma((double)v[k], __ldg(x + ci[k]), acc);
-        }
-        for (int o = G >> 1; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (r < rows && sub == 0) y[r] = acc;
+    spmv_binned(rp, ci, v, bins, gwarp, nwarps, xl, [&](int64_t r, double acc) { y[r] = acc; });
+}
+
+template <typename VT>
+static int spmv_grid() {
+    static int per_sm[2] = {0, 0};
+    int& ps = per_sm[sizeof(VT) == 4];
+    if (!ps) {
+        SVDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ps, k_spmv<VT>, 256, 0));
+        if (ps < 1) ps = 1;
     }
+    return ps * device_props().sms;
 }
 
 void spmv(const DevCompressed& m, bool fp32, const double* x, double* y, cudaStream_t s) {
     if (m.nmajor == 0) return;
-    const int G = group_for(m.avg_per_major());
-    const int threads = 256;
-    const int blocks = blocks_for(m.nmajor * G, threads, 16);
-    if (fp32 && m.val32.p)
-        k_spmv<float><<<blocks, threads, 0, s>>>(m.ptr.p, m.idx.p, m.val32.p, m.nmajor, G, x, y);
-    else
-        k_spmv<double><<<blocks, threads, 0, s>>>(m.ptr.p, m.idx.p, m.val.p, m.nmajor, G, x, y);
+    const bool f = fp32 && m.val32.p;
+    const int64_t work = std::max<int64_t>(m.plan.bins.items[kSpmvBins] / 8, m.plan.nmulti);
+    if (f) {
+        const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(work, spmv_grid<float>()));
+        k_spmv<float><<<blocks, 256, 0, s>>>(m.ptr.p, m.idx.p, m.val32.p, m.plan.bins, m.plan.multi_rows.p,
+                                             m.plan.nmulti, x, y);
+    } else {
+        const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(work, spmv_grid<double>()));
+        k_spmv<double><<<blocks, 256, 0, s>>>(m.ptr.p, m.idx.p, m.val.p, m.plan.bins, m.plan.multi_rows.p,
+                                              m.plan.nmulti, x, y);
+    }
     SVDB_CHECK_LAUNCH();
 }
 

@@ -204,6 +204,15 @@ __global__ void k_seg_fill(const int64_t* __restrict__ rp, const int64_t* __rest
     }
 }
 
+__global__ void k_bin_flags(const int64_t* __restrict__ rp, int64_t rows, int64_t lo, int64_t hi,
+                            uint8_t* __restrict__ flag, int32_t* __restrict__ ids) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t len = rp[r + 1] - rp[r];
+        flag[r] = (len > lo && len <= hi) ? 1 : 0;
+        ids[r] = (int32_t)r;
+    }
+}
+
 static int nblk(int64_t work, int threads, int per_sm) {
     int64_t b = (work + threads - 1) / threads;
     return (int)std::max<int64_t>(1, std::min<int64_t>(b, (int64_t)device_props().sms * per_sm));
@@ -242,6 +251,33 @@ void build_seg_plan(DevCompressed& m, cudaStream_t s) {
     SVDB_CUDA(cudaMemcpyAsync(&hm, nm.p, sizeof(hm), cudaMemcpyDeviceToHost, s));
     SVDB_CUDA(cudaStreamSynchronize(s));
     p.nmulti = (int64_t)hm;
+
+    // SpMV bins: a stable partition of the rows by length
+    p.bin_rows.alloc(std::max<int64_t>(rows, 1), s);
+    DevBuf<uint8_t> flag(rows, s);
+    DevBuf<int32_t> ids(rows, s);
+    DevBuf<int64_t> nsel(1, s);
+    size_t tb2 = 0;
+    SVDB_CUDA(cub::DeviceSelect::Flagged(nullptr, tb2, ids.p, flag.p, p.bin_rows.p, nsel.p, rows, s));
+    DevBuf<uint8_t> tmp2(std::max<size_t>(tb2, 1), s);
+    int64_t off = 0, items = 0;
+    for (int b = 0; b < kSpmvBins; ++b) {
+        const int64_t lo = b ? kSpmvBinLen[b - 1] : -1, hi = kSpmvBinLen[b];
+        k_bin_flags<<<nblk(rows, 256, 16), 256, 0, s>>>(m.ptr.p, rows, lo, hi, flag.p, ids.p);
+        SVDB_CHECK_LAUNCH();
+        SVDB_CUDA(cub::DeviceSelect::Flagged(tmp2.p, tb2, ids.p, flag.p, p.bin_rows.p + off, nsel.p, rows, s));
+        int64_t cnt = 0;
+        SVDB_CUDA(cudaMemcpyAsync(&cnt, nsel.p, sizeof(cnt), cudaMemcpyDeviceToHost, s));
+        SVDB_CUDA(cudaStreamSynchronize(s));
+        p.bins.off[b] = off;
+        p.bins.items[b] = items;
+        const int64_t rpw = 32 / (2 << b);
+        off += cnt;
+        items += (cnt + rpw - 1) / rpw;
+    }
+    p.bins.off[kSpmvBins] = off;
+    p.bins.items[kSpmvBins] = items;
+    p.bins.rows = p.bin_rows.p;
 }
 
 // ------------------------------------------------------------- launcher --

@@ -1,0 +1,73 @@
+// Device side of the sparse matrix-vector product, shared by the standalone
+// kernels (ops.cu) and the cooperative Lanczos kernel.
+//
+// Rows of at most kSegNnz entries are taken by groups of G lanes; longer rows
+// (the segment plan's multi-segment rows) by a whole block each, so that a
+// 20,000-entry row does not hold one warp while the rest of the grid idles.
+// Each lane keeps kSpmvUnroll independent (index, value, gather) chains in
+// flight and sums them in a fixed order, so the result does not depend on
+// the grid size.
+#pragma once
+
+#include <cstdint>
+
+#include "device_common.cuh"
+#include "svdb_internal.h"
+
+namespace svdb {
+
+constexpr int kSpmvUnroll = 4;
+
+// sum of v[k] * xload(ci[k]) over the entries k = s + sub + G (kSpmvUnroll t + u)
+// of [s, e) owned by lane `sub` of a G-lane group
+template <typename VT, typename XL>
+__device__ __forceinline__ double row_dot(const int32_t* __restrict__ ci, const VT* __restrict__ v, int64_t s,
+                                          int64_t e, int sub, int G, XL xload) {
+    double acc = 0.0;
+    for (int64_t k = s + sub; k < e; k += (int64_t)kSpmvUnroll * G) {
+        double vv[kSpmvUnroll], xv[kSpmvUnroll];
+#pragma unroll
+        for (int u = 0; u < kSpmvUnroll; ++u) {
+            const int64_t kk = k + (int64_t)u * G;
+            if (kk < e) {
+                vv[u] = (double)__ldg(v + kk);
+                xv[u] = xload(__ldg(ci + kk));
+            } else {
+                vv[u] = 0.0;
+                xv[u] = 0.0;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kSpmvUnroll; ++u) acc = fma(vv[u], xv[u], acc);
+    }
+    return acc;
+}
+
+// Rows of at most kSegNnz entries through the length bins: warp item i of
+// bin b covers 32 / G rows (G = 2 << b lanes each).  FIN(r, sum) is called
+// once per row by the row's first lane.
+template <typename VT, typename XL, typename FIN>
+__device__ __forceinline__ void spmv_binned(const int64_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                            const VT* __restrict__ v, const SpmvBins& bins, int64_t warp0,
+                                            int64_t nwarps, XL xload, FIN fin) {
+    const int lane = threadIdx.x & 31;
+    const int64_t total = bins.items[kSpmvBins];
+    for (int64_t it = warp0; it < total; it += nwarps) {
+        int b = 0;
+        while (b + 1 < kSpmvBins && it >= bins.items[b + 1]) ++b;
+        const int G = 2 << b;
+        const int sub = lane & (G - 1);
+        const int64_t p = bins.off[b] + (it - bins.items[b]) * (32 / G) + lane / G;
+        const bool valid = p < bins.off[b + 1];
+        double acc = 0.0;
+        int64_t r = 0;
+        if (valid) {
+            r = __ldg(bins.rows + p);
+            acc = row_dot(ci, v, __ldg(rp + r), __ldg(rp + r + 1), sub, G, xload);
+        }
+        for (int o = G >> 1; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (valid && sub == 0) fin(r, acc);
+    }
+}
+
+}  // namespace svdb

@@ -82,8 +82,21 @@ struct DevBuf {
 // seg_row[s], stored as -(row + 1) when the row has several segments; those
 // rows are listed in multi_rows and merged by a second, ordered pass.
 constexpr int64_t kSegNnz = 2048;
+// SpMV row bins: bin b (< kSpmvBins) holds the rows of at most
+// kSpmvBinLen[b] entries (and more than kSpmvBinLen[b-1]), ascending, taken
+// by groups of (2 << b) lanes; rows of more than kSegNnz entries are the
+// multi rows, one block each.
+constexpr int kSpmvBins = 5;
+constexpr int64_t kSpmvBinLen[kSpmvBins] = {8, 16, 32, 64, kSegNnz};
+struct SpmvBins {
+    const int32_t* rows;             // bin_rows
+    int64_t off[kSpmvBins + 1];      // bin b: rows[off[b] .. off[b+1])
+    int64_t items[kSpmvBins + 1];    // warp items before bin b (32 / (2 << b) rows per item)
+};
 struct SegPlan {
     int64_t nseg = 0, nmulti = 0;
+    DevBuf<int32_t> bin_rows;
+    SpmvBins bins{};
     DevBuf<int64_t> seg_first;
     DevBuf<int32_t> seg_row;
     DevBuf<int64_t> seg_beg, seg_end;
