@@ -24,6 +24,9 @@ Other workloads (--workload), one JSON line each with the same keys:
               FP64 recurrences against plain f64
   adjoint     truncated-SVD adjoint on a 50,000 x 20,000 CSR, density 0.5 %,
               N(0,1) values, k = 32: block-CG solve + SDDMM (FP32 throughput)
+  batch       randomized_svd on 256 column subsets (sizes uniform in 500..20,000,
+              seed 11) of the 100,000 x 30,000 count-like matrix: rank 30, 10
+              oversamples, 2 power iterations, QR, FP32 products, one CUDA graph
 """
 from __future__ import annotations
 
@@ -678,7 +681,148 @@ def run_adjoint(args):
     return 0
 
 
-WORKLOADS = {"las2": run_las2, "las2-large": run_las2_large, "adjoint": run_adjoint}
+BATCH_COUNT, BATCH_RANK, BATCH_OVER, BATCH_Q, BATCH_SEED = 256, 30, 10, 2, 11
+BATCH_WORKLOAD = ("randomized_svd on 256 MaskedCSRMatrix::with_columns subsets of the 100000x30000 count-like CSR, "
+                  "subset sizes uniform in 500..20000 columns drawn without replacement (seed 11), rank 30 + 10 "
+                  "oversamples, 2 power iterations, QR, seed 7, FP32 products with FP64 Gram/Cholesky/SVD")
+
+
+def batch_subsets(n, count=BATCH_COUNT, seed=BATCH_SEED):
+    rng = np.random.default_rng(seed)
+    sizes = rng.integers(500, 20001, count)
+    return [np.sort(rng.choice(n, int(k), replace=False)) for k in sizes]
+
+
+def batch_cpu_estimate(indptr, cols, vals, subs, threads, sample_rows, nsub=2):
+    """The CPU restatement on `nsub` subsets (first `sample_rows` rows each, scaled
+    to all rows phase by phase as for the randomized workload), then per subset
+    nonzero to the whole batch."""
+    import oracle as O
+    O.set_threads(threads)
+    nnz_s = int(indptr[sample_rows])
+    A = {"nrows": sample_rows, "ncols": N_COLS, "indptr": indptr[: sample_rows + 1], "indices": cols[:nnz_s],
+         "data": vals[:nnz_s]}
+    colnnz = np.bincount(cols, minlength=N_COLS)
+    l = BATCH_RANK + BATCH_OVER
+    t_est, nnz_est, measured = 0.0, 0, 0.0
+    for sub in subs[:nsub]:
+        mask = np.zeros(N_COLS, np.uint8)
+        mask[sub] = 1
+        om = np.random.default_rng(SEED).standard_normal((len(sub), l))
+        t0 = time.perf_counter()
+        r = O.randomized(A, BATCH_RANK, BATCH_OVER, BATCH_Q, "QR", omega=om, mask=mask)
+        measured += time.perf_counter() - t0
+        t = r["times"]
+        sub_nnz_sample = int(np.isin(A["indices"], sub).sum())
+        full_sub_nnz = int(colnnz[sub].sum())
+        t_est += t["sparse"] * (full_sub_nnz / max(1, sub_nnz_sample)) + t["rows"] * (M_ROWS / sample_rows) + t["fixed"]
+        nnz_est += full_sub_nnz
+    total_nnz = int(sum(int(colnnz[s].sum()) for s in subs))
+    return t_est / nnz_est * total_nnz, measured
+
+
+def run_batch(args):
+    rank, world, local, threads = _env()
+    indptr, cols, vals = load_or_generate(rank, world) if args.impl != "reference" or rank == 0 else (None,) * 3
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        subs = batch_subsets(N_COLS)
+        v, measured = batch_cpu_estimate(indptr, cols, vals, subs, threads, args.cpu_sample_rows)
+        cpu = {"value": v, "unit": "s", "cores": threads, "kind": "port",
+               "sample": f"2 of 256 subsets on the first {args.cpu_sample_rows} rows ({measured:.1f} s), scaled "
+                         f"phase by phase to all rows, then by subset nonzeros to the batch"}
+        _line(args, 1, "time per batch (s), 256 masked subsets, randomized_svd k=30", v, "f64",
+              {"workload": BATCH_WORKLOAD}, impl="reference", cpu_baseline=cpu,
+              e2e={"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+        return 0
+    torch = _gpu_setup(local, world)
+    from single_svdlib import _abi
+    from single_svdlib._core import check
+    from single_svdlib.randomized import PowerIterationNormalizer as PIN
+    from single_svdlib.randomized import RandomizedBatch
+    L = _abi.lib()
+    m, n, nnz = M_ROWS, N_COLS, len(vals)
+    subs = batch_subsets(n)
+    h_ip = torch.from_numpy(indptr.astype(np.uint64).view(np.int64)).pin_memory()
+    h_ix = torch.from_numpy(cols.astype(np.uint64).view(np.int64)).pin_memory()
+    h_v = torch.from_numpy(vals).pin_memory()
+
+    def create():
+        h = C.c_void_p()
+        check(L.svdb_matrix_create_csr(m, n, nnz, h_ip.data_ptr(), h_ix.data_ptr(), h_v.data_ptr(), C.byref(h)))
+        return h
+
+    from single_svdlib._core import BorrowedMatrix as _H
+
+    stage("batch create")
+    h = create()
+    stream = torch.cuda.Stream()
+    b = RandomizedBatch(_H(h), subs, BATCH_RANK, BATCH_OVER, BATCH_Q, PIN.QR, SEED, precision="mixed")
+    info0 = b.info()
+    stage("batch warmup")
+    for _ in range(args.warmup):
+        b.run(results=False)
+    launches0 = L.svdb_kernel_launches()
+    with ClockSampler(local) as clk:
+        ms, _ = _timed(torch, torch.cuda.current_stream(), world, lambda: b.run(results=False), args.steps)
+    launches = L.svdb_kernel_launches() - launches0
+    clocks = clk.summary()
+    info = b.info()
+    # sigma error of the FP32 batch against an f64 batch, first 8 subsets
+    stage("batch f64 check")
+    rf = RandomizedBatch(_H(h), subs[:8], BATCH_RANK, BATCH_OVER, BATCH_Q, PIN.QR, SEED, precision="f64").run()
+    rm = RandomizedBatch(_H(h), subs[:8], BATCH_RANK, BATCH_OVER, BATCH_Q, PIN.QR, SEED, precision="mixed").run()
+    sigma_err = float(max(np.max(np.abs(a.s - c.s) / np.abs(c.s)) for a, c in zip(rm, rf)))
+    # e2e: matrix upload + batch preparation + run + every result on the host
+    stage("batch e2e")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    hh = create()
+    be = RandomizedBatch(_H(hh), subs, BATCH_RANK, BATCH_OVER, BATCH_Q, PIN.QR, SEED, precision="mixed")
+    recs = be.run()
+    e2e_s = time.perf_counter() - t0
+    be.close()
+    L.svdb_matrix_destroy(hh)
+    d2h = sum(8 * (r.u.size + r.s.size + r.vt.size) for r in recs)
+    del recs
+    h2d = 8 * (m + 1) + 16 * nnz + 8 * sum(len(s_) for s_ in subs)
+    # algorithmic bytes: per subset and product pass (1 + 2q + 1 passes) the subset's
+    # nonzeros (FP32 value + index), its dense input and output rows (FP32)
+    l = BATCH_RANK + BATCH_OVER
+    colnnz = np.bincount(cols, minlength=n)
+    passes = 2 + 2 * BATCH_Q
+    alg = sum(passes * (8 * int(colnnz[s_].sum()) + 4 * l * (m + len(s_))) for s_ in subs)
+    peak, peak_kind = peak_hbm()
+    ach = alg / (ms * 1e-3) / 1e9
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        stage("batch cpu baseline")
+        v, measured = batch_cpu_estimate(indptr, cols, vals, subs, threads, args.cpu_sample_rows)
+        cpu = {"value": v, "unit": "s", "cores": threads, "kind": "port",
+               "sample": f"2 of 256 subsets on the first {args.cpu_sample_rows} rows ({measured:.1f} s), scaled "
+                         f"phase by phase to all rows, then by subset nonzeros to the batch"}
+    ms = max_over_ranks(ms, world)
+    if rank == 0:
+        _line(args, world, "time per batch (s), 256 masked subsets, randomized_svd k=30", ms / 1e3, "f32",
+              {"workload": BATCH_WORKLOAD, "nrows": m, "ncols": n, "nnz": nnz, "subsets": len(subs),
+               "subset_nnz_total": int(info["total_subset_nnz"]), "parallelism": f"replicas x{world}",
+               "l2": "inputs larger than L2 (subset operands 4.1 GB)"},
+              subsets_per_s=len(subs) / (ms / 1e3), sigma_rel_err_vs_f64_first8=sigma_err,
+              batch={"graph_nodes": info["graph_nodes"], "kernels_per_run": info["kernels_per_run"],
+                     "subsets_per_row_item": info["subsets_per_row_item"], "autotune_ms": info0["time_ms_tune"]},
+              roofline={"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                        "traffic": None, "kernel": "whole batch (algorithmic bytes of all subset products)",
+                        "peak_source": peak_kind},
+              cpu_baseline=cpu,
+              e2e={"value": e2e_s, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+              gpu_launches=int(launches), clocks=clocks)
+    b.close()
+    L.svdb_matrix_destroy(h)
+    return 0
+
+
+WORKLOADS = {"las2": run_las2, "las2-large": run_las2_large, "adjoint": run_adjoint, "batch": run_batch}
 
 
 # ------------------------------------------------------------------- main --
@@ -691,7 +835,8 @@ def main():
     ap.add_argument("--cpu-sample-rows", type=int, default=20000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--scale", type=float, default=1.0, help="shrink both dimensions (smoke runs only)")
-    ap.add_argument("--workload", default="randomized", choices=["randomized", "las2", "las2-large", "adjoint"])
+    ap.add_argument("--workload", default="randomized",
+                    choices=["randomized", "las2", "las2-large", "adjoint", "batch"])
     ap.add_argument("--las2-iterations", type=int, default=0, help="las2-large: Lanczos step cap (0 = the crate's)")
     args = ap.parse_args()
     faulthandler.enable()

@@ -268,6 +268,57 @@ int svdb_randomized_svd(const svdb_matrix* a, uint64_t target_rank, uint64_t n_o
                         uint64_t n_power_iters, int normalizer, int mean_center, int has_seed, uint64_t seed,
                         int verbose, const svdb_options* opts, svdb_rec* out);
 
+/* ---- batches of masked column subsets (no reference counterpart) ---- */
+
+/* A prepared batch: randomized_svd on `count` column subsets of one matrix,
+ * each equivalent to randomized_svd(MaskedCSRMatrix::with_columns(a, cols_b),
+ * ...) with the same arguments and seed.  The subsets are never compacted:
+ * the sparse products read A (CSR and CSC) and remap columns through
+ * per-subset maps.  Every kernel covers all subsets in one launch; the whole
+ * solve is captured once into a CUDA graph and replayed by svdb_batch_run. */
+typedef struct svdb_batch svdb_batch;
+
+typedef struct svdb_batch_options {
+    int32_t precision;        /* SVDB_MIXED (FP32 products and dense operands, FP64 Gram,
+                                 Cholesky, CholeskyQR passes and small SVD) or SVDB_F64 */
+    int32_t result_on_device; /* 1: u/s/vt of each record in HBM */
+    int32_t autotune;         /* 1: time the candidate product shapes on the first batch of
+                                 this shape class and keep the fastest (cached per process) */
+    int32_t use_graph;        /* 1: capture the solve into a CUDA graph (default) */
+    void* stream;             /* cudaStream_t, NULL = the matrix handle's stream */
+} svdb_batch_options;
+
+typedef struct svdb_batch_info {
+    uint64_t count;
+    int32_t subsets_per_row_item; /* autotuned: subsets sharing one read of a row of A */
+    int32_t columns_per_lane;     /* autotuned: dense columns per lane (vector width) */
+    uint64_t graph_nodes;         /* kernels and copies in the captured graph (0 without) */
+    uint64_t kernels_per_run;     /* kernel launches of one run */
+    double time_ms_tune;          /* autotuning time at creation */
+    double time_ms_last_run;      /* device time of the last svdb_batch_run */
+    uint64_t total_subset_nnz;    /* sum over subsets of their nonzeros */
+} svdb_batch_info;
+
+void svdb_batch_options_default(svdb_batch_options* opts);
+/* columns of subset b: columns[col_offsets[b] .. col_offsets[b+1]), as
+ * MaskedCSRMatrix::with_columns takes them (duplicates and order ignored,
+ * an index >= ncols is SVDB_ERR_SHAPE).  Every subset must keep at least
+ * target_rank + n_oversamples columns (SVDB_ERR_UNSUPPORTED otherwise).
+ * `a` is a CSR, CSC or COO handle. */
+int svdb_batch_create(const svdb_matrix* a, const uint64_t* col_offsets, const uint64_t* columns, uint64_t count,
+                      uint64_t target_rank, uint64_t n_oversamples, uint64_t n_power_iters, int normalizer,
+                      int has_seed, uint64_t seed, const svdb_batch_options* opts, svdb_batch** out);
+/* Runs the batch (one graph launch) and fills outs[0..count) like
+ * svdb_randomized_svd: u m x d, s d, vt d x ncols_b. */
+int svdb_batch_run(svdb_batch* batch, svdb_rec* outs);
+int svdb_batch_get_info(const svdb_batch* batch, svdb_batch_info* info);
+void svdb_batch_destroy(svdb_batch* batch);
+/* create + run + destroy. */
+int svdb_randomized_svd_batch(const svdb_matrix* a, const uint64_t* col_offsets, const uint64_t* columns,
+                              uint64_t count, uint64_t target_rank, uint64_t n_oversamples, uint64_t n_power_iters,
+                              int normalizer, int has_seed, uint64_t seed, const svdb_batch_options* opts,
+                              svdb_rec* outs);
+
 /* ---- adjoint of the truncated SVD (no reference counterpart) ---- */
 
 /* Options of svdb_svd_adjoint; svdb_adjoint_options_default gives FP64,

@@ -25,12 +25,19 @@ void svd_adjoint(const svdb_matrix*, int64_t, const double*, const double*, cons
 void sddmm_device(const svdb_matrix*, const void*, const void*, int64_t, void*, int, cudaStream_t);
 void svd_flip(double*, int64_t, int64_t, double*, int64_t, int64_t, bool, bool);
 void release_cached_memory();
+void batch_create(const svdb_matrix*, const uint64_t*, const uint64_t*, uint64_t, uint64_t, uint64_t, uint64_t, int, int,
+                  uint64_t, const svdb_batch_options&, svdb_batch**);
+void batch_run(svdb_batch*, svdb_rec*);
+void batch_info(const svdb_batch*, svdb_batch_info*);
+const svdb_matrix* batch_matrix(const svdb_batch*);
+void batch_destroy(svdb_batch*);
 
 static thread_local std::string g_last_error;
 void set_last_error(const std::string& m) { g_last_error = m; }
 
 static std::atomic<uint64_t> g_launches{0};
 void count_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+void discount_launches(uint64_t n) { g_launches.fetch_sub(n, std::memory_order_relaxed); }
 
 // Runs `f`, mapping exceptions to status codes and the thread's last error.
 template <typename F>
@@ -431,6 +438,71 @@ int svdb_sddmm_device(const svdb_matrix* a, const void* d_left, const void* d_ri
         DeviceGuard g(a->device);
         sddmm_device(a, d_left, d_right, (int64_t)rank, d_out, precision, stream ? (cudaStream_t)stream : a->stream);
     });
+}
+
+void svdb_batch_options_default(svdb_batch_options* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->precision = SVDB_MIXED;
+    o->autotune = 1;
+    o->use_graph = 1;
+}
+
+int svdb_batch_create(const svdb_matrix* a, const uint64_t* col_offsets, const uint64_t* columns, uint64_t count,
+                      uint64_t target_rank, uint64_t n_oversamples, uint64_t n_power_iters, int normalizer,
+                      int has_seed, uint64_t seed, const svdb_batch_options* opts, svdb_batch** out) {
+    return guarded([&] {
+        check_handle(a);
+        if (!out) throw Error(SVDB_ERR_ARG, "null out");
+        svdb_batch_options o;
+        svdb_batch_options_default(&o);
+        if (opts) o = *opts;
+        if (o.precision != SVDB_F64 && o.precision != SVDB_MIXED) throw Error(SVDB_ERR_ARG, "bad precision");
+        svdb_matrix* am = const_cast<svdb_matrix*>(a);
+        std::lock_guard<std::mutex> lk(am->mu);
+        DeviceGuard g(a->device);
+        batch_create(a, col_offsets, columns, count, target_rank, n_oversamples, n_power_iters, normalizer, has_seed,
+                     seed, o, out);
+    });
+}
+
+int svdb_batch_run(svdb_batch* b, svdb_rec* outs) {
+    return guarded([&] {
+        if (!b) throw Error(SVDB_ERR_ARG, "null batch");
+        svdb_matrix* am = const_cast<svdb_matrix*>(batch_matrix(b));
+        std::lock_guard<std::mutex> lk(am->mu);
+        DeviceGuard g(am->device);
+        batch_run(b, outs);
+    });
+}
+
+int svdb_batch_get_info(const svdb_batch* b, svdb_batch_info* info) {
+    return guarded([&] {
+        if (!b || !info) throw Error(SVDB_ERR_ARG, "null argument");
+        batch_info(b, info);
+    });
+}
+
+void svdb_batch_destroy(svdb_batch* b) {
+    if (!b) return;
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(batch_matrix(b)->device);
+    batch_destroy(b);
+    if (prev >= 0) cudaSetDevice(prev);
+}
+
+int svdb_randomized_svd_batch(const svdb_matrix* a, const uint64_t* col_offsets, const uint64_t* columns,
+                              uint64_t count, uint64_t target_rank, uint64_t n_oversamples, uint64_t n_power_iters,
+                              int normalizer, int has_seed, uint64_t seed, const svdb_batch_options* opts,
+                              svdb_rec* outs) {
+    svdb_batch* b = nullptr;
+    int st = svdb_batch_create(a, col_offsets, columns, count, target_rank, n_oversamples, n_power_iters, normalizer,
+                               has_seed, seed, opts, &b);
+    if (st != SVDB_OK) return st;
+    st = svdb_batch_run(b, outs);
+    svdb_batch_destroy(b);
+    return st;
 }
 
 int svdb_release_cached_memory(void) {

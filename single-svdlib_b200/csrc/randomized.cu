@@ -21,6 +21,7 @@
 #include <cstring>
 #include <vector>
 
+#include "dense_small.cuh"
 #include "device_common.cuh"
 #include "ops.cuh"
 #include "svdb_internal.h"
@@ -33,24 +34,11 @@ static int nb(int64_t work, int threads, int per_sm = 16) {
 }
 
 // --------------------------------------------------------------- Omega ----
-// N(0,1) entries from a counter-based generator: splitmix64 (Steele, Lea and
-// Flood 2014) of (seed, index) gives two uniforms, Box-Muller gives the
-// normal.  rand_distr's ziggurat stream is not reproduced.
-__device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
-    x += 0x9E3779B97F4A7C15ull;
-    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
-    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
-    return x ^ (x >> 31);
-}
 template <typename T>
 __global__ void k_omega(uint64_t seed, int64_t total, T* __restrict__ out) {
-    const uint64_t key = splitmix64(seed ^ 0x5DEECE66Dull);
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
-        const uint64_t a = splitmix64(key + 2 * (uint64_t)i), b = splitmix64(key + 2 * (uint64_t)i + 1);
-        const double u1 = ((double)(a >> 11) + 0.5) * (1.0 / 9007199254740992.0);  // (0,1)
-        const double u2 = (double)(b >> 11) * (1.0 / 9007199254740992.0);          // [0,1)
-        out[i] = (T)(sqrt(-2.0 * log(u1)) * cospi(2.0 * u2));
-    }
+    const uint64_t key = omega_key(seed);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = (T)omega_value(key, i);
 }
 
 // ---------------------------------------------------------------- Gram ----
@@ -122,83 +110,13 @@ __global__ void k_gram_reduce(const double* __restrict__ part, int nblocks, int 
 }
 
 // ------------------------------------------------------ small dense ops ----
-// One block: G = R^T R (upper R) in shared memory, then R^-1.  A non-positive
-// pivot restarts the factorisation on G + shift I with shift =
-// shift_scale * trace(G) (shifted CholeskyQR); that sets bit 1 of *flags and
-// *shifted (which enables the third pass).  A second breakdown sets bit 2 and
-// leaves R = R^-1 = I.  R and R^-1 are written to global memory.
 __global__ void __launch_bounds__(1024) k_chol_inv(const double* __restrict__ G, int c, double shift_scale,
                                                    double* __restrict__ R, double* __restrict__ Ri,
                                                    int* __restrict__ flags, int* __restrict__ shifted,
                                                    const int* __restrict__ cond, int ri_in_smem) {
     if (cond && *cond == 0) return;
     extern __shared__ double sm[];  // R work (c*c) | R^-1 (c*c) when ri_in_smem
-    __shared__ int s_fail;
-    __shared__ double s_shift;
-    const int cc = c * c;
-    double* ri = ri_in_smem ? sm + cc : Ri;
-    for (int attempt = 0; attempt < 2; ++attempt) {
-        for (int t = threadIdx.x; t < cc; t += blockDim.x)
-            sm[t] = G[t] + ((attempt == 1 && t / c == t % c) ? s_shift : 0.0);
-        if (threadIdx.x == 0) s_fail = 0;
-        __syncthreads();
-        for (int k = 0; k < c; ++k) {
-            if (threadIdx.x == 0) {
-                const double d = sm[k * c + k];
-                if (d > 0.0 && isfinite(d)) sm[k * c + k] = sqrt(d);
-                else s_fail = 1;
-            }
-            __syncthreads();
-            if (s_fail) break;
-            const double piv = sm[k * c + k];
-            for (int j = k + 1 + threadIdx.x; j < c; j += blockDim.x) sm[k * c + j] /= piv;
-            __syncthreads();
-            const int rem = c - k - 1;
-            for (int t = threadIdx.x; t < rem * rem; t += blockDim.x) {
-                const int i = k + 1 + t / rem, j = k + 1 + t % rem;
-                if (i <= j) sm[i * c + j] -= sm[k * c + i] * sm[k * c + j];
-            }
-            __syncthreads();
-        }
-        if (!s_fail) break;
-        if (attempt == 0) {
-            if (threadIdx.x == 0) {
-                double tr = 0.0;
-                for (int i = 0; i < c; ++i) tr += G[i * c + i];
-                s_shift = shift_scale * tr > 0.0 ? shift_scale * tr : 1e-300;
-                atomicOr(flags, 1);
-                *shifted = 1;
-            }
-            __syncthreads();
-        }
-    }
-    if (s_fail) {
-        if (threadIdx.x == 0) atomicOr(flags, 2);
-        for (int t = threadIdx.x; t < cc; t += blockDim.x) {
-            const double v = (t / c == t % c) ? 1.0 : 0.0;
-            R[t] = v;
-            Ri[t] = v;
-        }
-        return;
-    }
-    for (int t = threadIdx.x; t < cc; t += blockDim.x) {
-        if (t / c > t % c) sm[t] = 0.0;
-        ri[t] = 0.0;
-    }
-    __syncthreads();
-    for (int t = threadIdx.x; t < cc; t += blockDim.x) R[t] = sm[t];
-    // R^-1 column j by back substitution (one thread per column)
-    for (int j = threadIdx.x; j < c; j += blockDim.x) {
-        for (int i = j; i >= 0; --i) {
-            double s = (i == j) ? 1.0 : 0.0;
-            for (int k = i + 1; k <= j; ++k) s -= sm[i * c + k] * ri[k * c + j];
-            ri[i * c + j] = s / sm[i * c + i];
-        }
-    }
-    if (ri_in_smem) {
-        __syncthreads();
-        for (int t = threadIdx.x; t < cc; t += blockDim.x) Ri[t] = ri[t];
-    }
+    chol_inv_body(G, c, shift_scale, R, Ri, flags, shifted, ri_in_smem, sm);
 }
 
 // C (c x c) = A (c x c) B (c x c), one block
@@ -264,90 +182,12 @@ __global__ void k_colnorm(T* __restrict__ X, int64_t rows, int c) {
         for (int64_t r = threadIdx.x; r < rows; r += blockDim.x) X[r * c + j] = (T)((double)X[r * c + j] * scale);
 }
 
-// One-sided Jacobi SVD of R (c x c, row-major) in one block: W = R V with
-// orthogonal columns, sigma_j = |W_j|, U_j = W_j / sigma_j.  Round-robin pair
-// ordering, one warp per pair.  Outputs sorted by descending sigma:
-// U (c x c), V (c x c), sig (c).  status = 2 if the sweep limit is reached.
+// One-sided Jacobi SVD of the c x c R in one block (jacobi_svd_body).
 __global__ void __launch_bounds__(1024) k_jacobi_svd(const double* __restrict__ R, int c, double* __restrict__ U,
                                                      double* __restrict__ V, double* __restrict__ sig,
                                                      int* __restrict__ status) {
-    extern __shared__ double sm[];  // W (c x cp) | Vs (c x cp) | norms (cp) ; column-major
-    const int cp = c + (c & 1);     // even number of columns (zero padding column)
-    double* W = sm;
-    double* Vs = sm + (size_t)c * cp;
-    double* nr = Vs + (size_t)cp * cp;
-    __shared__ int s_rot;
-    for (int t = threadIdx.x; t < c * cp; t += blockDim.x) {
-        const int i = t % c, j = t / c;
-        W[j * c + i] = (j < c) ? R[i * c + j] : 0.0;
-    }
-    for (int t = threadIdx.x; t < cp * cp; t += blockDim.x) Vs[t] = ((t % cp) == (t / cp)) ? 1.0 : 0.0;
-    __syncthreads();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    const int half = cp / 2;
-    const double tol = 2.220446049250313e-16 * (double)(c > 4 ? c : 4);
-    int sweep = 0;
-    for (; sweep < 60; ++sweep) {
-        if (threadIdx.x == 0) s_rot = 0;
-        __syncthreads();
-        for (int round = 0; round < cp - 1; ++round) {
-            for (int pr = warp; pr < half; pr += nwarps) {
-                // round-robin: position 0 fixed, others rotate
-                int a_pos = pr, b_pos = cp - 1 - pr;
-                auto at = [&](int pos) { return pos == 0 ? 0 : 1 + (pos - 1 + round) % (cp - 1); };
-                int p = at(a_pos), q = at(b_pos);
-                if (p > q) { int t = p; p = q; q = t; }
-                double al = 0, be = 0, ga = 0;
-                for (int i = lane; i < c; i += 32) {
-                    const double x = W[p * c + i], y = W[q * c + i];
-                    al = fma(x, x, al);
-                    be = fma(y, y, be);
-                    ga = fma(x, y, ga);
-                }
-                al = warp_sum(al);
-                be = warp_sum(be);
-                ga = warp_sum(ga);
-                if (ga != 0.0 && fabs(ga) > tol * sqrt(al * be)) {
-                    const double zeta = (be - al) / (2.0 * ga);
-                    const double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-                    const double cs = 1.0 / sqrt(1.0 + t * t), sn = cs * t;
-                    for (int i = lane; i < c; i += 32) {
-                        const double x = W[p * c + i], y = W[q * c + i];
-                        W[p * c + i] = cs * x - sn * y;
-                        W[q * c + i] = sn * x + cs * y;
-                    }
-                    for (int i = lane; i < cp; i += 32) {
-                        const double x = Vs[p * cp + i], y = Vs[q * cp + i];
-                        Vs[p * cp + i] = cs * x - sn * y;
-                        Vs[q * cp + i] = sn * x + cs * y;
-                    }
-                    if (lane == 0) s_rot = 1;
-                }
-            }
-            __syncthreads();
-        }
-        if (!s_rot) break;
-        __syncthreads();
-    }
-    if (sweep == 60 && threadIdx.x == 0) *status = 2;
-    for (int j = warp; j < cp; j += nwarps) {
-        double s = 0.0;
-        for (int i = lane; i < c; i += 32) s = fma(W[j * c + i], W[j * c + i], s);
-        s = warp_sum(s);
-        if (lane == 0) nr[j] = sqrt(s);
-    }
-    __syncthreads();
-    // rank of each column by descending norm (ties by index) -> output position
-    for (int j = threadIdx.x; j < c; j += blockDim.x) {
-        int pos = 0;
-        for (int k = 0; k < c; ++k)
-            if (nr[k] > nr[j] || (nr[k] == nr[j] && k < j)) ++pos;
-        sig[pos] = nr[j];
-        for (int i = 0; i < c; ++i) {
-            U[i * c + pos] = nr[j] > 0.0 ? W[j * c + i] / nr[j] : (i == pos ? 1.0 : 0.0);
-            V[i * c + pos] = Vs[j * cp + i];
-        }
-    }
+    extern __shared__ double sm[];
+    jacobi_svd_body(R, c, U, V, sig, status, sm);
 }
 
 __global__ void k_to_float(const double* __restrict__ in, float* __restrict__ out, int64_t n) {

@@ -33,6 +33,7 @@ void set_last_error(const std::string& msg);
 // number of kernels launched since the previous check; the count feeds
 // svdb_kernel_launches().
 void count_launches(uint64_t n);
+void discount_launches(uint64_t n);  // launches recorded into a graph, counted when it runs
 #define SVDB_CHECK_LAUNCH_N(n)             \
     do {                                   \
         ::svdb::count_launches(n);         \

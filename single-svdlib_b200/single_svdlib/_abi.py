@@ -64,6 +64,17 @@ class svdb_adjoint_options(C.Structure):
                 ("cg_residual", C.c_double), ("time_ms_solve", C.c_double), ("time_ms_sddmm", C.c_double)]
 
 
+class svdb_batch_options(C.Structure):
+    _fields_ = [("precision", C.c_int32), ("result_on_device", C.c_int32), ("autotune", C.c_int32),
+                ("use_graph", C.c_int32), ("stream", C.c_void_p)]
+
+
+class svdb_batch_info(C.Structure):
+    _fields_ = [("count", C.c_uint64), ("subsets_per_row_item", C.c_int32), ("columns_per_lane", C.c_int32),
+                ("graph_nodes", C.c_uint64), ("kernels_per_run", C.c_uint64), ("time_ms_tune", C.c_double),
+                ("time_ms_last_run", C.c_double), ("total_subset_nnz", C.c_uint64)]
+
+
 # Every exported symbol with its prototype: (restype, argtypes).
 P = C.POINTER
 u64, i64, u32, i32, dbl, vp = C.c_uint64, C.c_int64, C.c_uint32, C.c_int32, C.c_double, C.c_void_p
@@ -99,6 +110,14 @@ SIGNATURES = {
     "svdb_las2_plan": (C.c_int, [u64, u64, u64, u64, u64, P(u64), P(u64), P(i32), P(i32)]),
     "svdb_randomized_svd": (C.c_int, [vp, u64, u64, u64, C.c_int, C.c_int, C.c_int, u64, C.c_int,
                                       P(svdb_options), P(svdb_rec)]),
+    "svdb_batch_options_default": (None, [P(svdb_batch_options)]),
+    "svdb_batch_create": (C.c_int, [vp, vp, vp, u64, u64, u64, u64, C.c_int, C.c_int, u64, P(svdb_batch_options),
+                                    P(vp)]),
+    "svdb_batch_run": (C.c_int, [vp, vp]),
+    "svdb_batch_get_info": (C.c_int, [vp, P(svdb_batch_info)]),
+    "svdb_batch_destroy": (None, [vp]),
+    "svdb_randomized_svd_batch": (C.c_int, [vp, vp, vp, u64, u64, u64, u64, C.c_int, C.c_int, u64,
+                                            P(svdb_batch_options), vp]),
     "svdb_adjoint_options_default": (None, [P(svdb_adjoint_options)]),
     "svdb_svd_adjoint": (C.c_int, [vp, u64, vp, vp, vp, vp, vp, vp, P(svdb_adjoint_options), vp]),
     "svdb_sddmm_device": (C.c_int, [vp, vp, vp, u64, vp, C.c_int, vp]),

@@ -324,6 +324,17 @@ class MaskedCSRMatrix(_Handle):
         return m2o[: self.ncols()], o2m[: self._parent.ncols()]
 
 
+class BorrowedMatrix(_Handle):
+    """A matrix handle created through the C ABI directly (svdb_matrix_create_*);
+    the caller keeps ownership and destroys it."""
+
+    def __init__(self, handle):
+        self._take(handle)
+
+    def close(self):
+        self._h = None
+
+
 def as_smat(a):
     """Accept the package's matrix types or a scipy.sparse matrix (uploaded as CSR)."""
     if isinstance(a, _Handle):
