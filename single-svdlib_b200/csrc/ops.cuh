@@ -17,6 +17,8 @@ int group_for(double avg);
 // Instantiated for (double, double), (float, float) and (float, double).
 template <typename XT, typename OT>
 void spmm_dev(const DevCompressed& m, bool fp32, const XT* X, int l, OT* Y, cudaStream_t s);
+// Raises the error a TMA gather wait of an earlier SpMM recorded (synchronises).
+void spmm_tma_check();
 
 void datx(double a, const double* x, double* y, int64_t n, cudaStream_t s);  // y = a * x
 

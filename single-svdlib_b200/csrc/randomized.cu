@@ -457,6 +457,7 @@ void randomized(const svdb_matrix* A, uint64_t target_rank, uint64_t n_oversampl
         cudaEventDestroy(ev.first);
         cudaEventDestroy(ev.second);
     }
+    spmm_tma_check();
     if (hflags & 2) throw Error(SVDB_ERR_LAS2, "randomized_svd: CholeskyQR broke down even with a shift");
 
     std::memset(rec, 0, sizeof(*rec));

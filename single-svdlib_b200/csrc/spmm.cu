@@ -12,8 +12,14 @@
 // FP64 across chunks).  Register caps: 64 per thread for FP32 operands, 85 for
 // FP64 operands (no spills at 4 gathers in flight per group).
 #include <cub/cub.cuh>
+#include <cuda.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <cstdlib>
+#include <mutex>
+#include <string>
+#include <type_traits>
 
 #include "device_common.cuh"
 #include "ops.cuh"
@@ -313,9 +319,250 @@ static void spmm_impl(const DevCompressed& m, const VT* v, const XT* X, int l, O
     }
 }
 
+
+// ------------------------------------------------------ TMA row gathers --
+// FP32 dense operand, FP32 matrix values: the rows X[c] of a chunk of 32
+// entries are fetched by the tensor memory accelerator (tile::gather4: four
+// rows of one box each, the box one row high and BOXW columns wide; columns
+// past l read as zero) into a per-warp shared-memory ring of kTS chunks, so
+// the bytes in flight cost no registers.  Each warp owns whole segments of
+// the plan; a chunk's sums are FP32, chunks are added in FP64 as in
+// k_spmm_seg.  Waits on the ring's mbarriers give up after 2 s of
+// %globaltimer and raise g_tma_err (read by spmm_tma_check).
+constexpr int kTW = 8;   // warps per CTA
+constexpr int kTS = 3;   // chunks in flight per warp
+constexpr int kTE = 32;  // entries per chunk
+__device__ int g_tma_err;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ uint64_t gtimer() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+                 : "=r"(ok)
+                 : "r"(bar), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity, uint64_t limit_ns) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = gtimer();
+    while (!mbar_try_wait(bar, parity))
+        if (gtimer() - t0 > limit_ns) return false;
+    return true;
+}
+
+template <typename OT, int BOXW>
+__global__ void __launch_bounds__(kTW * 32, 1) k_spmm_tma(const __grid_constant__ CUtensorMap xmap,
+                                                           const int32_t* __restrict__ ci,
+                                                           const float* __restrict__ val,
+                                                           const int32_t* __restrict__ seg_row,
+                                                           const int64_t* __restrict__ seg_beg,
+                                                           const int64_t* __restrict__ seg_end, int64_t nseg, int l,
+                                                           OT* __restrict__ Y, int64_t ldy,
+                                                           double* __restrict__ part) {
+    constexpr int ROWB = BOXW * 4;            // bytes of one gathered row
+    constexpr int CHUNKB = kTE * ROWB;        // bytes of one chunk
+    constexpr int CPL = BOXW / 32;            // columns per lane
+    const unsigned full = 0xffffffffu;
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ __align__(8) uint64_t bars[kTW][kTS];
+    __shared__ float svals[kTW][kTS][kTE];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (smem_u32(smem) & 127) {  // TMA destinations need 128-byte alignment
+        if (threadIdx.x == 0) atomicOr(&g_tma_err, 2);
+        return;
+    }
+    unsigned char* ring = smem + (size_t)w * kTS * CHUNKB;
+    if (lane == 0) {
+        for (int st = 0; st < kTS; ++st)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bars[w][st])) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+    const int64_t nw = (int64_t)gridDim.x * kTW;
+    int64_t i_sg = blockIdx.x * (int64_t)kTW + w, i_k0 = i_sg < nseg ? seg_beg[i_sg] : 0;
+    int64_t c_sg = i_sg, c_k0 = i_k0;
+    int issued = 0, consumed = 0;
+
+    auto issue = [&]() {
+        if (i_sg >= nseg) return;
+        const int64_t e = seg_end[i_sg];
+        const int cnt = (int)min((int64_t)kTE, e - i_k0);
+        const int st = issued % kTS;
+        const int32_t cm = lane < cnt ? __ldg(ci + i_k0 + lane) : 0;
+        svals[w][st][lane] = lane < cnt ? __ldg(val + i_k0 + lane) : 0.f;
+        const int ng = (cnt + 3) >> 2;
+        int32_t r[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int32_t cu = __shfl_sync(full, cm, (4 * lane + u) & 31);
+            const int32_t cb = __shfl_sync(full, cm, (4 * lane) & 31);
+            r[u] = (4 * lane + u < cnt) ? cu : cb;  // pad a short group with its first row
+        }
+        const uint32_t bar = smem_u32(&bars[w][st]);
+        if (lane == 0)
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(ng * 4 * ROWB)
+                         : "memory");
+        __syncwarp();
+        if (lane < ng) {
+            const uint32_t dst = smem_u32(ring + st * CHUNKB + lane * 4 * ROWB);
+            asm volatile(
+                "cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::bytes"
+                " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(dst),
+                "l"(reinterpret_cast<uint64_t>(&xmap)), "r"(0), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(bar)
+                : "memory");
+        }
+        ++issued;
+        i_k0 += kTE;
+        if (i_k0 >= e) {
+            i_sg += nw;
+            if (i_sg < nseg) i_k0 = seg_beg[i_sg];
+        }
+    };
+
+#pragma unroll
+    for (int p = 0; p < kTS; ++p) issue();
+    double acc[CPL];
+#pragma unroll
+    for (int u = 0; u < CPL; ++u) acc[u] = 0.0;
+    bool failed = false;
+    while (consumed < issued) {
+        const int st = consumed % kTS;
+        if (!mbar_wait_bounded(smem_u32(&bars[w][st]), (uint32_t)((consumed / kTS) & 1), 2000000000ull)) {
+            failed = true;
+            break;
+        }
+        const int64_t e = seg_end[c_sg];
+        const int cnt = (int)min((int64_t)kTE, e - c_k0);
+        const float v = svals[w][st][lane];
+        const float* xs = reinterpret_cast<const float*>(ring + st * CHUNKB) + CPL * lane;
+        float sum[CPL];
+#pragma unroll
+        for (int u = 0; u < CPL; ++u) sum[u] = 0.f;
+#pragma unroll 4
+        for (int q = 0; q < cnt; ++q) {
+            const float vq = __shfl_sync(full, v, q);
+            if (CPL == 2) {
+                const float2 x = *reinterpret_cast<const float2*>(xs + q * BOXW);
+                sum[0] = fmaf(vq, x.x, sum[0]);
+                sum[CPL - 1] = fmaf(vq, x.y, sum[CPL - 1]);
+            } else {
+                sum[0] = fmaf(vq, xs[q * BOXW], sum[0]);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < CPL; ++u) acc[u] += (double)sum[u];
+        __syncwarp();
+        ++consumed;
+        c_k0 += kTE;
+        if (c_k0 >= e) {
+            const int32_t rr = seg_row[c_sg];
+#pragma unroll
+            for (int u = 0; u < CPL; ++u) {
+                const int col = CPL * lane + u;
+                if (col < l) {
+                    if (rr >= 0) Y[(int64_t)rr * ldy + col] = (OT)acc[u];
+                    else part[c_sg * (int64_t)l + col] = acc[u];
+                }
+                acc[u] = 0.0;
+            }
+            c_sg += nw;
+            if (c_sg < nseg) c_k0 = seg_beg[c_sg];
+        }
+        issue();
+    }
+    if (failed) {
+        if (lane == 0) atomicOr(&g_tma_err, 1);
+        // let the copies already issued land before the ring goes away (bounded)
+        for (; consumed < issued; ++consumed)
+            mbar_wait_bounded(smem_u32(&bars[w][consumed % kTS]), (uint32_t)((consumed / kTS) & 1), 100000000ull);
+    }
+}
+
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        cudaDriverEntryPointQueryResult q;
+        void* p = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// TMA path: FP32 operand with contiguous rows of l (a multiple of 4, at most
+// 64) on a 16-byte aligned base; SVDB_SPMM=seg selects the register-gather
+// kernel instead.
+static bool tma_eligible(const void* X, int l, int64_t ldx) {
+    static const bool off = [] {
+        const char* e = getenv("SVDB_SPMM");
+        return e && std::string(e) == "seg";
+    }();
+    return !off && ldx == l && l % 4 == 0 && l <= 64 && (reinterpret_cast<uintptr_t>(X) % 16) == 0 && encode_fn();
+}
+
+template <typename OT>
+static void launch_tma(const DevCompressed& m, const float* v, const float* X, int l, OT* Y, double* part,
+                       cudaStream_t s) {
+    const int boxw = l <= 32 ? 32 : 64;
+    CUtensorMap map;
+    cuuint64_t gdim[2] = {(cuuint64_t)l, (cuuint64_t)m.nminor};
+    cuuint64_t gstr[1] = {(cuuint64_t)l * 4};
+    cuuint32_t box[2] = {(cuuint32_t)boxw, 1};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = encode_fn()(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(X), gdim, gstr, box, estr,
+                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw Error(SVDB_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+    const size_t smem = (size_t)kTW * kTS * kTE * boxw * 4;
+    const int blocks = (int)std::max<int64_t>(
+        1, std::min<int64_t>((m.plan.nseg + kTW - 1) / kTW, (int64_t)device_props().sms));
+    if (boxw == 32) {
+        SVDB_CUDA(cudaFuncSetAttribute(k_spmm_tma<OT, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_spmm_tma<OT, 32><<<blocks, kTW * 32, smem, s>>>(map, m.idx.p, v, m.plan.seg_row.p, m.plan.seg_beg.p,
+                                                          m.plan.seg_end.p, m.plan.nseg, l, Y, l, part);
+    } else {
+        SVDB_CUDA(cudaFuncSetAttribute(k_spmm_tma<OT, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_spmm_tma<OT, 64><<<blocks, kTW * 32, smem, s>>>(map, m.idx.p, v, m.plan.seg_row.p, m.plan.seg_beg.p,
+                                                          m.plan.seg_end.p, m.plan.nseg, l, Y, l, part);
+    }
+    SVDB_CHECK_LAUNCH();
+    if (m.plan.nmulti) {
+        k_spmm_merge<OT><<<nblk(m.plan.nmulti * 32, 256, 16), 256, 0, s>>>(m.plan.seg_first.p, m.plan.multi_rows.p,
+                                                                          m.plan.nmulti, part, l, Y, l);
+        SVDB_CHECK_LAUNCH();
+    }
+}
+
+void spmm_tma_check() {
+    int e = 0;
+    SVDB_CUDA(cudaMemcpyFromSymbol(&e, g_tma_err, sizeof(int)));
+    if (e) {
+        const int z = 0;
+        SVDB_CUDA(cudaMemcpyToSymbol(g_tma_err, &z, sizeof(int)));
+        if (e & 2) throw Error(SVDB_ERR_CUDA, "SpMM: shared-memory ring not 128-byte aligned; no gather was issued");
+        throw Error(SVDB_ERR_TIMEOUT, "SpMM: a tensor-memory gather did not complete within 2 s");
+    }
+}
+
 template <typename XT, typename OT>
 void spmm_dev(const DevCompressed& m, bool fp32, const XT* X, int l, OT* Y, cudaStream_t s) {
     if (m.nmajor == 0 || l == 0) return;
+    if constexpr (std::is_same<XT, float>::value) {
+        if (fp32 && m.val32.p && m.nnz > 0 && tma_eligible(X, l, l)) {
+            DevBuf<double> part;
+            if (m.plan.nmulti) part.alloc(m.plan.nseg * (int64_t)l, s);
+            launch_tma<OT>(m, m.val32.p, X, l, Y, part.p, s);
+            return;
+        }
+    }
     if (fp32 && m.val32.p) spmm_impl<float, XT, OT>(m, m.val32.p, X, l, Y, s);
     else spmm_impl<double, XT, OT>(m, m.val.p, X, l, Y, s);
 }

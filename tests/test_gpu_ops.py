@@ -74,3 +74,33 @@ def test_empty_rows_and_columns():
     x = np.arange(12.0)
     close(h.svd_opa(x), S @ x)
     close(h.svd_opa(np.ones(8), transposed=True), S.T @ np.ones(8))
+
+
+@pytest.mark.parametrize("l", [1, 8, 30, 40, 60, 64, 96])
+@pytest.mark.parametrize("transpose", [False, True])
+def test_device_fp32_spmm_against_numpy(l, transpose):
+    """svdb_multiply_with_dense_device with FP32 operands (tensor-memory row
+    gathers when the rows are 16-byte multiples of at most 64 columns, the
+    register-gather kernel otherwise) against numpy on FP32-rounded inputs;
+    includes a row long enough to be split into several segments."""
+    import torch
+    from single_svdlib import _abi
+    from single_svdlib._core import check
+    rng = np.random.default_rng(l)
+    D = (rng.random((700, 5000)) < 0.01) * rng.standard_normal((700, 5000))
+    D[3, :] = rng.standard_normal(5000)        # 5000 entries: three segments of the plan
+    D[:, 7] = rng.standard_normal(700)         # a dense column for A^T
+    A = M.dense(D)
+    h = upload("csr", A)
+    rows_in = 700 if transpose else 5000
+    X = rng.standard_normal((rows_in, l)).astype(np.float32)
+    Df = D.astype(np.float32).astype(np.float64)
+    ref = (Df.T if transpose else Df) @ X.astype(np.float64)
+    tx = torch.from_numpy(X).cuda()
+    ty = torch.empty((5000 if transpose else 700, l), dtype=torch.float32, device="cuda")
+    check(_abi.lib().svdb_multiply_with_dense_device(h.handle, tx.data_ptr(), l, ty.data_ptr(), int(transpose), 1,
+                                                     None))
+    torch.cuda.synchronize()
+    got = ty.cpu().numpy().astype(np.float64)
+    scale = np.abs(ref).max()
+    assert np.abs(got - ref).max() <= 2e-6 * scale
