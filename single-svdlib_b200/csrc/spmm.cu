@@ -289,14 +289,17 @@ void build_seg_plan(DevCompressed& m, cudaStream_t s) {
 // ------------------------------------------------------------- launcher --
 template <typename VT, typename XT, typename OT, int CPL, int H>
 static void launch_seg(const DevCompressed& m, const VT* v, const XT* X, int64_t ldx, int lc, OT* Y, int64_t ldy,
-                       double* part, cudaStream_t s) {
+                       double* part, cudaStream_t s, int64_t lo = 0, int64_t hi = -1) {
+    if (hi < 0) hi = m.plan.nseg;
+    if (hi <= lo) return;
     const uintptr_t align = std::min<uintptr_t>(16, sizeof(XT) * CPL);
     const bool vec = (CPL > 1) && (ldx % CPL == 0) && ((reinterpret_cast<uintptr_t>(X) % align) == 0);
-    const int blocks = nblk(m.plan.nseg * 32, 256, 16);
+    const int blocks = nblk((hi - lo) * 32, 256, 16);
     constexpr int U = 4;
-    k_spmm_seg<VT, XT, OT, CPL, H, U><<<blocks, 256, 0, s>>>(m.idx.p, v, m.plan.seg_row.p, m.plan.seg_beg.p,
-                                                             m.plan.seg_end.p, m.plan.nseg, X, ldx, lc, vec, Y,
-                                                             ldy, part);
+    // segment s of the range is segment lo + s of the plan; its partial row lives at part[(lo + s) * lc]
+    k_spmm_seg<VT, XT, OT, CPL, H, U><<<blocks, 256, 0, s>>>(m.idx.p, v, m.plan.seg_row.p + lo, m.plan.seg_beg.p + lo,
+                                                             m.plan.seg_end.p + lo, hi - lo, X, ldx, lc, vec, Y,
+                                                             ldy, part ? part + lo * (int64_t)lc : nullptr);
     SVDB_CHECK_LAUNCH();
 }
 
@@ -497,20 +500,28 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     return fn;
 }
 
-// TMA path: FP32 operand with contiguous rows of l (a multiple of 4, at most
-// 64) on a 16-byte aligned base; SVDB_SPMM=seg selects the register-gather
-// kernel instead.
+// TMA path (opt-in, SVDB_SPMM=tma): FP32 operand with contiguous rows of l
+// (a multiple of 4, at most 64) on a 16-byte aligned base.  On B200 it moved
+// about 4.9 TB/s of 256-byte rows against 7.4 TB/s for the register gathers
+// of k_spmm_seg (100,000 x 30,000, 65 M nonzeros, l = 60), so it is not the
+// default; the variable is read on every call.
+// TMA path (opt-in, SVDB_SPMM=tma): FP32 operand with contiguous rows of l
+// (a multiple of 4, at most 64) on a 16-byte aligned base.  On B200 it moved
+// about 4.9 TB/s of 256-byte rows against 7.4 TB/s for the register gathers
+// of k_spmm_seg (100,000 x 30,000, 65 M nonzeros, l = 60), and splitting the
+// segments between the two kernels on two streams was no faster than
+// k_spmm_seg alone: both are held by the same L2 gather traffic.  So it is
+// not the default; the variable is read on every call.
 static bool tma_eligible(const void* X, int l, int64_t ldx) {
-    static const bool off = [] {
-        const char* e = getenv("SVDB_SPMM");
-        return e && std::string(e) == "seg";
-    }();
-    return !off && ldx == l && l % 4 == 0 && l <= 64 && (reinterpret_cast<uintptr_t>(X) % 16) == 0 && encode_fn();
+    const char* e = getenv("SVDB_SPMM");
+    const bool on = e && std::string(e) == "tma";
+    return on && ldx == l && l % 4 == 0 && l <= 64 && (reinterpret_cast<uintptr_t>(X) % 16) == 0 && encode_fn();
 }
 
 template <typename OT>
 static void launch_tma(const DevCompressed& m, const float* v, const float* X, int l, OT* Y, double* part,
-                       cudaStream_t s) {
+                       cudaStream_t s, int64_t lo = 0, int64_t hi = -1, bool merge = true) {
+    if (hi < 0) hi = m.plan.nseg;
     const int boxw = l <= 32 ? 32 : 64;
     CUtensorMap map;
     cuuint64_t gdim[2] = {(cuuint64_t)l, (cuuint64_t)m.nminor};
@@ -522,19 +533,24 @@ static void launch_tma(const DevCompressed& m, const float* v, const float* X, i
                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) throw Error(SVDB_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
     const size_t smem = (size_t)kTW * kTS * kTE * boxw * 4;
-    const int blocks = (int)std::max<int64_t>(
-        1, std::min<int64_t>((m.plan.nseg + kTW - 1) / kTW, (int64_t)device_props().sms));
-    if (boxw == 32) {
-        SVDB_CUDA(cudaFuncSetAttribute(k_spmm_tma<OT, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_spmm_tma<OT, 32><<<blocks, kTW * 32, smem, s>>>(map, m.idx.p, v, m.plan.seg_row.p, m.plan.seg_beg.p,
-                                                          m.plan.seg_end.p, m.plan.nseg, l, Y, l, part);
-    } else {
-        SVDB_CUDA(cudaFuncSetAttribute(k_spmm_tma<OT, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_spmm_tma<OT, 64><<<blocks, kTW * 32, smem, s>>>(map, m.idx.p, v, m.plan.seg_row.p, m.plan.seg_beg.p,
-                                                          m.plan.seg_end.p, m.plan.nseg, l, Y, l, part);
+    const int64_t ns = hi - lo;
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((ns + kTW - 1) / kTW, (int64_t)device_props().sms));
+    double* pp = part ? part + lo * (int64_t)l : nullptr;
+    if (ns > 0) {
+        if (boxw == 32) {
+            SVDB_CUDA(cudaFuncSetAttribute(k_spmm_tma<OT, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            k_spmm_tma<OT, 32><<<blocks, kTW * 32, smem, s>>>(map, m.idx.p, v, m.plan.seg_row.p + lo,
+                                                              m.plan.seg_beg.p + lo, m.plan.seg_end.p + lo, ns, l, Y,
+                                                              l, pp);
+        } else {
+            SVDB_CUDA(cudaFuncSetAttribute(k_spmm_tma<OT, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            k_spmm_tma<OT, 64><<<blocks, kTW * 32, smem, s>>>(map, m.idx.p, v, m.plan.seg_row.p + lo,
+                                                              m.plan.seg_beg.p + lo, m.plan.seg_end.p + lo, ns, l, Y,
+                                                              l, pp);
+        }
+        SVDB_CHECK_LAUNCH();
     }
-    SVDB_CHECK_LAUNCH();
-    if (m.plan.nmulti) {
+    if (merge && m.plan.nmulti) {
         k_spmm_merge<OT><<<nblk(m.plan.nmulti * 32, 256, 16), 256, 0, s>>>(m.plan.seg_first.p, m.plan.multi_rows.p,
                                                                           m.plan.nmulti, part, l, Y, l);
         SVDB_CHECK_LAUNCH();
