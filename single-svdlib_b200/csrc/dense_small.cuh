@@ -34,38 +34,47 @@ __device__ __forceinline__ double omega_value(uint64_t key, int64_t i) {
 // shift_scale * trace(G) (shifted CholeskyQR); that sets bit 1 of *flags and
 // *shifted (which enables the third pass).  A second breakdown sets bit 2 and
 // leaves R = R^-1 = I.  R and R^-1 are written to global memory.
-// sm: c*c doubles of shared memory (2*c*c when ri_in_smem).  Any block size.
+// The factorisation runs on the first 128 threads with one named barrier per
+// step: step k updates a_ij -= a_ki a_kj / a_kk with the unscaled pivot row,
+// and every row is scaled by 1/sqrt(a_kk) at the end.
+// sm: c*c doubles of shared memory (2*c*c when ri_in_smem); c <= 128; at
+// least 128 threads.
 __device__ __forceinline__ void chol_inv_body(const double* __restrict__ G, int c, double shift_scale,
                                               double* __restrict__ R, double* __restrict__ Ri,
                                               int* __restrict__ flags, int* __restrict__ shifted, int ri_in_smem,
                                               double* sm) {
     __shared__ int s_fail;
     __shared__ double s_shift;
+    __shared__ double s_rd[128];  // 1 / sqrt(a_kk)
     const int cc = c * c;
     double* ri = ri_in_smem ? sm + cc : Ri;
+    if (blockDim.x < 128 || c > 128) {  // the named barrier needs 128 threads; s_rd holds 128 pivots
+        if (threadIdx.x == 0) atomicOr(flags, 2);
+        for (int t = threadIdx.x; t < cc; t += blockDim.x) R[t] = Ri[t] = (t / c == t % c) ? 1.0 : 0.0;
+        return;
+    }
     for (int attempt = 0; attempt < 2; ++attempt) {
         for (int t = threadIdx.x; t < cc; t += blockDim.x)
             sm[t] = G[t] + ((attempt == 1 && t / c == t % c) ? s_shift : 0.0);
         if (threadIdx.x == 0) s_fail = 0;
         __syncthreads();
-        for (int k = 0; k < c; ++k) {
-            if (threadIdx.x == 0) {
+        if (threadIdx.x < 128) {
+            for (int k = 0; k < c; ++k) {
                 const double d = sm[k * c + k];
-                if (d > 0.0 && isfinite(d)) sm[k * c + k] = sqrt(d);
-                else s_fail = 1;
+                if (!(d > 0.0 && isfinite(d))) {  // the same value for all 128 threads
+                    if (threadIdx.x == 0) s_fail = 1;
+                    break;
+                }
+                const int rem = c - k - 1;
+                const double inv = 1.0 / d;
+                for (int t = threadIdx.x; t < rem * rem; t += 128) {
+                    const int i = k + 1 + t / rem, j = k + 1 + t % rem;
+                    if (i <= j) sm[i * c + j] -= sm[k * c + i] * sm[k * c + j] * inv;
+                }
+                asm volatile("bar.sync 1, 128;" ::: "memory");
             }
-            __syncthreads();
-            if (s_fail) break;
-            const double piv = sm[k * c + k];
-            for (int j = k + 1 + threadIdx.x; j < c; j += blockDim.x) sm[k * c + j] /= piv;
-            __syncthreads();
-            const int rem = c - k - 1;
-            for (int t = threadIdx.x; t < rem * rem; t += blockDim.x) {
-                const int i = k + 1 + t / rem, j = k + 1 + t % rem;
-                if (i <= j) sm[i * c + j] -= sm[k * c + i] * sm[k * c + j];
-            }
-            __syncthreads();
         }
+        __syncthreads();
         if (!s_fail) break;
         if (attempt == 0) {
             if (threadIdx.x == 0) {
@@ -87,18 +96,34 @@ __device__ __forceinline__ void chol_inv_body(const double* __restrict__ G, int 
         }
         return;
     }
+    for (int k = threadIdx.x; k < c; k += blockDim.x) s_rd[k] = 1.0 / sqrt(sm[k * c + k]);
+    __syncthreads();
     for (int t = threadIdx.x; t < cc; t += blockDim.x) {
-        if (t / c > t % c) sm[t] = 0.0;
+        const int i = t / c, j = t % c;
+        double v = 0.0;
+        if (i == j) v = sqrt(sm[t]);
+        else if (i < j) v = sm[t] * s_rd[i];
+        ri[t] = v;  // staged: sm still holds the pivots other threads read
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < cc; t += blockDim.x) {
+        sm[t] = ri[t];
+        R[t] = ri[t];
         ri[t] = 0.0;
     }
     __syncthreads();
-    for (int t = threadIdx.x; t < cc; t += blockDim.x) R[t] = sm[t];
-    // R^-1 column j by back substitution (one thread per column)
-    for (int j = threadIdx.x; j < c; j += blockDim.x) {
-        for (int i = j; i >= 0; --i) {
-            double s = (i == j) ? 1.0 : 0.0;
-            for (int k = i + 1; k <= j; ++k) s -= sm[i * c + k] * ri[k * c + j];
-            ri[i * c + j] = s / sm[i * c + i];
+    // R^-1 column j by back substitution, one warp per column: the inner sums
+    // run across the lanes (a fixed tree), the rows in turn
+    {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+        for (int j = warp; j < c; j += nwarps) {
+            for (int i = j; i >= 0; --i) {
+                double s = 0.0;
+                for (int k = i + 1 + lane; k <= j; k += 32) s = fma(sm[i * c + k], ri[k * c + j], s);
+                s = warp_sum(s);
+                if (lane == 0) ri[i * c + j] = ((i == j ? 1.0 : 0.0) - s) / sm[i * c + i];
+                __syncwarp();
+            }
         }
     }
     if (ri_in_smem) {
@@ -110,7 +135,7 @@ __device__ __forceinline__ void chol_inv_body(const double* __restrict__ G, int 
 // One-sided Jacobi SVD of R (c x c, row-major) in one block: W = R V with
 // orthogonal columns, sigma_j = |W_j|, U_j = W_j / sigma_j.  Round-robin pair
 // ordering, one warp per pair.  Outputs sorted by descending sigma:
-// U (c x c), V (c x c), sig (c).  status = 2 if the sweep limit is reached.
+// U (c x c), V (c x c), sig (c).  *status = sweeps << 8, | 2 if the sweep limit is reached.
 // sm: (c * cp + cp * cp + cp) doubles, cp = c rounded up to even.  Any
 // block size that is a multiple of 32.
 __device__ __forceinline__ void jacobi_svd_body(const double* __restrict__ R, int c, double* __restrict__ U,
@@ -174,7 +199,7 @@ __device__ __forceinline__ void jacobi_svd_body(const double* __restrict__ R, in
         if (!s_rot) break;
         __syncthreads();
     }
-    if (sweep == 60 && threadIdx.x == 0) *status = 2;
+    if (threadIdx.x == 0) *status = (sweep << 8) | (sweep == 60 ? 2 : 0);  // sweeps, limit flag
     for (int j = warp; j < cp; j += nwarps) {
         double s = 0.0;
         for (int i = lane; i < c; i += 32) s = fma(W[j * c + i], W[j * c + i], s);

@@ -90,22 +90,30 @@ __global__ void __launch_bounds__(256) k_gram_part(const T* __restrict__ X, int6
             if (a < c && b < c) out[a * c + b] = acc[i][j];
         }
 }
-// G[p] = sum over blocks of part[b][p]: four interleaved partial sums, fixed order
-__global__ void k_gram_reduce(const double* __restrict__ part, int nblocks, int c, double* __restrict__ G,
-                              const int* __restrict__ cond) {
+// G[p] = sum over blocks of part[b][p].  A block covers 32 elements; its 8
+// warps sum fixed slices of the blocks, and the slices are added in slice
+// order, so G[a][b] and G[b][a] still see the same operations (G symmetric).
+constexpr int kRedSlices = 8;
+__global__ void __launch_bounds__(256) k_gram_reduce(const double* __restrict__ part, int nblocks, int c,
+                                                     double* __restrict__ G, const int* __restrict__ cond) {
     if (cond && *cond == 0) return;
+    __shared__ double sh[kRedSlices][32];
     const int cc = c * c;
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < cc; p += gridDim.x * blockDim.x) {
-        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-        int b = 0;
-        for (; b + 4 <= nblocks; b += 4) {
-            s0 += part[(int64_t)b * cc + p];
-            s1 += part[(int64_t)(b + 1) * cc + p];
-            s2 += part[(int64_t)(b + 2) * cc + p];
-            s3 += part[(int64_t)(b + 3) * cc + p];
-        }
-        for (; b < nblocks; ++b) s0 += part[(int64_t)b * cc + p];
-        G[p] = (s0 + s1) + (s2 + s3);
+    const int e = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int sl = threadIdx.x >> 5;
+    double acc = 0.0;
+    if (e < cc) {
+        const int per = (nblocks + kRedSlices - 1) / kRedSlices;
+        const int b0 = sl * per, b1 = min(nblocks, b0 + per);
+        for (int bq = b0; bq < b1; ++bq) acc += part[(int64_t)bq * cc + e];
+    }
+    sh[sl][threadIdx.x & 31] = acc;
+    __syncthreads();
+    if (sl == 0 && e < cc) {
+        double t = 0.0;
+#pragma unroll
+        for (int k = 0; k < kRedSlices; ++k) t += sh[k][threadIdx.x];
+        G[e] = t;
     }
 }
 
@@ -132,9 +140,10 @@ __global__ void k_small_gemm(const double* __restrict__ A, const double* __restr
 }
 
 // Out (rows x cout) = X (rows x c) S (c x lds, first cout columns).  S and a
-// 32-row tile of X are staged in shared memory.
-constexpr int kRmRows = 32;
-template <typename TI, typename TO>
+// 64-row tile of X are staged in shared memory; a 16 x 16 thread grid gives
+// every thread a 4 x NJ register tile (rows ty + 16 i, columns tx + 16 j).
+constexpr int kRmRows = 64;
+template <typename TI, typename TO, int NJ>
 __global__ void __launch_bounds__(256) k_right_mul(const TI* __restrict__ X, int64_t rows, int c,
                                                    const double* __restrict__ S, int lds, int cout,
                                                    TO* __restrict__ Out, const int* __restrict__ cond) {
@@ -142,18 +151,38 @@ __global__ void __launch_bounds__(256) k_right_mul(const TI* __restrict__ X, int
     extern __shared__ double sm[];  // S: c*cout | X tile: kRmRows*c
     double* ss = sm;
     double* xs = sm + c * cout;
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     for (int t = threadIdx.x; t < c * cout; t += blockDim.x) ss[t] = S[(t / cout) * lds + t % cout];
     for (int64_t r0 = (int64_t)blockIdx.x * kRmRows; r0 < rows; r0 += (int64_t)gridDim.x * kRmRows) {
         const int nr = (int)std::min<int64_t>(kRmRows, rows - r0);
         __syncthreads();
         for (int t = threadIdx.x; t < nr * c; t += blockDim.x) xs[t] = (double)X[r0 * c + t];
         __syncthreads();
-        for (int t = threadIdx.x; t < nr * cout; t += blockDim.x) {
-            const int rr = t / cout, j = t % cout;
-            const double* xr = xs + rr * c;
-            double s = 0.0;
-            for (int k = 0; k < c; ++k) s = fma(xr[k], ss[k * cout + j], s);
-            Out[(r0 + rr) * cout + j] = (TO)s;
+        double acc[4][NJ];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < NJ; ++j) acc[i][j] = 0.0;
+        for (int k = 0; k < c; ++k) {
+            double xv[4], sv[NJ];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) xv[i] = (ty + 16 * i < nr) ? xs[(ty + 16 * i) * c + k] : 0.0;
+#pragma unroll
+            for (int j = 0; j < NJ; ++j) sv[j] = (tx + 16 * j < cout) ? ss[k * cout + tx + 16 * j] : 0.0;
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < NJ; ++j) acc[i][j] = fma(xv[i], sv[j], acc[i][j]);
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int rr = ty + 16 * i;
+            if (rr >= nr) continue;
+#pragma unroll
+            for (int j = 0; j < NJ; ++j) {
+                const int col = tx + 16 * j;
+                if (col < cout) Out[(r0 + rr) * cout + col] = (TO)acc[i][j];
+            }
         }
     }
 }
@@ -231,20 +260,25 @@ static void gram(RandCtx& cx, const double* X, int64_t rows, int c, double* G, c
         case 7: k_gram_part<double, 7><<<nblk, 256, smem, cx.s>>>(X, rows, c, chunk, cx.part.p, cond); break;
         default: k_gram_part<double, 8><<<nblk, 256, smem, cx.s>>>(X, rows, c, chunk, cx.part.p, cond); break;
     }
-    k_gram_reduce<<<nb((int64_t)c * c, 128), 128, 0, cx.s>>>(cx.part.p, nblk, c, G, cond);
+    k_gram_reduce<<<(c * c + 31) / 32, 32 * kRedSlices, 0, cx.s>>>(cx.part.p, nblk, c, G, cond);
     SVDB_CHECK_LAUNCH_N(2);
 }
 
 static void right_mul(const double* X, int64_t rows, int c, const double* S, int lds, int cout, double* Out,
                       cudaStream_t s, const int* cond = nullptr) {
     const size_t smem = ((size_t)c * cout + (size_t)kRmRows * c) * sizeof(double);
-    if (smem > 200 * 1024) throw Error(SVDB_ERR_UNSUPPORTED, "dense factor wider than the shared-memory tile");
-    if (smem > 48 * 1024)
-        SVDB_CUDA(cudaFuncSetAttribute(k_right_mul<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem));
+    if (smem > 220 * 1024 || cout > 128) throw Error(SVDB_ERR_UNSUPPORTED, "dense factor wider than the shared-memory tile");
     const int blocks = (int)std::max<int64_t>(
         1, std::min<int64_t>((rows + kRmRows - 1) / kRmRows, (int64_t)device_props().sms * 4));
-    k_right_mul<double, double><<<blocks, 256, smem, s>>>(X, rows, c, S, lds, cout, Out, cond);
+    auto go = [&](auto kern) {
+        if (smem > 48 * 1024)
+            SVDB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kern<<<blocks, 256, smem, s>>>(X, rows, c, S, lds, cout, Out, cond);
+    };
+    if (cout <= 16) go(k_right_mul<double, double, 1>);
+    else if (cout <= 32) go(k_right_mul<double, double, 2>);
+    else if (cout <= 64) go(k_right_mul<double, double, 4>);
+    else go(k_right_mul<double, double, 8>);
     SVDB_CHECK_LAUNCH();
 }
 
@@ -413,9 +447,13 @@ void randomized(const svdb_matrix* A, uint64_t target_rank, uint64_t n_oversampl
         if (smem > 220 * 1024) throw Error(SVDB_ERR_UNSUPPORTED, "randomized_svd: sample width above the Jacobi tile");
         SVDB_CUDA(cudaFuncSetAttribute(k_jacobi_svd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         if (n >= c) {
-            // B^T = Q_b R;  R = U_J S V_J^T  ->  B = V_J S (Q_b U_J)^T
+            // B^T = Q_b R;  R = U_J S V_J^T  ->  B = V_J S (Q_b U_J)^T.  The one-sided
+            // Jacobi runs on R^T = V_J S U_J^T, whose columns (the rows of the QR
+            // factor) are graded, which takes fewer sweeps than R itself.
             cholesky_qr(cx, Bt.p, n, c, R.p);
-            k_jacobi_svd<<<1, 1024, smem, s>>>(R.p, r, Ur.p, Vr.p, sig.p, jac_status.p);
+            DevBuf<double> Rt((size_t)r * r, s);
+            transpose_dense<double>(R.p, Rt.p, r, r, s);
+            k_jacobi_svd<<<1, 1024, smem, s>>>(Rt.p, r, Vr.p, Ur.p, sig.p, jac_status.p);
             // U_B = V_J (c x r); V_B = Q_b U_J (n x r)
             SVDB_CUDA(cudaMemcpyAsync(UB.p, Vr.p, (size_t)r * r * 8, cudaMemcpyDeviceToDevice, s));
             DevBuf<double> VB((size_t)n * r, s);
@@ -426,7 +464,9 @@ void randomized(const svdb_matrix* A, uint64_t target_rank, uint64_t n_oversampl
             DevBuf<double> B((size_t)c * n, s);
             transpose_dense<double>(Bt.p, B.p, n, c, s);
             cholesky_qr(cx, B.p, c, (int)n, R.p);
-            k_jacobi_svd<<<1, 1024, smem, s>>>(R.p, r, Ur.p, Vr.p, sig.p, jac_status.p);
+            DevBuf<double> Rt((size_t)r * r, s);
+            transpose_dense<double>(R.p, Rt.p, r, r, s);
+            k_jacobi_svd<<<1, 1024, smem, s>>>(Rt.p, r, Vr.p, Ur.p, sig.p, jac_status.p);
             right_mul(B.p, c, (int)n, Ur.p, r, r, UB.p, s);
             transpose_dense<double>(Vr.p, VtB.p, r, r, s);
         }
@@ -443,8 +483,9 @@ void randomized(const svdb_matrix* A, uint64_t target_rank, uint64_t n_oversampl
         SVDB_CUDA(cudaMemcpyAsync(S.p, sig.p, actual * 8, cudaMemcpyDeviceToDevice, s));
     }
     SVDB_CUDA(cudaEventRecord(e1, s));
-    int hflags = 0;
+    int hflags = 0, hjac = 0;
     SVDB_CUDA(cudaMemcpyAsync(&hflags, cx.flags.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    SVDB_CUDA(cudaMemcpyAsync(&hjac, jac_status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     SVDB_CUDA(cudaStreamSynchronize(s));
     float tot = 0.f;
     cudaEventElapsedTime(&tot, e0, e1);
@@ -458,6 +499,7 @@ void randomized(const svdb_matrix* A, uint64_t target_rank, uint64_t n_oversampl
         cudaEventDestroy(ev.second);
     }
     spmm_tma_check();
+    if (verbose) printf("SVD | Randomized | Jacobi sweeps on R: %d%s\n", hjac >> 8, (hjac & 2) ? " (limit)" : "");
     if (hflags & 2) throw Error(SVDB_ERR_LAS2, "randomized_svd: CholeskyQR broke down even with a shift");
 
     std::memset(rec, 0, sizeof(*rec));
