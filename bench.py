@@ -179,11 +179,13 @@ def profiled_traffic(name):
 
 
 def max_over_ranks(x, world):
+    """The slowest rank's time (replicas: every rank solves the same workload)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
