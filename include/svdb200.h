@@ -222,6 +222,14 @@ int svdb_opb_device_noalloc(const svdb_matrix* a, const double* d_x, double* d_y
 int svdb_opa_device(const svdb_matrix* a, const double* d_x, double* d_y, int transposed, int precision,
                     void* stream);
 
+/* Gram matrix of a tall dense matrix on device buffers: d_g (c x c) =
+ * X^T X for d_x (rows x c, row-major FP64).  SVDB_F64 sums in FP64 on the
+ * CUDA cores; SVDB_MIXED uses the tensor cores (3xTF32 products, FP32
+ * accumulation per block, FP64 across blocks; c <= 64), the form the first
+ * CholeskyQR pass of randomized_svd takes under SVDB_MIXED.  Synchronises
+ * `stream`.  No counterpart in the reference (its QR is nalgebra's). */
+int svdb_gram_device(const double* d_x, uint64_t rows, uint64_t c, double* d_g, int precision, void* stream);
+
 /* Device buffers come from the device's stream-ordered pool, which the
  * library keeps cached between calls; this returns the cached memory of the
  * current device to the driver (after a device synchronisation). */

@@ -25,6 +25,7 @@ void svd_adjoint(const svdb_matrix*, int64_t, const double*, const double*, cons
 void sddmm_device(const svdb_matrix*, const void*, const void*, int64_t, void*, int, cudaStream_t);
 void svd_flip(double*, int64_t, int64_t, double*, int64_t, int64_t, bool, bool);
 void release_cached_memory();
+void gram_device(const double*, int64_t, int, double*, int, cudaStream_t);
 void batch_create(const svdb_matrix*, const uint64_t*, const uint64_t*, uint64_t, uint64_t, uint64_t, uint64_t, int, int,
                   uint64_t, const svdb_batch_options&, svdb_batch**);
 void batch_run(svdb_batch*, svdb_rec*);
@@ -503,6 +504,14 @@ int svdb_randomized_svd_batch(const svdb_matrix* a, const uint64_t* col_offsets,
     st = svdb_batch_run(b, outs);
     svdb_batch_destroy(b);
     return st;
+}
+
+int svdb_gram_device(const double* d_x, uint64_t rows, uint64_t c, double* d_g, int precision, void* stream) {
+    return guarded([&] {
+        if (!d_x || !d_g) throw Error(SVDB_ERR_ARG, "null argument");
+        if (precision != SVDB_F64 && precision != SVDB_MIXED) throw Error(SVDB_ERR_ARG, "bad precision");
+        gram_device(d_x, (int64_t)rows, (int)c, d_g, precision, (cudaStream_t)stream);
+    });
 }
 
 int svdb_release_cached_memory(void) {

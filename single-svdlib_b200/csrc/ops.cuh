@@ -19,6 +19,12 @@ template <typename XT, typename OT>
 void spmm_dev(const DevCompressed& m, bool fp32, const XT* X, int l, OT* Y, cudaStream_t s);
 // Raises the error a TMA gather wait of an earlier SpMM recorded (synchronises).
 void spmm_tma_check();
+// X^T X on the tensor cores (gram_tc.cu): part gets one c x c FP64 partial per
+// block (gram_tc_blocks(rows) of them); gram_tc_check raises a recorded timeout.
+int gram_tc_launch(const double* X, int64_t rows, int c, double* part, int64_t part_cap, const int* cond,
+                   cudaStream_t s);
+int gram_tc_blocks(int64_t rows);
+void gram_tc_check();
 
 void datx(double a, const double* x, double* y, int64_t n, cudaStream_t s);  // y = a * x
 

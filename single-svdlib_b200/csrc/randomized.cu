@@ -28,6 +28,11 @@
 
 namespace svdb {
 
+static bool getenv_is(const char* name, const char* value) {
+    const char* e = getenv(name);
+    return e && std::strcmp(e, value) == 0;
+}
+
 static int nb(int64_t work, int threads, int per_sm = 16) {
     int64_t b = (work + threads - 1) / threads;
     return (int)std::max<int64_t>(1, std::min<int64_t>(b, (int64_t)device_props().sms * per_sm));
@@ -233,11 +238,25 @@ __global__ void k_take_cols(const double* __restrict__ X, int64_t rows, int c, i
 // ------------------------------------------------------ host helpers ----
 struct RandCtx {
     cudaStream_t s;
+    bool tensor_gram = false;  // first CholeskyQR pass on the tensor cores (SVDB_MIXED)
     int cmax = 0;
     DevBuf<double> part, G, R1, R2, R3, Ri, Rtmp, T;
     DevBuf<int> flags, shifted;
     int64_t part_cap = 0;
 };
+
+// G = X^T X on the tensor cores (3xTF32, FP32 accumulation; gram_tc.cu), the
+// CTA partials summed in FP64 in block order
+static void gram_tensor(RandCtx& cx, const double* X, int64_t rows, int c, double* G, const int* cond) {
+    const int nblk = gram_tc_blocks(rows);
+    if ((int64_t)nblk * c * c > cx.part_cap) {
+        cx.part_cap = (int64_t)nblk * c * c;
+        cx.part.alloc(cx.part_cap, cx.s);
+    }
+    gram_tc_launch(X, rows, c, cx.part.p, cx.part_cap, cond, cx.s);
+    k_gram_reduce<<<(c * c + 31) / 32, 32 * kRedSlices, 0, cx.s>>>(cx.part.p, nblk, c, G, cond);
+    SVDB_CHECK_LAUNCH();
+}
 
 static void gram(RandCtx& cx, const double* X, int64_t rows, int c, double* G, const int* cond) {
     if (c > 128) throw Error(SVDB_ERR_UNSUPPORTED, "randomized_svd: more than 128 sample columns");
@@ -302,8 +321,10 @@ static void cholesky_qr(RandCtx& cx, double* X, int64_t rows, int c, double* Rou
     if ((int64_t)cx.T.n < rows * c) cx.T.alloc(rows * c, s);
     double* T = cx.T.p;
     SVDB_CUDA(cudaMemsetAsync(cx.shifted.p, 0, sizeof(int), s));
-    // pass 1: X -> T
-    gram(cx, X, rows, c, cx.G.p, nullptr);
+    // pass 1: X -> T (its Gram on the tensor cores under SVDB_MIXED: only its R1
+    // has to be good enough for pass 2, which is FP64)
+    if (cx.tensor_gram && c <= 64) gram_tensor(cx, X, rows, c, cx.G.p, nullptr);
+    else gram(cx, X, rows, c, cx.G.p, nullptr);
     chol_inv(cx, cx.G.p, c, rows, cx.R1.p, nullptr);
     right_mul(X, rows, c, cx.Ri.p, c, c, T, s);
     // pass 2: T -> X
@@ -346,6 +367,21 @@ static double ms_since(std::chrono::steady_clock::time_point t0) {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
 
+// svdb_gram_device: G (c x c) = X^T X for a device X (rows x c, FP64)
+void gram_device(const double* X, int64_t rows, int c, double* G, int precision, cudaStream_t s) {
+    if (c < 1 || c > 128) throw Error(SVDB_ERR_UNSUPPORTED, "gram: 1..128 columns");
+    RandCtx cx;
+    cx.s = s;
+    if (precision == SVDB_MIXED) {
+        if (c > 64) throw Error(SVDB_ERR_UNSUPPORTED, "gram: the tensor-core form takes at most 64 columns");
+        gram_tensor(cx, X, rows, c, G, nullptr);
+    } else {
+        gram(cx, X, rows, c, G, nullptr);
+    }
+    SVDB_CUDA(cudaStreamSynchronize(s));
+    gram_tc_check();
+}
+
 void randomized(const svdb_matrix* A, uint64_t target_rank, uint64_t n_oversamples, uint64_t n_power_iters,
                 int normalizer, int mean_center, int has_seed, uint64_t seed, int verbose, const svdb_options& o,
                 svdb_rec* rec) {
@@ -368,6 +404,7 @@ void randomized(const svdb_matrix* A, uint64_t target_rank, uint64_t n_oversampl
 
     RandCtx cx;
     cx.s = s;
+    cx.tensor_gram = mixed && !getenv_is("SVDB_GRAM", "fp64");
     const int cmax = l;
     for (DevBuf<double>* b : {&cx.G, &cx.R1, &cx.R2, &cx.R3, &cx.Ri, &cx.Rtmp}) b->alloc((size_t)cmax * cmax, s);
     cx.flags.alloc(1, s);
@@ -499,6 +536,7 @@ void randomized(const svdb_matrix* A, uint64_t target_rank, uint64_t n_oversampl
         cudaEventDestroy(ev.second);
     }
     spmm_tma_check();
+    gram_tc_check();
     if (verbose) printf("SVD | Randomized | Jacobi sweeps on R: %d%s\n", hjac >> 8, (hjac & 2) ? " (limit)" : "");
     if (hflags & 2) throw Error(SVDB_ERR_LAS2, "randomized_svd: CholeskyQR broke down even with a shift");
 

@@ -107,3 +107,36 @@ def test_device_fp32_spmm_against_numpy(l, transpose, impl, monkeypatch):
     got = ty.cpu().numpy().astype(np.float64)
     scale = np.abs(ref).max()
     assert np.abs(got - ref).max() <= 2e-6 * scale
+
+
+@pytest.mark.parametrize("rows", [5, 31, 1000, 10007, 200000])
+@pytest.mark.parametrize("c", [1, 8, 33, 60, 64])
+def test_gram_device(rows, c):
+    """svdb_gram_device: X^T X on the tensor cores (SVDB_MIXED: 3xTF32 products,
+    FP32 accumulation per block, FP64 across blocks) within 2e-6 of the largest
+    entry, and in FP64 on the CUDA cores within 1e-12, against numpy."""
+    import torch
+    from single_svdlib import _abi
+    from single_svdlib._core import check
+    rng = np.random.default_rng(rows + c)
+    X = rng.standard_normal((rows, c)) * np.exp(rng.standard_normal(c))  # columns of different scales
+    ref = X.T @ X
+    tx = torch.from_numpy(X).cuda()
+    for prec, tol in ((1, 2e-6), (0, 1e-12)):
+        tg = torch.empty((c, c), dtype=torch.float64, device="cuda")
+        check(_abi.lib().svdb_gram_device(tx.data_ptr(), rows, c, tg.data_ptr(), prec, None))
+        got = tg.cpu().numpy()
+        assert np.abs(got - ref).max() <= tol * np.abs(ref).max(), (prec, np.abs(got - ref).max())
+
+
+def test_gram_device_empty_and_limits():
+    import torch
+    from single_svdlib import UnsupportedError, _abi
+    from single_svdlib._core import check
+    tx = torch.zeros((0, 4), dtype=torch.float64, device="cuda")
+    tg = torch.full((4, 4), 7.0, dtype=torch.float64, device="cuda")
+    check(_abi.lib().svdb_gram_device(tx.data_ptr() or 1, 0, 4, tg.data_ptr(), 1, None))
+    assert not tg.cpu().numpy().any()
+    big = torch.zeros((10, 65), dtype=torch.float64, device="cuda")
+    with pytest.raises(UnsupportedError):
+        check(_abi.lib().svdb_gram_device(big.data_ptr(), 10, 65, tg.data_ptr(), 1, None))
