@@ -29,6 +29,7 @@ namespace svdb {
 
 constexpr int kGtK = 32;                 // rows of X per stage (the MMA K dimension)
 constexpr int kGtThreads = 128;
+constexpr int64_t kGtChunk = 256;        // rows per CTA
 constexpr int kGtTileBytes = 128 * kGtK * 4;
 constexpr int kGtSmem = kGtTileBytes + (128 * 64 + 64 * 64) * 4;  // stage + epilogue staging
 // instruction descriptor: F32 accumulator, TF32 A and B, both K-major, N = 64, M = 128
@@ -189,14 +190,16 @@ __global__ void __launch_bounds__(kGtThreads) k_gram_tc(const double* __restrict
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 128;" ::"r"(tmem) : "memory");
 }
 
-// part must hold nblk * c * c doubles; returns nblk
+// A CTA sums at most kGtChunk rows in FP32 in tensor memory; the partials
+// of the CTAs are added in FP64.
+int gram_tc_blocks(int64_t rows) { return (int)std::max<int64_t>(1, (rows + kGtChunk - 1) / kGtChunk); }
+
+// part must hold gram_tc_blocks(rows) * c * c doubles; returns that count
 int gram_tc_launch(const double* X, int64_t rows, int c, double* part, int64_t part_cap, const int* cond,
                    cudaStream_t s) {
     if (c > 64 || c < 1) throw Error(SVDB_ERR_UNSUPPORTED, "tensor-core Gram: 1..64 columns");
-    const int sms = device_props().sms;
-    int64_t chunk = std::max<int64_t>(256, (rows + 3 * sms - 1) / (3 * sms));
-    chunk = (chunk + kGtK - 1) / kGtK * kGtK;
-    int nblk = (int)std::max<int64_t>(1, (rows + chunk - 1) / chunk);
+    const int64_t chunk = kGtChunk;
+    const int nblk = gram_tc_blocks(rows);
     if ((int64_t)nblk * c * c > part_cap) throw Error(SVDB_ERR_ARG, "tensor-core Gram: partial buffer too small");
     static bool attr = false;
     if (!attr) {
@@ -208,12 +211,7 @@ int gram_tc_launch(const double* X, int64_t rows, int c, double* part, int64_t p
     return nblk;
 }
 
-int gram_tc_blocks(int64_t rows) {
-    const int sms = device_props().sms;
-    int64_t chunk = std::max<int64_t>(256, (rows + 3 * sms - 1) / (3 * sms));
-    chunk = (chunk + kGtK - 1) / kGtK * kGtK;
-    return (int)std::max<int64_t>(1, (rows + chunk - 1) / chunk);
-}
+
 
 void gram_tc_check() {
     int e = 0;

@@ -113,8 +113,9 @@ def test_device_fp32_spmm_against_numpy(l, transpose, impl, monkeypatch):
 @pytest.mark.parametrize("c", [1, 8, 33, 60, 64])
 def test_gram_device(rows, c):
     """svdb_gram_device: X^T X on the tensor cores (SVDB_MIXED: 3xTF32 products,
-    FP32 accumulation per block, FP64 across blocks) within 2e-6 of the largest
-    entry, and in FP64 on the CUDA cores within 1e-12, against numpy."""
+    FP32 accumulation over at most 256 rows per block, FP64 across blocks)
+    within 1e-5 of the largest entry (256 FP32 additions: 256 * 2^-24 = 1.5e-5
+    at most), and in FP64 on the CUDA cores within 1e-12, against numpy."""
     import torch
     from single_svdlib import _abi
     from single_svdlib._core import check
@@ -122,7 +123,7 @@ def test_gram_device(rows, c):
     X = rng.standard_normal((rows, c)) * np.exp(rng.standard_normal(c))  # columns of different scales
     ref = X.T @ X
     tx = torch.from_numpy(X).cuda()
-    for prec, tol in ((1, 2e-6), (0, 1e-12)):
+    for prec, tol in ((1, 1e-5), (0, 1e-12)):
         tg = torch.empty((c, c), dtype=torch.float64, device="cuda")
         check(_abi.lib().svdb_gram_device(tx.data_ptr(), rows, c, tg.data_ptr(), prec, None))
         got = tg.cpu().numpy()
