@@ -9,16 +9,19 @@
 // restores orthogonality, and a breakdown still falls back to the shifted
 // pass.
 //
-// One CTA of 128 threads takes a chunk of rows.  A stage of 32 rows is
+// One CTA of 128 threads takes a chunk of rows (48 KB of shared memory and 128
+// TMEM columns, so four CTAs fit an SM).  A stage of 32 rows is
 // written to shared memory as the 128 x 32 K-major operand A = [H^T ; L^T]
 // (core matrices of 8 rows x 16 bytes, no swizzle: 128 bytes between the
 // core matrices along K, 1024 bytes between groups of 8 rows).  Per 8 rows of
 // K one thread issues two MMAs (M = 128, N = 64): D += A H and D2 += A L, so
 // D = [H^T H ; L^T H] and D2 = [H^T L ; L^T L] in 128 TMEM columns.  The
-// commit arrives on an mbarrier before the stage is overwritten.  At the end
-// each warp reads its 32 TMEM lanes (tcgen05.ld 32x32b) and the CTA writes
-// its FP64 partial D[i][j] + D[64+i][j] + D2[i][j]; the partials are summed in
-// block order by k_gram_reduce.  Waits give up after 2 s (g_gram_tc_err).
+// commit arrives on the stage's mbarrier; with two stages, the global loads of
+// the next 32 rows run while the previous MMAs execute.  At the end each warp
+// reads its 32 TMEM lanes (tcgen05.ld 32x32b), warps 2-3 hand D's rows 64..127
+// over through shared memory, and warps 0-1 write the CTA's FP64 partial
+// D[i][j] + D[64+i][j] + D2[i][j]; the partials are summed in block order by
+// k_gram_reduce.  Waits give up after 2 s (g_gram_tc_err).
 #include <algorithm>
 
 #include "device_common.cuh"
@@ -31,7 +34,7 @@ constexpr int kGtK = 32;                 // rows of X per stage (the MMA K dimen
 constexpr int kGtThreads = 128;
 constexpr int64_t kGtChunk = 256;        // rows per CTA
 constexpr int kGtTileBytes = 128 * kGtK * 4;
-constexpr int kGtSmem = kGtTileBytes + (128 * 64 + 64 * 64) * 4;  // stage + epilogue staging
+constexpr int kGtSmem = 2 * kGtTileBytes + 64 * 64 * 4;  // two stages + the epilogue exchange
 // instruction descriptor: F32 accumulator, TF32 A and B, both K-major, N = 64, M = 128
 constexpr uint32_t kGtIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
 __device__ int g_gram_tc_err;
@@ -80,15 +83,13 @@ __global__ void __launch_bounds__(kGtThreads) k_gram_tc(const double* __restrict
                                                         const int* __restrict__ cond) {
     if (cond && *cond == 0) return;
     extern __shared__ __align__(1024) unsigned char sm[];
-    unsigned char* tile = sm;
-    float* stD = reinterpret_cast<float*>(sm + kGtTileBytes);  // 128 x 64
-    float* stD2 = stD + 128 * 64;                               // 64 x 64 (rows 0..63 of D2)
+    float* xch = reinterpret_cast<float*>(sm + 2 * kGtTileBytes);  // 64 x 64: rows 64..127 of D
     __shared__ uint32_t s_tmem;
-    __shared__ __align__(8) uint64_t s_bar;
+    __shared__ __align__(8) uint64_t s_bar[2];
     __shared__ int s_failed;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int64_t r0 = blockIdx.x * chunk, r1 = min(rows, r0 + chunk);
-    if (gt_smem(sm) & 1023) {  // descriptors address 16-byte units; keep the stage on a 1 KB boundary
+    if (gt_smem(sm) & 1023) {  // descriptors address 16-byte units; keep the stages on a 1 KB boundary
         if (tid == 0) atomicOr(&g_gram_tc_err, 2);
         return;
     }
@@ -98,7 +99,8 @@ __global__ void __launch_bounds__(kGtThreads) k_gram_tc(const double* __restrict
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(gt_smem(&s_bar)) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(gt_smem(&s_bar[0])) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(gt_smem(&s_bar[1])) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         s_failed = 0;
     }
@@ -106,31 +108,46 @@ __global__ void __launch_bounds__(kGtThreads) k_gram_tc(const double* __restrict
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = s_tmem;
-    const uint32_t tile_a = gt_smem(tile);
-    uint32_t phase = 0;
-    bool first = true;
-    for (int64_t kb = r0; kb < r1; kb += kGtK) {
+    // Two stages: stage s lives in buffer s & 1; before it is rewritten, thread 0
+    // waits for the commit of stage s - 2 (the MMAs of stage s - 1 may still run).
+    const int nstage = (int)((r1 - r0 + kGtK - 1) / kGtK);
+    uint32_t uses[2] = {0, 0};  // commits per buffer so far (its phase parity)
+    for (int st = 0; st < nstage; ++st) {
+        const int buf = st & 1;
+        unsigned char* tile = sm + buf * kGtTileBytes;
+        const int64_t kb = r0 + (int64_t)st * kGtK;
         const int nk = (int)min((int64_t)kGtK, r1 - kb);
-        for (int t = tid; t < kGtK * 64; t += kGtThreads) {
-            const int k = t >> 6, col = t & 63;
-            float h = 0.f, lo = 0.f;
-            if (k < nk && col < c) {
-                const float x = (float)X[(kb + k) * c + col];
-                h = __uint_as_float(__float_as_uint(x) & 0xFFFFE000u);
-                lo = x - h;
-            }
+        double xv[kGtK * 64 / kGtThreads];
+#pragma unroll
+        for (int u = 0; u < kGtK * 64 / kGtThreads; ++u) {  // global loads first: they overlap the wait below
+            const int t = tid + u * kGtThreads, k = t >> 6, col = t & 63;
+            xv[u] = (k < nk && col < c) ? X[(kb + k) * c + col] : 0.0;
+        }
+        if (st >= 2) {
+            if (tid == 0 && !gt_wait(gt_smem(&s_bar[buf]), (uses[buf] - 1) & 1, 2000000000ull)) s_failed = 1;
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncthreads();
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            if (s_failed) break;
+        }
+#pragma unroll
+        for (int u = 0; u < kGtK * 64 / kGtThreads; ++u) {
+            const int t = tid + u * kGtThreads, k = t >> 6, col = t & 63;
+            const float x = (float)xv[u];
+            const float h = __uint_as_float(__float_as_uint(x) & 0xFFFFE000u);
             *reinterpret_cast<float*>(tile + gt_off(col, k)) = h;
-            *reinterpret_cast<float*>(tile + gt_off(64 + col, k)) = lo;
+            *reinterpret_cast<float*>(tile + gt_off(64 + col, k)) = x - h;
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         if (tid == 0) {
+            const uint32_t ta = gt_smem(tile);
 #pragma unroll
             for (int kk = 0; kk < kGtK / 8; ++kk) {
-                const uint64_t a = gt_desc(tile_a + kk * 256);             // rows 0..127, K 8kk .. 8kk+7
-                const uint64_t bl = gt_desc(tile_a + 8 * 1024 + kk * 256);  // rows 64..127 (the L part)
-                const uint32_t acc = (first && kk == 0) ? 0u : 1u;
+                const uint64_t a = gt_desc(ta + kk * 256);             // rows 0..127, K 8kk .. 8kk+7
+                const uint64_t bl = gt_desc(ta + 8 * 1024 + kk * 256);  // rows 64..127 (the L part)
+                const uint32_t acc = (st == 0 && kk == 0) ? 0u : 1u;
                 asm volatile(
                     "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
                     " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}" ::"r"(tmem),
@@ -143,46 +160,53 @@ __global__ void __launch_bounds__(kGtThreads) k_gram_tc(const double* __restrict
                     : "memory");
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                             gt_smem(&s_bar))
+                             gt_smem(&s_bar[buf]))
                          : "memory");
-            // the stage is overwritten next: wait for the MMAs that read it
-            if (!gt_wait(gt_smem(&s_bar), phase, 2000000000ull)) s_failed = 1;
         }
-        first = false;
-        phase ^= 1;
-        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncthreads();
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        if (s_failed) break;
+        ++uses[buf];
     }
-    if (!s_failed && r0 < r1) {
+    // the last commit covers every MMA issued before it
+    if (tid == 0 && !s_failed && nstage > 0) {
+        const int lb = (nstage - 1) & 1;
+        if (!gt_wait(gt_smem(&s_bar[lb]), (uses[lb] - 1) & 1, 2000000000ull)) s_failed = 1;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    double* out = part + (int64_t)blockIdx.x * c * c;
+    if (!s_failed && nstage > 0) {
+        // warp w holds TMEM lanes 32w .. 32w+31: D rows; warps 0-1 also D2 rows 0..63
         const uint32_t lanes = (uint32_t)(warp * 32) << 16;
         const int row = warp * 32 + lane;
-#pragma unroll 1
-        for (int q = 0; q < 4; ++q) {  // TMEM columns 32q .. 32q+31: D (q < 2), D2 (q >= 2)
-            uint32_t v[32];
-            SVDB_LD32(v, tmem + lanes + 32 * q);
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        uint32_t d[64];
+        SVDB_LD32(d, tmem + lanes + 0);
+        SVDB_LD32((d + 32), tmem + lanes + 32);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (warp >= 2) {
 #pragma unroll
-            for (int j = 0; j < 32; ++j) {
-                const int col = 32 * q + j;
-                if (col < 64) stD[row * 64 + col] = __uint_as_float(v[j]);
-                else if (row < 64) stD2[row * 64 + col - 64] = __uint_as_float(v[j]);
-            }
+            for (int j = 0; j < 64; ++j) xch[(row - 64) * 64 + j] = __uint_as_float(d[j]);
         }
         __syncthreads();
-        double* out = part + (int64_t)blockIdx.x * c * c;
-        for (int t = tid; t < c * c; t += kGtThreads) {
-            const int i = t / c, j = t % c;
-            out[t] = (double)stD[i * 64 + j] + (double)stD[(64 + i) * 64 + j] + (double)stD2[i * 64 + j];
+        if (warp < 2) {  // tcgen05.ld is warp-collective: every lane of warps 0-1 loads, rows < c write
+            uint32_t e[64];
+            SVDB_LD32(e, tmem + lanes + 64);
+            SVDB_LD32((e + 32), tmem + lanes + 96);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (row < c) {
+#pragma unroll
+                for (int j = 0; j < 64; ++j)
+                    if (j < c)
+                        out[row * c + j] = (double)__uint_as_float(d[j]) + (double)xch[row * 64 + j] +
+                                           (double)__uint_as_float(e[j]);
+            }
         }
-    } else if (r0 >= r1) {
-        double* out = part + (int64_t)blockIdx.x * c * c;
+    } else if (!s_failed) {
         for (int t = tid; t < c * c; t += kGtThreads) out[t] = 0.0;
     }
     if (s_failed && tid == 0) {
         atomicOr(&g_gram_tc_err, 1);
-        gt_wait(gt_smem(&s_bar), phase ^ 1, 100000000ull);  // give the MMAs in flight a last chance to land
+        for (int bq = 0; bq < 2; ++bq)  // give the MMAs in flight a last chance to land
+            if (uses[bq]) gt_wait(gt_smem(&s_bar[bq]), (uses[bq] - 1) & 1, 100000000ull);
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
