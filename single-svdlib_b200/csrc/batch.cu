@@ -506,7 +506,8 @@ static void right_mul(svdb_batch& B, const TI* X, SubLayout L, const double* S, 
 static void chol(svdb_batch& B, SubLayout L, double* R, const int* cond) {
     const int c = (int)B.l;
     const size_t smem = 2 * (size_t)c * c * sizeof(double);
-    if (smem > 48 * 1024)
+    // chol_inv_body also holds about 1 KB of static shared memory
+    if (smem > 40 * 1024)
         SVDB_CUDA(cudaFuncSetAttribute(k_b_chol_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_b_chol_inv<<<(unsigned)B.count, 256, smem, B.s>>>(B.G.p, c, L, B.coff.p, R, B.Ri.p, B.flags.p, B.shifted.p,
                                                          cond);
@@ -570,7 +571,7 @@ static void enqueue(svdb_batch& B) {
     cols_product<T, double>(B, Y, B.Bt.p);  // B^T = A^T Q (FP64)
     cholesky_qr<double>(B, B.Bt.p, LZ, true);
     const size_t smem = ((size_t)c * (c + 1) + (size_t)(c + 1) * (c + 1) + (c + 1)) * sizeof(double);
-    if (smem > 48 * 1024)
+    if (smem > 40 * 1024)  // jacobi_svd_body keeps a little static shared memory too
         SVDB_CUDA(cudaFuncSetAttribute(k_b_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_b_jacobi<<<(unsigned)B.count, 512, smem, B.s>>>(B.Rout.p, c, B.Ur.p, B.Vr.p, B.sig.p, B.jstat.p);
     SVDB_CHECK_LAUNCH();

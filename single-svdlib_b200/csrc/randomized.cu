@@ -304,7 +304,8 @@ static void right_mul(const double* X, int64_t rows, int c, const double* S, int
 static void chol_inv(RandCtx& cx, const double* G, int c, int64_t rows, double* R, const int* cond) {
     const bool two = 2 * (size_t)c * c * sizeof(double) <= 200 * 1024;
     const size_t smem = (two ? 2 : 1) * (size_t)c * c * sizeof(double);
-    if (smem > 48 * 1024)
+    // chol_inv_body also holds about 1 KB of static shared memory
+    if (smem > 40 * 1024)
         SVDB_CUDA(cudaFuncSetAttribute(k_chol_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     // shifted CholeskyQR: shift = 11 (rows c + c (c + 1)) u ||X||_F^2, ||X||_F^2 = trace(G)
     const double shift_scale = 11.0 * ((double)rows * c + (double)c * (c + 1)) * 1.1102230246251565e-16;

@@ -7,6 +7,7 @@
 // sees the crate's exact operation sequence (s*z[i] + c*f, c*z[i] - s*f,
 // unfused), so Z is bit-identical to the sequential loop's.
 #include <algorithm>
+#include <string>
 
 #include "device_common.cuh"
 #include "ops.cuh"
@@ -32,6 +33,52 @@ __global__ void __launch_bounds__(128) k_rot_apply(double* __restrict__ z, int64
         *zi1 = add_rn(mul_rn(s, a), mul_rn(c, f));
         *zi = sub_rn(mul_rn(c, a), mul_rn(s, f));
     }
+}
+
+// The same in shared memory: block b owns rows b*ROWS .. +ROWS of Z, stored
+// as zs[i * ROWS + local row]; the rotation list is staged in chunks that
+// every thread reads (a broadcast).  Within a QL sweep the rotations walk i
+// downwards, and rotation i - 1 reads as f the z[i] that rotation i has just
+// written: it is handed over in a register.  Each element still sees the
+// crate's operations in order (unfused), so Z is bit-identical.
+constexpr int kRotChunk = 1024;
+__global__ void __launch_bounds__(64) k_rot_apply_smem(double* __restrict__ z, int64_t js,
+                                                       const int32_t* __restrict__ ri,
+                                                       const double* __restrict__ rc,
+                                                       const double* __restrict__ rs, int64_t nrot) {
+    extern __shared__ double zs[];  // js x blockDim.x
+    __shared__ int32_t sri[kRotChunk];
+    __shared__ double src_[kRotChunk], srs[kRotChunk];
+    const int rows = blockDim.x, tid = threadIdx.x;
+    const int64_t k = blockIdx.x * (int64_t)rows + tid;
+    for (int64_t i = 0; i < js; ++i) zs[i * rows + tid] = (i == k) ? 1.0 : 0.0;
+    int64_t prev = -2;
+    double carry = 0.0;
+    for (int64_t t0 = 0; t0 < nrot; t0 += kRotChunk) {
+        const int cnt = (int)min((int64_t)kRotChunk, nrot - t0);
+        __syncthreads();
+        for (int u = tid; u < cnt; u += rows) {
+            sri[u] = ri[t0 + u];
+            src_[u] = rc[t0 + u];
+            srs[u] = rs[t0 + u];
+        }
+        __syncthreads();
+        for (int u = 0; u < cnt; ++u) {
+            const int64_t i = sri[u];
+            const double c = src_[u], s = srs[u];
+            const double f = (i + 1 == prev) ? carry : zs[(i + 1) * rows + tid];
+            const double a = zs[i * rows + tid];
+            const double hi = add_rn(mul_rn(s, a), mul_rn(c, f));
+            const double lo = sub_rn(mul_rn(c, a), mul_rn(s, f));
+            zs[(i + 1) * rows + tid] = hi;
+            zs[i * rows + tid] = lo;
+            carry = lo;
+            prev = i;
+        }
+    }
+    __syncthreads();
+    if (k < js)
+        for (int64_t i = 0; i < js; ++i) z[i * js + k] = zs[i * rows + tid];
 }
 
 // C (d x js) row-major.  The final Z after imtql2's column sort is
@@ -136,7 +183,22 @@ static int nblk(int64_t work, int threads) {
 
 void rot_apply(double* z, int64_t js, const int32_t* ri, const double* rc, const double* rs, int64_t nrot,
                cudaStream_t s) {
-    k_rot_apply<<<(unsigned)((js + 127) / 128), 128, 0, s>>>(z, js, ri, rc, rs, nrot);
+    // rows per block in shared memory: as many as fit next to the staged rotations
+    const size_t avail = 200 * 1024;
+    int rows = 64;
+    while (rows >= 16 && (size_t)js * rows * sizeof(double) > avail) rows >>= 1;
+    if (rows >= 16) {
+        const size_t smem = (size_t)js * rows * sizeof(double);
+        // the kernel also holds 20 KB of static shared memory: always raise the dynamic limit
+        SVDB_CUDA(cudaFuncSetAttribute(k_rot_apply_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_rot_apply_smem<<<(unsigned)((js + rows - 1) / rows), rows, smem, s>>>(z, js, ri, rc, rs, nrot);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess)
+            throw Error(SVDB_ERR_CUDA, "k_rot_apply_smem(js=" + std::to_string(js) + ", rows=" + std::to_string(rows) +
+                                           ", smem=" + std::to_string(smem) + "): " + cudaGetErrorString(e));
+    } else {
+        k_rot_apply<<<(unsigned)((js + 127) / 128), 128, 0, s>>>(z, js, ri, rc, rs, nrot);
+    }
     SVDB_CHECK_LAUNCH();
 }
 
