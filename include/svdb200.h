@@ -271,7 +271,11 @@ int svdb_las2_plan(uint64_t nrows, uint64_t ncols, uint64_t nnz, uint64_t dimens
 /* randomized::randomized_svd (src/randomized/mod.rs:24-199).  has_seed = 0
  * means seed None (the crate then seeds with 0, :304-307).  Omega is drawn on
  * the device from a counter-based generator keyed by the seed, or taken from
- * opts->omega.  mean_center = 1 returns SVDB_ERR_UNSUPPORTED. */
+ * opts->omega.  mean_center = 1 factorises the centred matrix A - 1 mu^T,
+ * mu the column means of the (masked) matrix (src/lanczos/masked.rs:240-263),
+ * through the exact products A X - 1 (mu^T X) and A^T Y - mu (1^T Y); the
+ * crate's own adjusted products (masked.rs:496-509, 793-809) do not equal
+ * these.  With mean_center the sample width is at most 128 columns. */
 int svdb_randomized_svd(const svdb_matrix* a, uint64_t target_rank, uint64_t n_oversamples,
                         uint64_t n_power_iters, int normalizer, int mean_center, int has_seed, uint64_t seed,
                         int verbose, const svdb_options* opts, svdb_rec* out);

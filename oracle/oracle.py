@@ -87,7 +87,7 @@ def lib():
         L.orc_masked_dense.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64, u64, u64, f64, u8, C.c_int,
                                        f64, C.c_uint64, f64, C.c_int]
         L.orc_randomized.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64, u64, u64, f64, C.c_void_p,
-                                     C.c_uint64, C.c_uint64, C.c_uint64, C.c_int, f64, C.c_int,
+                                     C.c_uint64, C.c_uint64, C.c_uint64, C.c_int, f64, C.c_int, C.c_int,
                                      C.POINTER(_RandOut)]
         L.orc_rand_free.argtypes = [C.POINTER(_RandOut)]
         _lib = L
@@ -237,14 +237,14 @@ def masked_dense(A, mask, op, X, compat_d3=False):
 
 
 def randomized(A, target_rank, n_oversamples, n_power_iters, normalizer="QR", omega=None, mask=None,
-               compat_d3=False):
+               compat_d3=False, mean_center=False):
     """Randomized SVD on the masked view (all columns when mask is None); omega is n_masked x l row-major."""
     mk = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
     out = _RandOut()
     rc = lib().orc_randomized(A["nrows"], A["ncols"], len(A["indices"]), _u64(A["indptr"]), _u64(A["indices"]),
                               _f64(A["data"]), mk.ctypes.data if mk is not None else None, target_rank,
                               n_oversamples, n_power_iters, {"QR": 0, "LU": 1, "None": 2}[normalizer],
-                              _f64(omega), int(compat_d3), C.byref(out))
+                              _f64(omega), int(compat_d3), int(mean_center), C.byref(out))
     if rc:
         raise OracleError(rc, lib().orc_last_error().decode())
     try:

@@ -1415,11 +1415,47 @@ static double wall() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
+// compute_column_means (masked.rs:240-263): sums of the masked columns over
+// the rows, times 1/nrows
+static std::vector<double> column_means(const MaskedOp& M) {
+    const Compressed* a = M.a;
+    std::vector<double> mu(M.ncols(), 0.0);
+    for (size_t i = 0; i < a->nmajor; ++i)
+        for (uint64_t j = a->ptr[i]; j < a->ptr[i + 1]; ++j) {
+            int64_t mc = M.o2m[a->idx[j]];
+            if (mc >= 0) mu[(size_t)mc] += a->val[j];
+        }
+    const double rc = 1.0 / (double)a->nmajor;
+    for (double& v : mu) v *= rc;
+    return mu;
+}
+
+// Products of the centred matrix A - 1 mu^T (mean_center, mod.rs:46-53), by
+// the rank-1 corrections A X - 1 (mu^T X) and A^T Y - mu (1^T Y).  The crate's
+// own adjustments (masked.rs:496-509, 793-809) differ from this algebra.
+static void center_rows(DMatrix& y, const DMatrix& x, const std::vector<double>& mu) {
+    for (size_t c = 0; c < y.c; ++c) {
+        double t = 0.0;
+        for (size_t j = 0; j < mu.size(); ++j) t += mu[j] * x(j, c);
+        for (size_t i = 0; i < y.r; ++i) y(i, c) -= t;
+    }
+}
+static void center_cols(DMatrix& z, const DMatrix& y, const std::vector<double>& mu) {
+    for (size_t c = 0; c < z.c; ++c) {
+        double t = 0.0;
+        for (size_t i = 0; i < y.r; ++i) t += y(i, c);
+        for (size_t j = 0; j < z.r; ++j) z(j, c) -= mu[j] * t;
+    }
+}
+
 // normalizer: 0 = QR, 1 = LU (column normalisation), 2 = None
 static RandResult randomized_svd(const MaskedOp& M, size_t target_rank, size_t n_oversamples, size_t n_power_iters,
-                                 int normalizer, const double* omega_rowmajor, bool compat_d3) {
+                                 int normalizer, const double* omega_rowmajor, bool compat_d3,
+                                 bool mean_center = false) {
     RandResult R;
     size_t m = M.nrows(), n = M.ncols();
+    std::vector<double> mu;
+    if (mean_center) mu = column_means(M);
     size_t rank = std::min(target_rank, std::min(m, n));
     size_t l = rank + n_oversamples;
     DMatrix omega(n, l);
@@ -1429,16 +1465,19 @@ static RandResult randomized_svd(const MaskedOp& M, size_t target_rank, size_t n
     double t = wall();
     auto lap = [&](double& acc) { double now = wall(); acc += now - t; t = now; };
     masked_multiply_with_dense(M, omega, y, false, compat_d3);
+    if (mean_center) center_rows(y, omega, mu);
     lap(R.t_sparse);
     if (n_power_iters > 0) {
         DMatrix z;
         for (size_t it = 0; it < n_power_iters; ++it) {
             masked_multiply_with_dense(M, y, z, true, compat_d3);
+            if (mean_center) center_cols(z, y, mu);
             lap(R.t_sparse);
             if (normalizer == 0) z = thin_q(z);
             else if (normalizer == 1) normalize_columns(z);
             lap(R.t_fixed);
             masked_multiply_with_dense(M, z, y, false, compat_d3);
+            if (mean_center) center_rows(y, z, mu);
             lap(R.t_sparse);
             if (normalizer == 0) y = thin_q(y);
             else if (normalizer == 1) normalize_columns(y);
@@ -1449,6 +1488,13 @@ static RandResult randomized_svd(const MaskedOp& M, size_t target_rank, size_t n
     lap(R.t_rows);
     DMatrix B;
     masked_multiply_transposed_by_dense(M, Q, B);
+    if (mean_center) {  // B = Q^T (A - 1 mu^T): row c of B loses (1^T Q e_c) mu^T
+        for (size_t c = 0; c < B.r; ++c) {
+            double t = 0.0;
+            for (size_t i = 0; i < Q.r; ++i) t += Q(i, c);
+            for (size_t j = 0; j < B.c; ++j) B(c, j) -= t * mu[j];
+        }
+    }
     lap(R.t_sparse);
     DMatrix Ub, Vt;
     std::vector<double> sig;
@@ -1705,7 +1751,8 @@ void orc_rand_free(orc_rand_out* o) {
 
 int orc_randomized(uint64_t nrows, uint64_t ncols, uint64_t nnz, const uint64_t* ptr, const uint64_t* idx,
                    const double* val, const uint8_t* mask, uint64_t target_rank, uint64_t n_oversamples,
-                   uint64_t n_power_iters, int normalizer, const double* omega, int compat_d3, orc_rand_out* out) {
+                   uint64_t n_power_iters, int normalizer, const double* omega, int compat_d3, int mean_center,
+                   orc_rand_out* out) {
     std::memset(out, 0, sizeof(*out));
     try {
         orc::Compressed cm;
@@ -1717,7 +1764,7 @@ int orc_randomized(uint64_t nrows, uint64_t ncols, uint64_t nnz, const uint64_t*
         if (mask) mk.assign(mask, mask + ncols);
         orc::MaskedOp M(&cm, mk.data());
         orc::RandResult r = orc::randomized_svd(M, target_rank, n_oversamples, n_power_iters, normalizer, omega,
-                                                compat_d3 != 0);
+                                                compat_d3 != 0, mean_center != 0);
         out->d = r.d; out->m = r.m; out->n = r.n;
         out->u = dup_vec(r.u); out->s = dup_vec(r.s); out->vt = dup_vec(r.vt);
         out->t_sparse = r.t_sparse; out->t_rows = r.t_rows; out->t_fixed = r.t_fixed;

@@ -235,6 +235,73 @@ __global__ void k_take_cols(const double* __restrict__ X, int64_t rows, int c, i
         Out[t] = X[(t / cout) * c + t % cout];
 }
 
+// ------------------------------------------------------------ centring ----
+// Products of the centred matrix A - 1 mu^T, mu the column means
+// (compute_column_means, masked.rs:240-263), as A X - 1 (mu^T X) and
+// A^T Y - mu (1^T Y).  mu comes from the column-major copy, one warp per
+// column with a fixed lane order.
+__global__ void k_major_means(const int64_t* __restrict__ ptr, const double* __restrict__ val, int64_t nmajor,
+                              double inv, double* __restrict__ mu) {
+    const int lane = threadIdx.x & 31;
+    const int64_t w0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t j = w0; j < nmajor; j += nw) {
+        double acc = 0.0;
+        for (int64_t k = ptr[j] + lane; k < ptr[j + 1]; k += 32) acc += val[k];
+#pragma unroll
+        for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) mu[j] = acc * inv;
+    }
+}
+// part[b][j] = sum over the rows of chunk b of w[r] X[r][j] (w = 1 when null).
+// 32 x 8 threads: x walks the columns, y the rows; the y partials are added
+// in y order.
+constexpr int kCsCols = 128;
+__global__ void __launch_bounds__(256) k_wcolsum_part(const double* __restrict__ X, int64_t rows, int c,
+                                                      const double* __restrict__ w, int64_t chunk,
+                                                      double* __restrict__ part) {
+    __shared__ double sh[8][kCsCols];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int64_t r0 = blockIdx.x * chunk, r1 = std::min<int64_t>(rows, r0 + chunk);
+    double acc[kCsCols / 32];
+#pragma unroll
+    for (int q = 0; q < kCsCols / 32; ++q) acc[q] = 0.0;
+    for (int64_t r = r0 + ty; r < r1; r += 8) {
+        const double wr = w ? w[r] : 1.0;
+#pragma unroll
+        for (int q = 0; q < kCsCols / 32; ++q) {
+            const int j = tx + 32 * q;
+            if (j < c) acc[q] = fma(wr, X[r * c + j], acc[q]);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < kCsCols / 32; ++q) sh[ty][tx + 32 * q] = acc[q];
+    __syncthreads();
+    for (int j = threadIdx.x; j < c; j += blockDim.x) {
+        double t = 0.0;
+#pragma unroll
+        for (int y = 0; y < 8; ++y) t += sh[y][j];
+        part[(int64_t)blockIdx.x * c + j] = t;
+    }
+}
+// t[j] = sum of part[b][j] in block order
+__global__ void k_colsum_total(const double* __restrict__ part, int nblocks, int c, double* __restrict__ t) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < c; j += gridDim.x * blockDim.x) {
+        double acc = 0.0;
+        for (int b = 0; b < nblocks; ++b) acc += part[(int64_t)b * c + j];
+        t[j] = acc;
+    }
+}
+// Y[r][j] -= a[r] t[j] (a = 1 when null)
+__global__ void k_rank1_sub(double* __restrict__ Y, int64_t rows, int c, const double* __restrict__ a,
+                            const double* __restrict__ t) {
+    const int64_t total = rows * c;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = i / c;
+        Y[i] -= (a ? a[r] : 1.0) * t[i - r * c];
+    }
+}
+
 // ------------------------------------------------------ host helpers ----
 struct RandCtx {
     cudaStream_t s;
@@ -386,7 +453,6 @@ void gram_device(const double* X, int64_t rows, int c, double* G, int precision,
 void randomized(const svdb_matrix* A, uint64_t target_rank, uint64_t n_oversamples, uint64_t n_power_iters,
                 int normalizer, int mean_center, int has_seed, uint64_t seed, int verbose, const svdb_options& o,
                 svdb_rec* rec) {
-    if (mean_center) throw Error(SVDB_ERR_UNSUPPORTED, "randomized_svd: mean_center is not provided");
     cudaStream_t s = o.stream ? (cudaStream_t)o.stream : A->stream;
     const bool mixed = o.precision == SVDB_MIXED;
     const int64_t m = A->nrows, n = A->ncols;
@@ -449,9 +515,35 @@ void randomized(const svdb_matrix* A, uint64_t target_rank, uint64_t n_oversampl
         return c;
     };
 
+    // mean_center: Out = A X - 1 (mu^T X) for Out = A X (m rows), and
+    // Out = A^T X - mu (1^T X) for Out = A^T X (n rows)
+    DevBuf<double> mu, csum_part, csum;
+    int csum_blocks = 1;
+    if (mean_center) {
+        if (l > kCsCols) throw Error(SVDB_ERR_UNSUPPORTED, "randomized_svd: mean_center takes at most 128 sample columns");
+        mu.alloc(std::max<int64_t>(n, 1), s);
+        k_major_means<<<nb(n * 32, 256), 256, 0, s>>>(Acsc.ptr.p, Acsc.val.p, n, m > 0 ? 1.0 / (double)m : 0.0, mu.p);
+        SVDB_CHECK_LAUNCH();
+        csum_blocks = (int)std::max<int64_t>(1, std::min<int64_t>((std::max(m, n) + 255) / 256,
+                                                                 (int64_t)device_props().sms * 4));
+        csum_part.alloc((size_t)csum_blocks * l, s);
+        csum.alloc(l, s);
+    }
+    auto center = [&](const double* X, int64_t xrows, int c, double* Out, int64_t orows, bool out_is_rows) {
+        if (!mean_center) return;
+        const int64_t chunk = (xrows + csum_blocks - 1) / csum_blocks;
+        k_wcolsum_part<<<csum_blocks, 256, 0, s>>>(X, xrows, c, out_is_rows ? mu.p : nullptr, chunk, csum_part.p);
+        SVDB_CHECK_LAUNCH();
+        k_colsum_total<<<1, 128, 0, s>>>(csum_part.p, csum_blocks, c, csum.p);
+        SVDB_CHECK_LAUNCH();
+        k_rank1_sub<<<nb(orows * c, 256), 256, 0, s>>>(Out, orows, c, out_is_rows ? nullptr : mu.p, csum.p);
+        SVDB_CHECK_LAUNCH();
+    };
+
     if (verbose) printf("SVD | Randomized | Multiplying m with omega matrix....\n");
     DevBuf<double> Y(std::max<int64_t>(m * l, 1), s);
     spmm(Acsr, Om.p, l, Y.p);
+    center(Om.p, n, l, Y.p, m, true);
     int c = l;
     if (verbose) printf("SVD | Randomized | Multiplication done, took: %.3f ms of total running time\n", ms_since(t0));
     if (verbose) printf("SVD | Randomized | Starting power iterations....\n");
@@ -461,9 +553,11 @@ void randomized(const svdb_matrix* A, uint64_t target_rank, uint64_t n_oversampl
                    (unsigned long long)it, ms_since(t0));
         DevBuf<double> Z(std::max<int64_t>(n * c, 1), s);
         spmm(Acsc, Y.p, c, Z.p);
+        center(Y.p, m, c, Z.p, n, false);
         c = normalize(Z, n, c);
         DevBuf<double> Y2(std::max<int64_t>(m * c, 1), s);
         spmm(Acsr, Z.p, c, Y2.p);
+        center(Z.p, n, c, Y2.p, m, true);
         Y = std::move(Y2);
         c = normalize(Y, m, c);
         if (verbose)
@@ -474,6 +568,7 @@ void randomized(const svdb_matrix* A, uint64_t target_rank, uint64_t n_oversampl
     // B^T = A^T Q (n x c)
     DevBuf<double> Bt(std::max<int64_t>(n * c, 1), s);
     spmm(Acsc, Y.p, c, Bt.p);
+    center(Y.p, m, c, Bt.p, n, false);
     if (verbose) printf("SVD | Randomized | Transposed Matrix Multiplication %.3f ms\n", ms_since(t0));
 
     // SVD(B), B = Bt^T (c x n).  r = min(c, n).

@@ -86,8 +86,46 @@ def test_small_wide_and_rank_edge_cases():
     got = randomized.randomized_svd(upload("csr", A), 5, 10, 2, PIN.QR, False, 3, False)
     truth = np.linalg.svd(M.to_scipy(A).toarray(), compute_uv=False)[:5]
     np.testing.assert_allclose(got.s, truth, rtol=1e-8)
-    with pytest.raises(UnsupportedError):
-        randomized.randomized_svd(upload("csr", A), 3, 2, 1, PIN.QR, True, 3, False)
+
+
+@pytest.mark.parametrize("fmt", ["csr", "csc", "masked"])
+@pytest.mark.parametrize("norm", ["QR", "LU"])
+def test_mean_center_parity_with_checker(fmt, norm):
+    # A - 1 mu^T through the rank-1 corrected products, same Omega as the checker
+    A = M.uniform(350, 140, 0.15, 61, low=0.0, high=4.0)
+    mask = (np.random.default_rng(8).random(140) < 0.7).astype(np.uint8) if fmt == "masked" else None
+    nc = int(mask.sum()) if mask is not None else 140
+    om = M.omega(nc, 16, 6)
+    mat = MaskedCSRMatrix(upload("csr", A), mask) if mask is not None else upload(fmt, A)
+    got = randomized.randomized_svd(mat, 10, 6, 2, getattr(PIN, norm), True, 3, False, omega=om)
+    ref = O.randomized(A, 10, 6, 2, norm, omega=om, mask=mask, mean_center=True)
+    np.testing.assert_allclose(got.s, ref["s"], rtol=1e-10 if norm == "QR" else 1e-7)
+    assert np.all(subspace_cos(got.u[:, :4], ref["u"][:, :4]) > 1 - 1e-8)
+    assert np.all(subspace_cos(got.vt[:4].T, ref["vt"][:4].T) > 1 - 1e-8)
+    # U spans columns of the centred matrix: every column of U sums to zero
+    assert np.max(np.abs(got.u.sum(0))) < 1e-10 * np.sqrt(350)
+
+
+def test_mean_center_matches_dense_centred_svd():
+    # sketch as wide as the matrix: the exact SVD of A - 1 mu^T, in both precisions
+    A = M.lowrank_plus_noise(600, 90, 6, 1e-2, 62, density=0.4)
+    Ad = M.to_scipy(A).toarray() + 0.0
+    U, s, Vt = np.linalg.svd(Ad - Ad.mean(0), full_matrices=False)
+    got = randomized.randomized_svd(upload("csr", A), 6, 84, 1, PIN.QR, True, 5, False)
+    np.testing.assert_allclose(got.s, s[:6], rtol=1e-10)
+    assert np.all(subspace_cos(got.vt.T, Vt[:6].T) > 1 - 1e-10)
+    mix = randomized.randomized_svd(upload("csr", A), 6, 84, 1, PIN.QR, True, 5, False, precision="mixed")
+    assert np.max(np.abs(mix.s - s[:6]) / s[:6]) < 1e-5
+
+
+def test_mean_center_limits():
+    A = M.uniform(400, 300, 0.05, 63)
+    with pytest.raises(UnsupportedError):  # sample width above 128 columns
+        randomized.randomized_svd(upload("csr", A), 100, 40, 1, PIN.QR, True, 3, False)
+    # a constant column has zero variance: centring removes it exactly
+    Z = M.dense(np.tile(np.arange(1.0, 6.0), (40, 1)))
+    got = randomized.randomized_svd(upload("csr", Z), 3, 2, 1, PIN.QR, True, 3, False)
+    assert np.all(np.abs(got.s) < 1e-12)
 
 
 def test_rank_deficient_input_takes_the_shifted_qr():

@@ -183,6 +183,25 @@ def test_randomized_checker_power_iterations_and_d3():
     assert e3_d3 > 2 * e3
 
 
+@pytest.mark.parametrize("masked", [False, True])
+def test_randomized_checker_mean_center_is_the_centred_svd(masked):
+    # mean_center (randomized/mod.rs:46-53, column means masked.rs:240-263): with a
+    # sketch as wide as the matrix the result is the exact SVD of A - 1 mu^T
+    A = M.uniform(120, 40, 0.3, 17, low=0.5, high=3.0)
+    mask = (np.arange(40) % 4 != 1).astype(np.uint8) if masked else None
+    Ad = M.to_scipy(A).toarray()
+    if masked:
+        Ad = Ad[:, mask.astype(bool)]
+    nc = Ad.shape[1]
+    U, s, Vt = np.linalg.svd(Ad - Ad.mean(0), full_matrices=False)
+    r = O.randomized(A, 8, nc - 8, 1, "QR", omega=M.omega(nc, nc, 4), mask=mask, mean_center=True)
+    np.testing.assert_allclose(r["s"], s[:8], rtol=1e-12)
+    np.testing.assert_allclose(np.abs(np.sum(r["u"] * U[:, :8], 0)), 1.0, atol=1e-12)
+    # uncentred, the column means dominate the leading singular value
+    r0 = O.randomized(A, 8, nc - 8, 1, "QR", omega=M.omega(nc, nc, 4), mask=mask)
+    assert r0["s"][0] > 2 * r["s"][0]
+
+
 def test_poisson_workload_fixture_shape():
     f = FIX["poisson_5000x2000_seed42_dim10"]
     A = M.poisson_rows(5000, 2000, 20, 42)
