@@ -194,6 +194,21 @@ int svdb_multiply_with_dense(const svdb_matrix* a, const double* dense, uint64_t
 /* SMat::multiply_transposed_by_dense (masked.rs:616-733): result (l x ncols) = Q^T A, Q: nrows x l. */
 int svdb_multiply_transposed_by_dense(const svdb_matrix* a, const double* q, uint64_t q_cols, double* result);
 
+/* The column means of the (masked) matrix, ncols values: column sums over
+ * the rows times 1/nrows (masked.rs:240-263, compute_column_means). */
+int svdb_column_means(const svdb_matrix* a, double* means);
+/* SMat::multiply_with_dense_centered (src/utils.rs:29): products of the
+ * centred matrix A - 1 means^T (means: ncols values), result = A X - 1 (means^T X)
+ * or, when transpose_self, A^T X - means (1^T X).  The crate's masked version
+ * (masked.rs:473-614) subtracts other terms; this is the exact product. */
+int svdb_multiply_with_dense_centered(const svdb_matrix* a, const double* dense, uint64_t dense_cols,
+                                      const double* means, double* result, int transpose_self);
+/* SMat::multiply_transposed_by_dense_centered (src/utils.rs:32): result
+ * (l x ncols) = Q^T (A - 1 means^T); the crate's masked version is
+ * masked.rs:735-874. */
+int svdb_multiply_transposed_by_dense_centered(const svdb_matrix* a, const double* q, uint64_t q_cols,
+                                               const double* means, double* result);
+
 /* multiply_with_dense on device buffers: d_result = A d_dense (transpose_self
  * = 0, d_dense ncols x l) or A^T d_dense (nrows x l), row-major, enqueued on
  * `stream` (cudaStream_t, NULL = the handle's stream) without synchronising.
@@ -275,7 +290,7 @@ int svdb_las2_plan(uint64_t nrows, uint64_t ncols, uint64_t nnz, uint64_t dimens
  * mu the column means of the (masked) matrix (src/lanczos/masked.rs:240-263),
  * through the exact products A X - 1 (mu^T X) and A^T Y - mu (1^T Y); the
  * crate's own adjusted products (masked.rs:496-509, 793-809) do not equal
- * these.  With mean_center the sample width is at most 128 columns. */
+ * these. */
 int svdb_randomized_svd(const svdb_matrix* a, uint64_t target_rank, uint64_t n_oversamples,
                         uint64_t n_power_iters, int normalizer, int mean_center, int has_seed, uint64_t seed,
                         int verbose, const svdb_options* opts, svdb_rec* out);

@@ -284,6 +284,65 @@ int svdb_multiply_transposed_by_dense(const svdb_matrix* a, const double* q, uin
     });
 }
 
+int svdb_column_means(const svdb_matrix* a, double* means) {
+    return guarded([&] {
+        check_handle(a);
+        if (!means) throw Error(SVDB_ERR_ARG, "null argument");
+        svdb_matrix* am = const_cast<svdb_matrix*>(a);
+        std::lock_guard<std::mutex> lk(am->mu);
+        DeviceGuard g(a->device);
+        cudaStream_t s = a->stream;
+        const DevCompressed& t = csc_of(a);
+        DevBuf<double> mu(std::max<int64_t>(t.nmajor, 1), s);
+        column_means_dev(t, a->nrows, mu.p, s);
+        if (t.nmajor) SVDB_CUDA(cudaMemcpyAsync(means, mu.p, t.nmajor * 8, cudaMemcpyDeviceToHost, s));
+        SVDB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int svdb_multiply_with_dense_centered(const svdb_matrix* a, const double* dense, uint64_t l, const double* means,
+                                      double* result, int transpose_self) {
+    return guarded([&] {
+        check_handle(a);
+        if (!dense || !result || !means) throw Error(SVDB_ERR_ARG, "null argument");
+        svdb_matrix* am = const_cast<svdb_matrix*>(a);
+        std::lock_guard<std::mutex> lk(am->mu);
+        DeviceGuard g(a->device);
+        cudaStream_t s = a->stream;
+        const DevCompressed& op = transpose_self ? csc_of(a) : csr_of(a);
+        DevBuf<double> dx(std::max<int64_t>(op.nminor * l, 1), s), dy(std::max<int64_t>(op.nmajor * l, 1), s),
+            mu(std::max<int64_t>(a->ncols, 1), s);
+        SVDB_CUDA(cudaMemcpyAsync(dx.p, dense, op.nminor * l * 8, cudaMemcpyHostToDevice, s));
+        SVDB_CUDA(cudaMemcpyAsync(mu.p, means, a->ncols * 8, cudaMemcpyHostToDevice, s));
+        spmm_dev<double, double>(op, false, dx.p, (int)l, dy.p, s);
+        center_product(dx.p, op.nminor, (int)l, mu.p, dy.p, op.nmajor, !transpose_self, s);
+        SVDB_CUDA(cudaMemcpyAsync(result, dy.p, op.nmajor * l * 8, cudaMemcpyDeviceToHost, s));
+        SVDB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int svdb_multiply_transposed_by_dense_centered(const svdb_matrix* a, const double* q, uint64_t l, const double* means,
+                                               double* result) {
+    return guarded([&] {
+        check_handle(a);
+        if (!q || !result || !means) throw Error(SVDB_ERR_ARG, "null argument");
+        svdb_matrix* am = const_cast<svdb_matrix*>(a);
+        std::lock_guard<std::mutex> lk(am->mu);
+        DeviceGuard g(a->device);
+        cudaStream_t s = a->stream;
+        const DevCompressed& op = csc_of(a);  // (Q^T (A - 1 mu^T))^T = A^T Q - mu (1^T Q)
+        DevBuf<double> dq(std::max<int64_t>(op.nminor * l, 1), s), dz(std::max<int64_t>(op.nmajor * l, 1), s),
+            dr(std::max<int64_t>(op.nmajor * l, 1), s), mu(std::max<int64_t>(a->ncols, 1), s);
+        SVDB_CUDA(cudaMemcpyAsync(dq.p, q, op.nminor * l * 8, cudaMemcpyHostToDevice, s));
+        SVDB_CUDA(cudaMemcpyAsync(mu.p, means, a->ncols * 8, cudaMemcpyHostToDevice, s));
+        spmm_dev<double, double>(op, false, dq.p, (int)l, dz.p, s);
+        center_product(dq.p, op.nminor, (int)l, mu.p, dz.p, op.nmajor, false, s);
+        transpose_dense<double>(dz.p, dr.p, op.nmajor, (int64_t)l, s);
+        SVDB_CUDA(cudaMemcpyAsync(result, dr.p, op.nmajor * l * 8, cudaMemcpyDeviceToHost, s));
+        SVDB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
 static int las2_common(const svdb_matrix* a, uint64_t dimensions, uint64_t iterations, const double end_interval[2],
                        double kappa, uint32_t seed, const svdb_options* opts, svdb_rec* out, int force_legacy) {
     return guarded([&] {

@@ -26,6 +26,15 @@ int gram_tc_launch(const double* X, int64_t rows, int c, double* part, int64_t p
 int gram_tc_blocks(int64_t rows);
 void gram_tc_check();
 
+// Centred products (randomized.cu).  mu (csc.nmajor) = the column sums of A
+// over its `rows` rows, divided by rows.  center_product turns Out = A X
+// (out_is_rows, X: xrows = ncols rows) into A X - 1 (mu^T X), or Out = A^T X
+// (X: xrows = nrows rows) into A^T X - mu (1^T X).  X and Out are row-major
+// with c columns.
+void column_means_dev(const DevCompressed& csc, int64_t rows, double* mu, cudaStream_t s);
+void center_product(const double* X, int64_t xrows, int c, const double* mu, double* Out, int64_t orows,
+                    bool out_is_rows, cudaStream_t s);
+
 void datx(double a, const double* x, double* y, int64_t n, cudaStream_t s);  // y = a * x
 
 void gemv_t(const double* Q, int64_t n, int64_t i0, int64_t cnt, const double* x, double* t, double* scratch,

@@ -253,11 +253,11 @@ __global__ void k_major_means(const int64_t* __restrict__ ptr, const double* __r
         if (lane == 0) mu[j] = acc * inv;
     }
 }
-// part[b][j] = sum over the rows of chunk b of w[r] X[r][j] (w = 1 when null).
-// 32 x 8 threads: x walks the columns, y the rows; the y partials are added
-// in y order.
+// part[b][j] = sum over the rows of chunk b of w[r] X[r][j] (w = 1 when null),
+// for the c <= 128 columns of X starting at X (row stride ld).  32 x 8
+// threads: x walks the columns, y the rows; the y partials are added in y order.
 constexpr int kCsCols = 128;
-__global__ void __launch_bounds__(256) k_wcolsum_part(const double* __restrict__ X, int64_t rows, int c,
+__global__ void __launch_bounds__(256) k_wcolsum_part(const double* __restrict__ X, int64_t rows, int64_t ld, int c,
                                                       const double* __restrict__ w, int64_t chunk,
                                                       double* __restrict__ part) {
     __shared__ double sh[8][kCsCols];
@@ -271,7 +271,7 @@ __global__ void __launch_bounds__(256) k_wcolsum_part(const double* __restrict__
 #pragma unroll
         for (int q = 0; q < kCsCols / 32; ++q) {
             const int j = tx + 32 * q;
-            if (j < c) acc[q] = fma(wr, X[r * c + j], acc[q]);
+            if (j < c) acc[q] = fma(wr, X[r * ld + j], acc[q]);
         }
     }
 #pragma unroll
@@ -292,7 +292,7 @@ __global__ void k_colsum_total(const double* __restrict__ part, int nblocks, int
         t[j] = acc;
     }
 }
-// Y[r][j] -= a[r] t[j] (a = 1 when null)
+// Y[r][j] -= a[r] t[j] (a = 1 when null), Y rows x c
 __global__ void k_rank1_sub(double* __restrict__ Y, int64_t rows, int c, const double* __restrict__ a,
                             const double* __restrict__ t) {
     const int64_t total = rows * c;
@@ -300,6 +300,30 @@ __global__ void k_rank1_sub(double* __restrict__ Y, int64_t rows, int c, const d
         const int64_t r = i / c;
         Y[i] -= (a ? a[r] : 1.0) * t[i - r * c];
     }
+}
+
+void column_means_dev(const DevCompressed& csc, int64_t rows, double* mu, cudaStream_t s) {
+    if (csc.nmajor == 0) return;
+    k_major_means<<<nb(csc.nmajor * 32, 256), 256, 0, s>>>(csc.ptr.p, csc.val.p, csc.nmajor,
+                                                          rows > 0 ? 1.0 / (double)rows : 0.0, mu);
+    SVDB_CHECK_LAUNCH();
+}
+
+void center_product(const double* X, int64_t xrows, int c, const double* mu, double* Out, int64_t orows,
+                    bool out_is_rows, cudaStream_t s) {
+    if (c <= 0 || orows <= 0) return;
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((xrows + 255) / 256, (int64_t)device_props().sms * 4));
+    const int64_t chunk = (xrows + blocks - 1) / blocks;
+    DevBuf<double> part((size_t)blocks * kCsCols, s), tot(c, s);
+    for (int j0 = 0; j0 < c; j0 += kCsCols) {
+        const int w = std::min(kCsCols, c - j0);
+        k_wcolsum_part<<<blocks, 256, 0, s>>>(X + j0, xrows, c, w, out_is_rows ? mu : nullptr, chunk, part.p);
+        SVDB_CHECK_LAUNCH();
+        k_colsum_total<<<1, 128, 0, s>>>(part.p, blocks, w, tot.p + j0);
+        SVDB_CHECK_LAUNCH();
+    }
+    k_rank1_sub<<<nb(orows * c, 256), 256, 0, s>>>(Out, orows, c, out_is_rows ? nullptr : mu, tot.p);
+    SVDB_CHECK_LAUNCH();
 }
 
 // ------------------------------------------------------ host helpers ----
@@ -515,29 +539,14 @@ void randomized(const svdb_matrix* A, uint64_t target_rank, uint64_t n_oversampl
         return c;
     };
 
-    // mean_center: Out = A X - 1 (mu^T X) for Out = A X (m rows), and
-    // Out = A^T X - mu (1^T X) for Out = A^T X (n rows)
-    DevBuf<double> mu, csum_part, csum;
-    int csum_blocks = 1;
+    // mean_center: the products of A - 1 mu^T
+    DevBuf<double> mu;
     if (mean_center) {
-        if (l > kCsCols) throw Error(SVDB_ERR_UNSUPPORTED, "randomized_svd: mean_center takes at most 128 sample columns");
         mu.alloc(std::max<int64_t>(n, 1), s);
-        k_major_means<<<nb(n * 32, 256), 256, 0, s>>>(Acsc.ptr.p, Acsc.val.p, n, m > 0 ? 1.0 / (double)m : 0.0, mu.p);
-        SVDB_CHECK_LAUNCH();
-        csum_blocks = (int)std::max<int64_t>(1, std::min<int64_t>((std::max(m, n) + 255) / 256,
-                                                                 (int64_t)device_props().sms * 4));
-        csum_part.alloc((size_t)csum_blocks * l, s);
-        csum.alloc(l, s);
+        column_means_dev(Acsc, m, mu.p, s);
     }
     auto center = [&](const double* X, int64_t xrows, int c, double* Out, int64_t orows, bool out_is_rows) {
-        if (!mean_center) return;
-        const int64_t chunk = (xrows + csum_blocks - 1) / csum_blocks;
-        k_wcolsum_part<<<csum_blocks, 256, 0, s>>>(X, xrows, c, out_is_rows ? mu.p : nullptr, chunk, csum_part.p);
-        SVDB_CHECK_LAUNCH();
-        k_colsum_total<<<1, 128, 0, s>>>(csum_part.p, csum_blocks, c, csum.p);
-        SVDB_CHECK_LAUNCH();
-        k_rank1_sub<<<nb(orows * c, 256), 256, 0, s>>>(Out, orows, c, out_is_rows ? nullptr : mu.p, csum.p);
-        SVDB_CHECK_LAUNCH();
+        if (mean_center) center_product(X, xrows, c, mu.p, Out, orows, out_is_rows, s);
     };
 
     if (verbose) printf("SVD | Randomized | Multiplying m with omega matrix....\n");

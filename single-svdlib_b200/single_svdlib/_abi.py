@@ -96,6 +96,9 @@ SIGNATURES = {
     "svdb_opb": (C.c_int, [vp, vp, vp, C.c_int]),
     "svdb_multiply_with_dense": (C.c_int, [vp, vp, u64, vp, C.c_int]),
     "svdb_multiply_transposed_by_dense": (C.c_int, [vp, vp, u64, vp]),
+    "svdb_column_means": (C.c_int, [vp, vp]),
+    "svdb_multiply_with_dense_centered": (C.c_int, [vp, vp, u64, vp, vp, C.c_int]),
+    "svdb_multiply_transposed_by_dense_centered": (C.c_int, [vp, vp, u64, vp, vp]),
     "svdb_multiply_with_dense_device": (C.c_int, [vp, vp, u64, vp, C.c_int, C.c_int, vp]),
     "svdb_opa_device": (C.c_int, [vp, vp, vp, C.c_int, C.c_int, vp]),
     "svdb_release_cached_memory": (C.c_int, []),

@@ -241,6 +241,40 @@ class _Handle:
         check(_abi.lib().svdb_multiply_transposed_by_dense(self._h, q.ctypes.data, l, out.ctypes.data))
         return out
 
+    # compute_column_means (masked.rs:240-263)
+    def column_means(self) -> np.ndarray:
+        out = np.zeros(self.ncols())
+        check(_abi.lib().svdb_column_means(self._h, out.ctypes.data))
+        return out
+
+    # SMat::multiply_with_dense_centered / multiply_transposed_by_dense_centered
+    # (src/utils.rs:29-32): exact products of A - 1 means^T
+    def _means(self, means):
+        means = _f64(means)
+        if means.shape != (self.ncols(),):
+            raise ShapeError(f"means has {means.size} values for {self.ncols()} columns")
+        return means
+
+    def multiply_with_dense_centered(self, dense, means, transpose_self=False) -> np.ndarray:
+        dense, means = _f64(dense), self._means(means)
+        if dense.shape[0] != (self.nrows() if transpose_self else self.ncols()):
+            raise ShapeError("dense operand has the wrong number of rows")
+        l = dense.shape[1]
+        out = np.zeros((self.ncols() if transpose_self else self.nrows(), l))
+        check(_abi.lib().svdb_multiply_with_dense_centered(self._h, dense.ctypes.data, l, means.ctypes.data,
+                                                           out.ctypes.data, int(transpose_self)))
+        return out
+
+    def multiply_transposed_by_dense_centered(self, q, means) -> np.ndarray:
+        q, means = _f64(q), self._means(means)
+        if q.shape[0] != self.nrows():
+            raise ShapeError("q has the wrong number of rows")
+        l = q.shape[1]
+        out = np.zeros((l, self.ncols()))
+        check(_abi.lib().svdb_multiply_transposed_by_dense_centered(self._h, q.ctypes.data, l, means.ctypes.data,
+                                                                    out.ctypes.data))
+        return out
+
 
 class CsrMatrix(_Handle):
     """nalgebra_sparse::CsrMatrix<f64>, uploaded to the current CUDA device."""

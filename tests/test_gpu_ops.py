@@ -66,6 +66,30 @@ def test_dense_products(l):
         close(h.multiply_transposed_by_dense(Y), O.masked_dense(A, mk, "XTA", Y), 1e-12)
 
 
+@pytest.mark.parametrize("l", [3, 130, 300])
+def test_centred_products_and_column_means(l):
+    """compute_column_means (masked.rs:240-263) and the centred products of
+    src/utils.rs:29-32 as exact products of A - 1 means^T, against numpy;
+    l above 128 crosses the 128-column slices of the rank-1 correction."""
+    A = M.uniform(400, 180, 0.1, 17)
+    mk = (np.random.default_rng(5).random(180) < 0.6).astype(np.uint8)
+    nm = int(mk.sum())
+    D = M.to_scipy(A).toarray()[:, mk.astype(bool)]
+    h = upload("masked", A, mk)
+    mu = h.column_means()
+    close(mu, D.mean(0))
+    rng = np.random.default_rng(9)
+    means = mu + rng.standard_normal(nm)  # any means vector, not only the column means
+    Dc = D - means[None, :]
+    X = rng.standard_normal((nm, l))
+    Y = rng.standard_normal((400, l))
+    close(h.multiply_with_dense_centered(X, means), Dc @ X, 1e-12)
+    close(h.multiply_with_dense_centered(Y, means, transpose_self=True), Dc.T @ Y, 1e-12)
+    close(h.multiply_transposed_by_dense_centered(Y, means), Y.T @ Dc, 1e-12)
+    with pytest.raises(Exception):
+        h.multiply_with_dense_centered(X, means[:-1])
+
+
 def test_empty_rows_and_columns():
     import scipy.sparse as sp
     S = sp.csr_matrix(([1.0, 2.0, 3.0], ([0, 5, 5], [3, 3, 9])), shape=(8, 12))
