@@ -105,6 +105,25 @@ typedef struct svdb_rec {
     double time_ms_ritvec;
 } svdb_rec;
 
+/* SvdRec<f32> (T = f32, src/utils.rs:44-99): svdb_rec with f32 buffers.
+ * diagnostics.end_interval and kappa hold the f32 values, widened. */
+typedef struct svdb_rec_f32 {
+    uint64_t d;
+    uint64_t u_rows, u_cols;
+    float* u;
+    float* s;
+    uint64_t vt_rows, vt_cols;
+    float* vt;
+    svdb_diagnostics diagnostics;
+    int32_t on_device;
+    int32_t origin;
+    double time_ms_total;
+    double time_ms_spmv;
+    double time_ms_ortho;
+    double time_ms_tridiag;
+    double time_ms_ritvec;
+} svdb_rec_f32;
+
 /* Internals of one LAS2 run, filled when svdb_options.trace is set: the
  * tridiagonal T (alf: steps+1 values, bet: steps+2 values) and the Ritz values
  * and bounds of the last lanso analysis (steps+1 values each), copied into
@@ -150,6 +169,16 @@ int svdb_matrix_create_csc(uint64_t nrows, uint64_t ncols, uint64_t nnz, const u
  * Replaces `impl SMat<T> for CooMatrix<T>` (src/lanczos/mod.rs:1657-1740). */
 int svdb_matrix_create_coo(uint64_t nrows, uint64_t ncols, uint64_t nnz, const uint64_t* rows,
                            const uint64_t* cols, const double* values, svdb_matrix** out);
+/* The same matrices with f32 values (CsrMatrix<f32>, CscMatrix<f32>,
+ * CooMatrix<f32>): the values travel and stay as f32, widened exactly to f64
+ * on the device.  Any solver runs on them; the *_f32 entry points give the
+ * crate's T = f32 semantics. */
+int svdb_matrix_create_csr_f32(uint64_t nrows, uint64_t ncols, uint64_t nnz, const uint64_t* indptr,
+                               const uint64_t* indices, const float* values, svdb_matrix** out);
+int svdb_matrix_create_csc_f32(uint64_t nrows, uint64_t ncols, uint64_t nnz, const uint64_t* colptr,
+                               const uint64_t* rowidx, const float* values, svdb_matrix** out);
+int svdb_matrix_create_coo_f32(uint64_t nrows, uint64_t ncols, uint64_t nnz, const uint64_t* rows,
+                               const uint64_t* cols, const float* values, svdb_matrix** out);
 /* CSR whose arrays are already in device memory (int64 indptr, int32 column
  * indices); the library copies them.  Same contract as svdb_matrix_create_csr. */
 int svdb_matrix_create_csr_device(uint64_t nrows, uint64_t ncols, uint64_t nnz, const int64_t* d_indptr,
@@ -294,6 +323,29 @@ int svdb_las2_plan(uint64_t nrows, uint64_t ncols, uint64_t nnz, uint64_t dimens
 int svdb_randomized_svd(const svdb_matrix* a, uint64_t target_rank, uint64_t n_oversamples,
                         uint64_t n_power_iters, int normalizer, int mean_center, int has_seed, uint64_t seed,
                         int verbose, const svdb_options* opts, svdb_rec* out);
+
+/* ---- T = f32 (impl SvdFloat for f32, src/utils.rs:87-99) ---- */
+
+/* lanczos::svd_las2 / svd / svd_dim / svd_dim_seed monomorphised at T = f32
+ * (src/lanczos/mod.rs:27-189): every tolerance takes f32::EPSILON (eps,
+ * eps34, sqrt(eps), compare), kappa is clamped to f32 eps34, and the start
+ * vector's f64 draws are rounded to f32.  The products use the FP32 values
+ * and FP32 operand vectors; sums and the recurrences stay FP64, and u/s/vt
+ * are rounded to f32 at the end.  opts->algorithm = SVDB_LEGACY returns
+ * SVDB_ERR_UNSUPPORTED (legacy::svdLAS2 is f64-only); opts->precision is
+ * ignored. */
+int svdb_las2_f32(const svdb_matrix* a, uint64_t dimensions, uint64_t iterations, const float end_interval[2],
+                  float kappa, uint32_t random_seed, const svdb_options* opts, svdb_rec_f32* out);
+int svdb_svd_f32(const svdb_matrix* a, svdb_rec_f32* out);
+int svdb_svd_dim_f32(const svdb_matrix* a, uint64_t dimensions, svdb_rec_f32* out);
+int svdb_svd_dim_seed_f32(const svdb_matrix* a, uint64_t dimensions, uint32_t random_seed, svdb_rec_f32* out);
+/* randomized::randomized_svd at T = f32: Omega's f64 draws (or opts->omega)
+ * rounded to f32, FP32 operands in the products, FP64 factorisations,
+ * results rounded to f32. */
+int svdb_randomized_svd_f32(const svdb_matrix* a, uint64_t target_rank, uint64_t n_oversamples,
+                            uint64_t n_power_iters, int normalizer, int mean_center, int has_seed, uint64_t seed,
+                            int verbose, const svdb_options* opts, svdb_rec_f32* out);
+void svdb_rec_f32_free(svdb_rec_f32* r);
 
 /* ---- batches of masked column subsets (no reference counterpart) ---- */
 

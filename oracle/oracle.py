@@ -18,8 +18,9 @@ import subprocess
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-_LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
-_lib = None
+_LIB_PATHS = {"f64": os.path.join(_HERE, "_build", "liboracle.so"),
+              "f32": os.path.join(_HERE, "_build", "liboracle_f32.so")}
+_libs = {}
 
 KIND = {"csr": 0, "csc": 1, "coo": 2, "masked": 3}
 ERRORS = {0: "ok", 1: "ImtqlbError", 2: "StartvError", 3: "StponeError", 4: "Imtql2Error",
@@ -58,12 +59,15 @@ def build():
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not os.path.exists(_LIB_PATH):
+def lib(scalar="f64"):
+    """The checker built for the crate's scalar T: "f64" (every solver) or
+    "f32" (lanczos and randomized; legacy is f64-only in the crate).  Arrays
+    cross the interface as float64 either way."""
+    if scalar not in _libs:
+        path = _LIB_PATHS[scalar]
+        if not os.path.exists(path):
             build()
-        L = C.CDLL(_LIB_PATH)
+        L = C.CDLL(path)
         p = np.ctypeslib.ndpointer
         u64, f64, u8, i64 = (p(np.uint64, flags="C"), p(np.float64, flags="C"), p(np.uint8, flags="C"),
                              p(np.int64, flags="C"))
@@ -72,10 +76,12 @@ def lib():
         L.orc_chacha_block.argtypes = [p(np.uint8, flags="C"), C.c_uint64, C.c_uint64, C.c_int,
                                        p(np.uint32, flags="C")]
         L.orc_start_vector.argtypes = [C.c_uint32, f64, C.c_size_t]
-        L.orc_pythag.argtypes = [C.c_double, C.c_double, C.c_int]
-        L.orc_pythag.restype = C.c_double
-        L.orc_imtqlb.argtypes = [C.c_size_t, f64, f64, f64, C.c_int, C.c_size_t]
-        L.orc_imtql2.argtypes = [C.c_size_t, f64, f64, f64, C.c_int, C.c_size_t]
+        if scalar == "f64":
+            L.orc_pythag.argtypes = [C.c_double, C.c_double, C.c_int]
+            L.orc_pythag.restype = C.c_double
+            L.orc_imtqlb.argtypes = [C.c_size_t, f64, f64, f64, C.c_int, C.c_size_t]
+            L.orc_imtql2.argtypes = [C.c_size_t, f64, f64, f64, C.c_int, C.c_size_t]
+        assert L.orc_real_bytes() == (8 if scalar == "f64" else 4)
         L.orc_las2.argtypes = [C.c_int, C.c_uint64, C.c_uint64, C.c_uint64, u64, u64, f64, C.c_void_p,
                                C.c_uint64, C.c_uint64, C.c_double, C.c_double, C.c_double, C.c_uint32,
                                C.c_int, C.POINTER(_Las2Out)]
@@ -90,8 +96,8 @@ def lib():
                                      C.c_uint64, C.c_uint64, C.c_uint64, C.c_int, f64, C.c_int, C.c_int,
                                      C.POINTER(_RandOut)]
         L.orc_rand_free.argtypes = [C.POINTER(_RandOut)]
-        _lib = L
-    return _lib
+        _libs[scalar] = L
+    return _libs[scalar]
 
 
 def set_threads(t: int):
@@ -113,9 +119,9 @@ def chacha_block(key: bytes, counter: int, stream: int, rounds: int) -> np.ndarr
     return out
 
 
-def start_vector(seed: int, n: int) -> np.ndarray:
+def start_vector(seed: int, n: int, scalar="f64") -> np.ndarray:
     out = np.zeros(n, dtype=np.float64)
-    lib().orc_start_vector(seed, out, n)
+    lib(scalar).orc_start_vector(seed, out, n)
     return out
 
 
@@ -150,18 +156,22 @@ def _sparse_args(kind, A):
 
 
 def las2(kind, A, dimensions=0, iterations=0, end_interval=(-1e-30, 1e-30), kappa=1e-6, seed=0,
-         legacy=False, mask=None):
-    """Run lanczos::svd_las2 (legacy=False) or legacy::svdLAS2 (legacy=True)."""
+         legacy=False, mask=None, scalar="f64"):
+    """Run lanczos::svd_las2 (legacy=False) or legacy::svdLAS2 (legacy=True),
+    at T = f64 or, for lanczos, T = f32 (values rounded to f32 on entry)."""
+    if legacy and scalar != "f64":
+        raise ValueError("legacy::svdLAS2 is f64-only")
+    L = lib(scalar)
     p, i, v = _sparse_args(kind, A)
     mk = None
     if kind == "masked":
         mk = np.ascontiguousarray(mask, dtype=np.uint8)
     out = _Las2Out()
-    rc = lib().orc_las2(KIND[kind], A["nrows"], A["ncols"], len(v), p, i, v,
-                        mk.ctypes.data if mk is not None else None, dimensions, iterations,
-                        float(end_interval[0]), float(end_interval[1]), kappa, seed, int(legacy), C.byref(out))
+    rc = L.orc_las2(KIND[kind], A["nrows"], A["ncols"], len(v), p, i, v,
+                    mk.ctypes.data if mk is not None else None, dimensions, iterations,
+                    float(end_interval[0]), float(end_interval[1]), kappa, seed, int(legacy), C.byref(out))
     if rc:
-        err = OracleError(rc, lib().orc_last_error().decode())
+        err = OracleError(rc, L.orc_last_error().decode())
         err.steps, err.neig = out.steps, out.ritz_values_stabilized
         raise err
     try:
@@ -191,11 +201,11 @@ def las2(kind, A, dimensions=0, iterations=0, end_interval=(-1e-30, 1e-30), kapp
             "masked_would_panic": bool(out.masked_would_panic),
         }
     finally:
-        lib().orc_las2_free(C.byref(out))
+        L.orc_las2_free(C.byref(out))
     return res
 
 
-def opa(kind, A, x, transposed=False, legacy=False, mask=None):
+def opa(kind, A, x, transposed=False, legacy=False, mask=None, scalar="f64"):
     p, i, v = _sparse_args(kind, A)
     m, n = A["nrows"], A["ncols"]
     if kind == "masked":
@@ -205,10 +215,11 @@ def opa(kind, A, x, transposed=False, legacy=False, mask=None):
     ylen = ncol_eff if transposed else m
     y = np.zeros(ylen)
     mk = np.ascontiguousarray(mask, dtype=np.uint8) if mask is not None else None
-    rc = lib().orc_opa(KIND[kind], m, n, len(v), p, i, v, mk.ctypes.data if mk is not None else None,
-                       _f64(x), y, int(transposed), int(legacy))
+    L = lib(scalar)
+    rc = L.orc_opa(KIND[kind], m, n, len(v), p, i, v, mk.ctypes.data if mk is not None else None,
+                   _f64(x), y, int(transposed), int(legacy))
     if rc:
-        raise OracleError(rc, lib().orc_last_error().decode())
+        raise OracleError(rc, L.orc_last_error().decode())
     return y
 
 
@@ -237,16 +248,18 @@ def masked_dense(A, mask, op, X, compat_d3=False):
 
 
 def randomized(A, target_rank, n_oversamples, n_power_iters, normalizer="QR", omega=None, mask=None,
-               compat_d3=False, mean_center=False):
-    """Randomized SVD on the masked view (all columns when mask is None); omega is n_masked x l row-major."""
+               compat_d3=False, mean_center=False, scalar="f64"):
+    """Randomized SVD on the masked view (all columns when mask is None); omega is n_masked x l row-major
+    (float64 draws, rounded to T inside as T::from_f64 does)."""
     mk = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
     out = _RandOut()
-    rc = lib().orc_randomized(A["nrows"], A["ncols"], len(A["indices"]), _u64(A["indptr"]), _u64(A["indices"]),
+    L = lib(scalar)
+    rc = L.orc_randomized(A["nrows"], A["ncols"], len(A["indices"]), _u64(A["indptr"]), _u64(A["indices"]),
                               _f64(A["data"]), mk.ctypes.data if mk is not None else None, target_rank,
                               n_oversamples, n_power_iters, {"QR": 0, "LU": 1, "None": 2}[normalizer],
                               _f64(omega), int(compat_d3), int(mean_center), C.byref(out))
     if rc:
-        raise OracleError(rc, lib().orc_last_error().decode())
+        raise OracleError(rc, L.orc_last_error().decode())
     try:
         d, m, n = out.d, out.m, out.n
         res = {"d": d,
@@ -255,7 +268,7 @@ def randomized(A, target_rank, n_oversamples, n_power_iters, normalizer="QR", om
                "vt": np.ctypeslib.as_array(out.vt, (max(1, d * n),))[: d * n].reshape(d, n).copy(),
                "times": {"sparse": out.t_sparse, "rows": out.t_rows, "fixed": out.t_fixed}}
     finally:
-        lib().orc_rand_free(C.byref(out))
+        L.orc_rand_free(C.byref(out))
     return res
 
 

@@ -44,17 +44,25 @@
 
 namespace orc {
 
-static const double EPS = std::numeric_limits<double>::epsilon();
+// The scalar T of the crate's generic solvers (SvdFloat): f64, or f32 when
+// built with -DORC_F32 (lanczos and randomized only; legacy is f64-only).
+#ifdef ORC_F32
+using real = float;
+#else
+using real = double;
+#endif
+
+static const real EPS = std::numeric_limits<real>::epsilon();  // SvdFloat::eps, src/utils.rs:87-113
 static int g_threads = 1;  // stands in for rayon::current_num_threads()
 
-static double eps34() { return std::pow(EPS, 0.75); }  // src/utils.rs:106-108
+static real eps34() { return std::pow(EPS, 0.75); }  // src/utils.rs:106-108
 
 // SvdFloat::compare, src/utils.rs:110-112 (absolute epsilon)
-static inline bool compare(double a, double b) { return std::fabs(b - a) < EPS; }
+static inline bool compare(real a, real b) { return std::fabs(b - a) < EPS; }
 
 // Rust f64::max / f64::min ignore a NaN operand, like C fmax / fmin.
-static inline double fmax_(double a, double b) { return std::fmax(a, b); }
-static inline double fmin_(double a, double b) { return std::fmin(a, b); }
+static inline real fmax_(real a, real b) { return std::fmax(a, b); }
+static inline real fmin_(real a, real b) { return std::fmin(a, b); }
 
 struct Error : std::runtime_error {
     int code;
@@ -132,13 +140,14 @@ static inline double uniform_pm1(uint64_t u) {
     return v01 * scale + (-1.0);
 }
 
-// startv's fill: StdRng::from_seed(seed u32 in bytes 0..3), src/lanczos/mod.rs:598-605
-static void start_vector(uint32_t seed, double* w, size_t n) {
+// startv's fill: StdRng::from_seed(seed u32 in bytes 0..3), src/lanczos/mod.rs:598-605;
+// each f64 draw is rounded to T (T::from_f64)
+static void start_vector(uint32_t seed, real* w, size_t n) {
     uint8_t bytes[32] = {0};
     bytes[0] = seed & 0xff; bytes[1] = (seed >> 8) & 0xff;
     bytes[2] = (seed >> 16) & 0xff; bytes[3] = (seed >> 24) & 0xff;
     ChaChaRng rng(bytes, 12);
-    for (size_t i = 0; i < n; ++i) w[i] = uniform_pm1(rng.next_u64());
+    for (size_t i = 0; i < n; ++i) w[i] = (real)uniform_pm1(rng.next_u64());
 }
 
 // ---------------------------------------------------------------------------
@@ -156,13 +165,13 @@ struct SMat {
     virtual size_t nrows() const = 0;
     virtual size_t ncols() const = 0;
     virtual size_t nnz() const = 0;
-    virtual void svd_opa(const double* x, double* y, bool transposed) const = 0;
+    virtual void svd_opa(const real* x, real* y, bool transposed) const = 0;
 };
 
 struct Compressed {  // major offsets, minor indices, values
     size_t nmajor = 0, nminor = 0;
     std::vector<uint64_t> ptr, idx;
-    std::vector<double> val;
+    std::vector<real> val;
 };
 
 // SMat for CsrMatrix, src/lanczos/mod.rs:1506-1603.  `legacy` selects the
@@ -174,16 +183,16 @@ struct CsrOp : SMat {
     size_t nrows() const override { return a->nmajor; }
     size_t ncols() const override { return a->nminor; }
     size_t nnz() const override { return a->idx.size(); }
-    void svd_opa(const double* x, double* y, bool transposed) const override {
+    void svd_opa(const real* x, real* y, bool transposed) const override {
         const size_t m = a->nmajor, n = a->nminor;
         const uint64_t* p = a->ptr.data();
         const uint64_t* ci = a->idx.data();
-        const double* v = a->val.data();
+        const real* v = a->val.data();
         if (!transposed) {
             // row gather, mod.rs:1551-1570 (per-row sequential sum, rows in parallel)
 #pragma omp parallel for schedule(static) num_threads(g_threads) if (g_threads > 1)
             for (size_t i = 0; i < m; ++i) {
-                double sum = 0.0;
+                real sum = 0.0;
                 for (uint64_t j = p[i]; j < p[i + 1]; ++j) sum += v[j] * x[ci[j]];
                 y[i] = sum;
             }
@@ -198,13 +207,13 @@ struct CsrOp : SMat {
         // chunk-private buffers + serial combine, mod.rs:1571-1602
         size_t cs = determine_chunk_size(m);
         size_t nch = (m + cs - 1) / cs;
-        std::vector<std::vector<double>> loc(nch);
+        std::vector<std::vector<real>> loc(nch);
 #pragma omp parallel for schedule(dynamic, 1) num_threads(g_threads) if (g_threads > 1)
         for (size_t c = 0; c < nch; ++c) {
-            std::vector<double> ly(n, 0.0);
+            std::vector<real> ly(n, 0.0);
             size_t s = c * cs, e = std::min(s + cs, m);
             for (size_t i = s; i < e; ++i) {
-                double rv = x[i];
+                real rv = x[i];
                 for (uint64_t j = p[i]; j < p[i + 1]; ++j) ly[ci[j]] += v[j] * rv;
             }
             loc[c].swap(ly);
@@ -222,10 +231,10 @@ struct CscOp : SMat {
     size_t nrows() const override { return a->nminor; }
     size_t ncols() const override { return a->nmajor; }
     size_t nnz() const override { return a->idx.size(); }
-    void svd_opa(const double* x, double* y, bool transposed) const override {
+    void svd_opa(const real* x, real* y, bool transposed) const override {
         const uint64_t* p = a->ptr.data();
         const uint64_t* ri = a->idx.data();
-        const double* v = a->val.data();
+        const real* v = a->val.data();
         size_t ylen = transposed ? a->nmajor : a->nminor;
         std::fill(y, y + ylen, 0.0);
         if (transposed) {
@@ -233,7 +242,7 @@ struct CscOp : SMat {
                 for (uint64_t j = p[i]; j < p[i + 1]; ++j) y[i] += v[j] * x[ri[j]];
         } else {
             for (size_t i = 0; i < a->nmajor; ++i) {
-                double xv = x[i];
+                real xv = x[i];
                 for (uint64_t j = p[i]; j < p[i + 1]; ++j) y[ri[j]] += v[j] * xv;
             }
         }
@@ -244,11 +253,11 @@ struct CscOp : SMat {
 struct CooOp : SMat {
     size_t m, n;
     std::vector<uint64_t> r, c;
-    std::vector<double> v;
+    std::vector<real> v;
     size_t nrows() const override { return m; }
     size_t ncols() const override { return n; }
     size_t nnz() const override { return v.size(); }
-    void svd_opa(const double* x, double* y, bool transposed) const override {
+    void svd_opa(const real* x, real* y, bool transposed) const override {
         size_t ylen = transposed ? n : m;
         std::fill(y, y + ylen, 0.0);
         if (transposed) {
@@ -289,11 +298,11 @@ struct MaskedOp : SMat {
         for (size_t i = 0; i < a->idx.size(); ++i) if (mask[a->idx[i]]) ++cnt;
         return cnt;
     }
-    void svd_opa(const double* x, double* y, bool transposed) const override {
+    void svd_opa(const real* x, real* y, bool transposed) const override {
         const size_t m = a->nmajor;
         const uint64_t* p = a->ptr.data();
         const uint64_t* ci = a->idx.data();
-        const double* v = a->val.data();
+        const real* v = a->val.data();
         if (uses_all_columns()) {
             CsrOp(a, false).svd_opa(x, y, transposed);
             return;
@@ -303,7 +312,7 @@ struct MaskedOp : SMat {
         if (!transposed) {  // masked.rs:145-196
 #pragma omp parallel for schedule(static) num_threads(g_threads) if (g_threads > 1)
             for (size_t i = 0; i < m; ++i) {
-                double sum = 0.0;
+                real sum = 0.0;
                 for (uint64_t j = p[i]; j < p[i + 1]; ++j) {
                     int64_t mc = o2m[ci[j]];
                     if (mc >= 0) sum += v[j] * x[mc];
@@ -316,13 +325,13 @@ struct MaskedOp : SMat {
         std::fill(y, y + nm, 0.0);
         size_t cs = determine_chunk_size(m);
         size_t nch = (m + cs - 1) / cs;
-        std::vector<std::vector<double>> loc(nch);
+        std::vector<std::vector<real>> loc(nch);
 #pragma omp parallel for schedule(dynamic, 1) num_threads(g_threads) if (g_threads > 1)
         for (size_t c = 0; c < nch; ++c) {
-            std::vector<double> ly(nm, 0.0);
+            std::vector<real> ly(nm, 0.0);
             size_t s = c * cs, e = std::min(s + cs, m);
             for (size_t i = s; i < e; ++i) {
-                double rv = x[i];
+                real rv = x[i];
                 if (rv == 0.0) continue;
                 for (uint64_t j = p[i]; j < p[i + 1]; ++j) {
                     int64_t mc = o2m[ci[j]];
@@ -342,15 +351,15 @@ struct MaskedOp : SMat {
 // ---------------------------------------------------------------------------
 static bool g_legacy_blas = false;  // legacy BLAS-1 is always sequential
 
-static void svd_opb(const SMat& A, const double* x, double* y, double* temp, bool transposed) {
+static void svd_opb(const SMat& A, const real* x, real* y, real* temp, bool transposed) {
     A.svd_opa(x, temp, transposed);
     A.svd_opa(temp, y, !transposed);
 }
-static void svd_daxpy(double da, const double* x, double* y, size_t n) {
+static void svd_daxpy(real da, const real* x, real* y, size_t n) {
 #pragma omp parallel for schedule(static) num_threads(g_threads) if (g_threads > 1 && n >= 1000 && !g_legacy_blas)
     for (size_t i = 0; i < n; ++i) y[i] += da * x[i];
 }
-static size_t svd_idamax(size_t n, const double* x) {
+static size_t svd_idamax(size_t n, const real* x) {
     if (n == 0) throw Error(E_PANIC, "svd_idamax: unexpected inputs!");
     if (n == 1) return 0;
     size_t imax = 0;
@@ -358,85 +367,85 @@ static size_t svd_idamax(size_t n, const double* x) {
         if (std::fabs(x[i]) > std::fabs(x[imax])) imax = i;
     return imax;
 }
-static double svd_fsign(double a, double b) {
+static real svd_fsign(real a, real b) {
     return ((a >= 0.0 && b >= 0.0) || (a < 0.0 && b < 0.0)) ? a : -a;
 }
 // Current crate: mod.rs:361-380.  The loop sets r = (s/u)^2 (the factor r of
 // the Moler-Morrison update is absent), so for comparable |a|, |b| the result
 // exceeds hypot(a, b); restated as written.
-static double svd_pythag_current(double a, double b) {
-    double n = fmax_(std::fabs(a), std::fabs(b));
+static real svd_pythag_current(real a, real b) {
+    real n = fmax_(std::fabs(a), std::fabs(b));
     if (!(n > 0.0)) return 0.0;
-    double p = n;
-    double q = fmin_(std::fabs(a), std::fabs(b)) / p;
-    double r = q * q;
-    double t = 4.0 + r;
+    real p = n;
+    real q = fmin_(std::fabs(a), std::fabs(b)) / p;
+    real r = q * q;
+    real t = 4.0 + r;
     while (!compare(t, 4.0)) {
-        double s = r / t;
-        double u = 1.0 + 2.0 * s;
+        real s = r / t;
+        real u = 1.0 + 2.0 * s;
         p = p * u;
-        double su = s / u;
+        real su = s / u;
         r = su * su;
         t = 4.0 + r;
     }
     return p;
 }
 // Legacy: legacy.rs:878-895 (r *= (s/u)^2)
-static double svd_pythag_legacy(double a, double b) {
-    double n = fmax_(std::fabs(a), std::fabs(b));
+static real svd_pythag_legacy(real a, real b) {
+    real n = fmax_(std::fabs(a), std::fabs(b));
     if (!(n > 0.0)) return 0.0;
-    double p = n;
-    double q = fmin_(std::fabs(a), std::fabs(b)) / p;
-    double r = q * q;
-    double t = 4.0 + r;
+    real p = n;
+    real q = fmin_(std::fabs(a), std::fabs(b)) / p;
+    real r = q * q;
+    real t = 4.0 + r;
     while (!compare(t, 4.0)) {
-        double s = r / t;
-        double u = 1.0 + 2.0 * s;
+        real s = r / t;
+        real u = 1.0 + 2.0 * s;
         p *= u;
-        double su = s / u;
+        real su = s / u;
         r *= su * su;
         t = 4.0 + r;
     }
     return p;
 }
-static double svd_ddot(const double* x, const double* y, size_t n) {
+static real svd_ddot(const real* x, const real* y, size_t n) {
     if (g_threads <= 1 || n < 1000 || g_legacy_blas) {
-        double s = 0.0;
+        real s = 0.0;
         for (size_t i = 0; i < n; ++i) s += x[i] * y[i];
         return s;
     }
     // Rayon's reduction tree is scheduling dependent; a fixed-chunk ordered
     // reduction stands in for it.
     int T = g_threads;
-    std::vector<double> part(T, 0.0);
+    std::vector<real> part(T, 0.0);
 #pragma omp parallel for schedule(static, 1) num_threads(T)
     for (int t = 0; t < T; ++t) {
         size_t s = n * t / T, e = n * (t + 1) / T;
-        double acc = 0.0;
+        real acc = 0.0;
         for (size_t i = s; i < e; ++i) acc += x[i] * y[i];
         part[t] = acc;
     }
-    double s = 0.0;
+    real s = 0.0;
     for (int t = 0; t < T; ++t) s += part[t];
     return s;
 }
-static double svd_norm(const double* x, size_t n) { return std::sqrt(svd_ddot(x, x, n)); }
-static void svd_datx(double d, const double* x, double* y, size_t n) {
+static real svd_norm(const real* x, size_t n) { return std::sqrt(svd_ddot(x, x, n)); }
+static void svd_datx(real d, const real* x, real* y, size_t n) {
     for (size_t i = 0; i < n; ++i) y[i] = d * x[i];
 }
-static void svd_dscal(double d, double* x, size_t n) {
+static void svd_dscal(real d, real* x, size_t n) {
 #pragma omp parallel for schedule(static) num_threads(g_threads) if (g_threads > 1 && n >= 1000 && !g_legacy_blas)
     for (size_t i = 0; i < n; ++i) x[i] *= d;
 }
 // reversing copy, mod.rs:417-424
-static void svd_dcopy(size_t n, size_t off, const double* x, double* y) {
+static void svd_dcopy(size_t n, size_t off, const real* x, real* y) {
     if (n > 0) {
         size_t start = n - 1;
         for (size_t i = 0; i < n; ++i) y[off + start - i] = x[off + i];
     }
 }
 // mod.rs:297-307
-static void insert_sort(size_t n, double* a1, double* a2) {
+static void insert_sort(size_t n, real* a1, real* a2) {
     for (size_t i = 1; i < n; ++i)
         for (size_t j = i; j >= 1; --j) {
             if (a1[j - 1] <= a1[j]) break;
@@ -451,49 +460,49 @@ static void insert_sort(size_t n, double* a1, double* a2) {
 static const size_t MAXLL = 2;
 struct Store {
     size_t n;
-    std::vector<std::vector<double>> vecs;
+    std::vector<std::vector<real>> vecs;
     explicit Store(size_t n_) : n(n_) {}
-    void storq(size_t idx, const double* v) {
+    void storq(size_t idx, const real* v) {
         while (idx + MAXLL >= vecs.size()) vecs.emplace_back(n, 0.0);
-        std::memcpy(vecs[idx + MAXLL].data(), v, n * sizeof(double));
+        std::memcpy(vecs[idx + MAXLL].data(), v, n * sizeof(real));
     }
-    void storp(size_t idx, const double* v) {
+    void storp(size_t idx, const real* v) {
         while (idx >= vecs.size()) vecs.emplace_back(n, 0.0);
-        std::memcpy(vecs[idx].data(), v, n * sizeof(double));
+        std::memcpy(vecs[idx].data(), v, n * sizeof(real));
     }
-    const double* retrq(size_t idx) const { return vecs.at(idx + MAXLL).data(); }
-    const double* retrp(size_t idx) const { return vecs.at(idx).data(); }
+    const real* retrq(size_t idx) const { return vecs.at(idx + MAXLL).data(); }
+    const real* retrp(size_t idx) const { return vecs.at(idx).data(); }
 };
 
 struct Work {
     size_t nrows, ncols;
     bool transposed;
-    std::vector<double> w0, w1, w2, w3, w4, w5, alf, eta, oldeta, bet, bnd, ritz, temp;
+    std::vector<real> w0, w1, w2, w3, w4, w5, alf, eta, oldeta, bet, bnd, ritz, temp;
     Work(size_t nr, size_t nc, bool tr, size_t it)
         : nrows(nr), ncols(nc), transposed(tr), w0(nc), w1(nc), w2(nc), w3(nc), w4(nc), w5(nc),
-          alf(it), eta(it), oldeta(it), bet(1 + it), bnd(1 + it, std::numeric_limits<double>::max()),
+          alf(it), eta(it), oldeta(it), bet(1 + it), bnd(1 + it, std::numeric_limits<real>::max()),
           ritz(1 + it), temp(nr) {}
 };
 
 // Per-run settings that differ between lanczos::* and legacy::*.
 struct Mode {
     bool legacy = false;
-    double sparsity = 0.0;
-    double adaptive_eps = EPS;
+    real sparsity = 0.0;
+    real adaptive_eps = EPS;
     size_t max_imtqlb = 100;
     size_t max_imtql2 = 50;
     size_t extra_steps = 0;
 };
 
 // mod.rs:1068-1070 / 1273-1275
-static double sparsity_of(const SMat& A) {
-    return 1.0 - ((double)A.nnz() / ((double)A.nrows() * (double)A.ncols()));
+static real sparsity_of(const SMat& A) {
+    return 1.0 - ((real)A.nnz() / ((real)A.nrows() * (real)A.ncols()));
 }
 static Mode make_mode(const SMat& A, bool legacy) {
     Mode md;
     md.legacy = legacy;
     if (legacy) { md.max_imtqlb = 30; md.max_imtql2 = 30; return md; }
-    double sp = sparsity_of(A);
+    real sp = sparsity_of(A);
     md.sparsity = sp;
     md.max_imtqlb = sp > 0.999 ? 500 : sp > 0.99 ? 300 : sp > 0.9 ? 100 : 50;    // mod.rs:1276-1288
     md.adaptive_eps = sp > 0.99 ? EPS * 100.0 : sp > 0.9 ? EPS * 10.0 : EPS;     // mod.rs:1291-1300
@@ -507,9 +516,9 @@ static Mode make_mode(const SMat& A, bool legacy) {
 // ---------------------------------------------------------------------------
 static bool g_imtqlb_warned = false;
 
-static void imtqlb_current(size_t n, double* d, double* e, double* bnd, size_t max_imtqlb) {
+static void imtqlb_current(size_t n, real* d, real* e, real* bnd, size_t max_imtqlb) {
     if (n == 1) return;
-    double msf = std::sqrt((double)n);
+    real msf = std::sqrt((real)n);
     bnd[0] = 1.0;
     size_t last = n - 1;
     for (size_t i = 1; i <= last; ++i) { bnd[i] = 0.0; e[i - 1] = e[i]; }
@@ -518,14 +527,14 @@ static void imtqlb_current(size_t n, double* d, double* e, double* bnd, size_t m
     bool had_issues = false;
     for (size_t l = 0; l <= last; ++l) {
         size_t iteration = 0;
-        double p = d[l];   // set once per l (mod.rs:452-453)
-        double f = bnd[l];
+        real p = d[l];   // set once per l (mod.rs:452-453)
+        real f = bnd[l];
         while (iteration <= max_imtqlb) {
             size_t m = l;
             while (m < n) {
                 if (m == last) break;
-                double test = std::fabs(d[m]) + std::fabs(d[m + 1]);
-                double tol = EPS * 100.0 * fmax_(test, 1.0) * msf;
+                real test = std::fabs(d[m]) + std::fabs(d[m + 1]);
+                real tol = EPS * 100.0 * fmax_(test, 1.0) * msf;
                 if (std::fabs(e[m]) <= tol) break;
                 ++m;
             }
@@ -550,17 +559,17 @@ static void imtqlb_current(size_t n, double* d, double* e, double* bnd, size_t m
                     break;
                 }
                 ++iteration;
-                double g = (d[l + 1] - p) / (2.0 * e[l]);
-                double r = svd_pythag_current(g, 1.0);
+                real g = (d[l + 1] - p) / (2.0 * e[l]);
+                real r = svd_pythag_current(g, 1.0);
                 g = d[m] - p + e[l] / (g + svd_fsign(r, g));
-                double s = 1.0, c = 1.0;
+                real s = 1.0, c = 1.0;
                 p = 0.0;
                 if (m == 0) throw Error(E_PANIC, "imtqlb: expected 'm' to be non-zero");
                 i = m - 1;
                 bool underflow = false;
                 while (!underflow && i >= l) {
                     f = s * e[i];
-                    double b = c * e[i];
+                    real b = c * e[i];
                     r = svd_pythag_current(f, g);
                     e[i + 1] = r;
                     if (r < EPS * 1000.0 * (std::fabs(f) + std::fabs(g))) { underflow = true; break; }
@@ -587,7 +596,7 @@ static void imtqlb_current(size_t n, double* d, double* e, double* bnd, size_t m
     if (had_issues) g_imtqlb_warned = true;
 }
 
-static void imtqlb_legacy(size_t n, double* d, double* e, double* bnd) {
+static void imtqlb_legacy(size_t n, real* d, real* e, real* bnd) {
     if (n == 1) return;
     bnd[0] = 1.0;
     size_t last = n - 1;
@@ -600,12 +609,12 @@ static void imtqlb_legacy(size_t n, double* d, double* e, double* bnd) {
             size_t m = l;
             while (m < n) {
                 if (m == last) break;
-                double test = std::fabs(d[m]) + std::fabs(d[m + 1]);
+                real test = std::fabs(d[m]) + std::fabs(d[m + 1]);
                 if (compare(test, test + std::fabs(e[m]))) break;
                 ++m;
             }
-            double p = d[l];
-            double f = bnd[l];
+            real p = d[l];
+            real f = bnd[l];
             if (m == l) {
                 bool exchange = true;
                 if (l > 0) {
@@ -623,17 +632,17 @@ static void imtqlb_legacy(size_t n, double* d, double* e, double* bnd) {
                 if (iteration == 30)
                     throw Error(E_IMTQLB, "svdlibrs/imtqlb: imtqlb no convergence to an eigenvalue after 30 iterations");
                 ++iteration;
-                double g = (d[l + 1] - p) / (2.0 * e[l]);
-                double r = svd_pythag_legacy(g, 1.0);
+                real g = (d[l + 1] - p) / (2.0 * e[l]);
+                real r = svd_pythag_legacy(g, 1.0);
                 g = d[m] - p + e[l] / (g + svd_fsign(r, g));
-                double s = 1.0, c = 1.0;
+                real s = 1.0, c = 1.0;
                 p = 0.0;
                 if (m == 0) throw Error(E_PANIC, "imtqlb: expected 'm' to be non-zero");
                 i = m - 1;
                 bool underflow = false;
                 while (!underflow && i >= l) {
                     f = s * e[i];
-                    double b = c * e[i];
+                    real b = c * e[i];
                     r = svd_pythag_legacy(f, g);
                     e[i + 1] = r;
                     if (compare(r, 0.0)) { underflow = true; break; }
@@ -662,9 +671,9 @@ static void imtqlb_legacy(size_t n, double* d, double* e, double* bnd) {
 // startv / stpone / lanczos_step / purge / ortbnd / error_bound
 // mod.rs:587-899 (identical in legacy.rs:1100-1540)
 // ---------------------------------------------------------------------------
-static double startv(const SMat& A, Work& w, size_t step, Store& store, uint32_t seed) {
+static real startv(const SMat& A, Work& w, size_t step, Store& store, uint32_t seed) {
     size_t n = w.ncols;
-    double rnm2 = svd_ddot(w.w0.data(), w.w0.data(), n);
+    real rnm2 = svd_ddot(w.w0.data(), w.w0.data(), n);
     for (int id = 0; id < 3; ++id) {
         if (id > 0 || step > 0 || compare(rnm2, 0.0)) start_vector(seed, w.w0.data(), n);
         w.w3 = w.w0;
@@ -680,37 +689,37 @@ static double startv(const SMat& A, Work& w, size_t step, Store& store, uint32_t
     }
     if (step > 0) {
         for (size_t i = 0; i < step; ++i) {
-            const double* v = store.retrq(i);
+            const real* v = store.retrq(i);
             svd_daxpy(-svd_ddot(w.w3.data(), v, n), v, w.w0.data(), n);
         }
         svd_daxpy(-svd_ddot(w.w4.data(), w.w0.data(), n), w.w2.data(), w.w0.data(), n);
         w.w3 = w.w0;
-        double dot = svd_ddot(w.w3.data(), w.w3.data(), n);
+        real dot = svd_ddot(w.w3.data(), w.w3.data(), n);
         rnm2 = (dot <= EPS * rnm2) ? 0.0 : dot;
     }
     return std::sqrt(rnm2);
 }
 
-static void stpone(const SMat& A, Work& w, Store& store, uint32_t seed, double& rnm_out, double& tol_out) {
+static void stpone(const SMat& A, Work& w, Store& store, uint32_t seed, real& rnm_out, real& tol_out) {
     size_t n = w.ncols;
-    double rnm = startv(A, w, 0, store, seed);
+    real rnm = startv(A, w, 0, store, seed);
     if (compare(rnm, 0.0)) throw Error(E_STPONE, "svdlibrs/stpone: rnm == 0.0");
     svd_datx(1.0 / rnm, w.w0.data(), w.w1.data(), n);
     svd_dscal(1.0 / rnm, w.w3.data(), n);
     svd_opb(A, w.w3.data(), w.w0.data(), w.temp.data(), w.transposed);
     w.alf[0] = svd_ddot(w.w0.data(), w.w3.data(), n);
     svd_daxpy(-w.alf[0], w.w1.data(), w.w0.data(), n);
-    double t = svd_ddot(w.w0.data(), w.w3.data(), n);
+    real t = svd_ddot(w.w0.data(), w.w3.data(), n);
     w.alf[0] += t;
     svd_daxpy(-t, w.w1.data(), w.w0.data(), n);
     w.w4 = w.w0;
     rnm = svd_norm(w.w4.data(), n);
-    double anorm = rnm + std::fabs(w.alf[0]);
+    real anorm = rnm + std::fabs(w.alf[0]);
     rnm_out = rnm;
     tol_out = std::sqrt(EPS) * anorm;
 }
 
-static void ortbnd(Work& w, size_t step, double rnm, double eps1) {
+static void ortbnd(Work& w, size_t step, real rnm, real eps1) {
     if (step < 1) return;
     if (!compare(rnm, 0.0) && step > 1) {
         w.oldeta[0] = (w.bet[1] * w.eta[1] + (w.alf[0] - w.alf[step]) * w.eta[0] -
@@ -727,23 +736,23 @@ static void ortbnd(Work& w, size_t step, double rnm, double eps1) {
 
 static size_t g_purge_count = 0;
 
-static void purge(size_t n, size_t ll, Work& w, size_t step, double& rnm, double tol, Store& store) {
+static void purge(size_t n, size_t ll, Work& w, size_t step, real& rnm, real tol, Store& store) {
     if (step < ll + 2) return;
-    double reps = std::sqrt(EPS);
-    double eps1 = EPS * std::sqrt((double)n);
+    real reps = std::sqrt(EPS);
+    real eps1 = EPS * std::sqrt((real)n);
     size_t k = svd_idamax(step - (ll + 1), w.eta.data()) + ll;
     if (std::fabs(w.eta[k]) > reps) {
         ++g_purge_count;
-        double reps1 = eps1 / reps;
+        real reps1 = eps1 / reps;
         int iteration = 0;
         bool flag = true;
         size_t nn = w.ncols;
         while (iteration < 2 && flag) {
             if (rnm > tol) {
-                double tq = 0.0, tr = 0.0;
+                real tq = 0.0, tr = 0.0;
                 for (size_t i = ll; i < step; ++i) {
-                    const double* v = store.retrq(i);
-                    double t = svd_ddot(v, w.w3.data(), nn);
+                    const real* v = store.retrq(i);
+                    real t = svd_ddot(v, w.w3.data(), nn);
                     tq += std::fabs(t);
                     svd_daxpy(-t, v, w.w1.data(), nn);
                     t = svd_ddot(v, w.w4.data(), nn);
@@ -751,7 +760,7 @@ static void purge(size_t n, size_t ll, Work& w, size_t step, double& rnm, double
                     svd_daxpy(-t, v, w.w0.data(), nn);
                 }
                 w.w3 = w.w1;
-                double t = svd_ddot(w.w0.data(), w.w3.data(), nn);
+                real t = svd_ddot(w.w0.data(), w.w3.data(), nn);
                 tr += std::fabs(t);
                 svd_daxpy(-t, w.w1.data(), w.w0.data(), nn);
                 w.w4 = w.w0;
@@ -765,9 +774,9 @@ static void purge(size_t n, size_t ll, Work& w, size_t step, double& rnm, double
 }
 
 static size_t lanczos_step(const SMat& A, Work& w, size_t first, size_t last, size_t& ll, bool& enough,
-                           double& rnm, double& tol, Store& store) {
+                           real& rnm, real& tol, Store& store) {
     size_t n = w.ncols;
-    double eps1 = EPS * std::sqrt((double)n);
+    real eps1 = EPS * std::sqrt((real)n);
     size_t j = first;
     while (j < last) {
         std::swap(w.w1, w.w2);
@@ -788,12 +797,12 @@ static size_t lanczos_step(const SMat& A, Work& w, size_t first, size_t last, si
         svd_daxpy(-w.alf[j], w.w1.data(), w.w0.data(), n);
         if (j <= MAXLL && std::fabs(w.alf[j - 1]) > 4.0 * std::fabs(w.alf[j])) ll = j;
         for (size_t i = 0; i < std::min(j - 1, ll); ++i) {
-            double t = svd_ddot(store.retrp(i), w.w0.data(), n);
+            real t = svd_ddot(store.retrp(i), w.w0.data(), n);
             svd_daxpy(-t, store.retrq(i), w.w0.data(), n);
             w.eta[i] = eps1;
             w.oldeta[i] = eps1;
         }
-        double t = svd_ddot(w.w0.data(), w.w4.data(), n);
+        real t = svd_ddot(w.w0.data(), w.w4.data(), n);
         svd_daxpy(-t, w.w2.data(), w.w0.data(), n);
         if (w.bet[j] > 0.0) w.bet[j] += t;
         t = svd_ddot(w.w0.data(), w.w3.data(), n);
@@ -801,7 +810,7 @@ static size_t lanczos_step(const SMat& A, Work& w, size_t first, size_t last, si
         w.alf[j] += t;
         w.w4 = w.w0;
         rnm = svd_norm(w.w4.data(), n);
-        double anorm = w.bet[j] + std::fabs(w.alf[j]) + rnm;
+        real anorm = w.bet[j] + std::fabs(w.alf[j]) + rnm;
         tol = std::sqrt(EPS) * anorm;
         ortbnd(w, j, rnm, eps1);
         purge(w.ncols, ll, w, j, rnm, tol, store);
@@ -811,11 +820,11 @@ static size_t lanczos_step(const SMat& A, Work& w, size_t first, size_t last, si
     return j;
 }
 
-static size_t error_bound(bool& enough, double endl, double endr, double* ritz, double* bnd, size_t step,
-                          double tol) {
+static size_t error_bound(bool& enough, real endl, real endr, real* ritz, real* bnd, size_t step,
+                          real tol) {
     if (step == 0) throw Error(E_PANIC, "error_bound: expected 'step' to be non-zero");
     size_t mid = svd_idamax(step + 1, bnd);
-    double e34 = eps34();
+    real e34 = eps34();
     size_t i = ((step + 1) + (step - 1)) / 2;
     while (i > mid + 1) {
         if (std::fabs(ritz[i - 1] - ritz[i]) < e34 * std::fabs(ritz[i]) && bnd[i] > tol && bnd[i - 1] > tol) {
@@ -833,9 +842,9 @@ static size_t error_bound(bool& enough, double endl, double endr, double* ritz, 
         ++i;
     }
     size_t neig = 0;
-    double gapl = ritz[step] - ritz[0];
+    real gapl = ritz[step] - ritz[0];
     for (size_t k = 0; k <= step; ++k) {
-        double gap = gapl;
+        real gap = gapl;
         if (k < step) gapl = ritz[k + 1] - ritz[k];
         gap = fmin_(gap, gapl);
         if (gap > bnd[k]) bnd[k] *= bnd[k] / gap;
@@ -849,7 +858,7 @@ static size_t error_bound(bool& enough, double endl, double endr, double* ritz, 
 
 // imtql2: current mod.rs:901-1028 (pythag as written, max iterations by
 // sparsity) / legacy legacy.rs:1590-1700 (30 iterations).
-static void imtql2(size_t nm, size_t n, double* d, double* e, double* z, const Mode& md) {
+static void imtql2(size_t nm, size_t n, real* d, real* e, real* z, const Mode& md) {
     size_t max_it = md.max_imtql2;
     if (n == 1) return;
     size_t last = n - 1;
@@ -862,7 +871,7 @@ static void imtql2(size_t nm, size_t n, double* d, double* e, double* z, const M
             size_t m = l;
             while (m < n) {
                 if (m == last) break;
-                double test = std::fabs(d[m]) + std::fabs(d[m + 1]);
+                real test = std::fabs(d[m]) + std::fabs(d[m + 1]);
                 if (compare(test, test + std::fabs(e[m]))) break;
                 ++m;
             }
@@ -874,15 +883,15 @@ static void imtql2(size_t nm, size_t n, double* d, double* e, double* z, const M
                 throw Error(E_IMTQL2, buf);
             }
             ++iteration;
-            double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
-            double r = md.legacy ? svd_pythag_legacy(g, 1.0) : svd_pythag_current(g, 1.0);
+            real g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+            real r = md.legacy ? svd_pythag_legacy(g, 1.0) : svd_pythag_current(g, 1.0);
             g = d[m] - d[l] + e[l] / (g + svd_fsign(r, g));
-            double s = 1.0, c = 1.0, p = 0.0;
+            real s = 1.0, c = 1.0, p = 0.0;
             size_t i = m - 1;
             bool underflow = false;
             while (!underflow && i >= l) {
-                double f = s * e[i];
-                double b = c * e[i];
+                real f = s * e[i];
+                real b = c * e[i];
                 r = md.legacy ? svd_pythag_legacy(f, g) : svd_pythag_current(f, g);
                 e[i + 1] = r;
                 if (compare(r, 0.0)) underflow = true;
@@ -911,7 +920,7 @@ static void imtql2(size_t nm, size_t n, double* d, double* e, double* z, const M
     }
     for (size_t l = 1; l < n; ++l) {
         size_t i = l - 1, k = i;
-        double p = d[i];
+        real p = d[i];
         for (size_t j = l; j < n; ++j)
             if (d[j] < p) { k = j; p = d[j]; }
         if (k != i) {
@@ -923,12 +932,12 @@ static void imtql2(size_t nm, size_t n, double* d, double* e, double* z, const M
 }
 
 // rotate_array, mod.rs:1030-1053 / legacy.rs:1702-1725
-static void rotate_array(double* a, size_t n, size_t x) {
+static void rotate_array(real* a, size_t n, size_t x) {
     size_t j = 0, start = 0;
-    double t1 = a[0];
+    real t1 = a[0];
     for (size_t c = 0; c < n; ++c) {
         j = (j >= x) ? j - x : j + n - x;
-        double t2 = a[j];
+        real t2 = a[j];
         a[j] = t1;
         if (j == start) { ++j; start = j; t1 = a[j]; }
         else t1 = t2;
@@ -936,51 +945,51 @@ static void rotate_array(double* a, size_t n, size_t x) {
 }
 
 struct Trace {  // per-run internals exposed to the tests
-    std::vector<double> alf, bet, ritz, bnd;
+    std::vector<real> alf, bet, ritz, bnd;
     size_t steps = 0, neig = 0, nsig = 0, purges = 0;
-    double sparsity = 0.0;
+    real sparsity = 0.0;
     bool imtqlb_warned = false;
 };
 
 struct Raw {
     size_t d = 0, nsig = 0, ut_cols = 0, vt_cols = 0;
-    std::vector<double> ut, s, vt;
+    std::vector<real> ut, s, vt;
 };
 
 // ritvec: current mod.rs:1056-1259; legacy legacy.rs:1766-1850
-static Raw ritvec(const SMat& A, size_t dimensions, double kappa, Work& w, size_t steps, size_t neig,
+static Raw ritvec(const SMat& A, size_t dimensions, real kappa, Work& w, size_t steps, size_t neig,
                   Store& store, const Mode& md) {
     size_t js = steps + 1, jsq = js * js;
-    std::vector<double> s(jsq, 0.0);
+    std::vector<real> s(jsq, 0.0);
     for (size_t i = 0; i < jsq; i += js + 1) s[i] = 1.0;
     Raw R;
     size_t cols = w.ncols;
-    std::vector<double> vt(cols * dimensions, 0.0);
+    std::vector<real> vt(cols * dimensions, 0.0);
     svd_dcopy(js, 0, w.alf.data(), vt.data());
     svd_dcopy(steps, 1, w.bet.data(), w.w5.data());
     imtql2(js, js, vt.data(), w.w5.data(), s.data(), md);
 
-    std::vector<std::vector<double>> rows;  // selected Vt rows, in output order
+    std::vector<std::vector<real>> rows;  // selected Vt rows, in output order
     size_t nsig = 0;
     if (!md.legacy) {
-        double ae = md.adaptive_eps;
-        double max_eig = 0.0;
-        for (double v : vt) max_eig = fmax_(max_eig, std::fabs(v));
-        double akappa = md.sparsity > 0.99 ? kappa * 10.0 : kappa;
+        real ae = md.adaptive_eps;
+        real max_eig = 0.0;
+        for (real v : vt) max_eig = fmax_(max_eig, std::fabs(v));
+        real akappa = md.sparsity > 0.99 ? kappa * 10.0 : kappa;
         std::vector<size_t> sig;
         for (size_t k = 0; k < js; ++k) {
-            double rel = akappa * fmax_(std::fabs(w.ritz[k]), max_eig * ae);
+            real rel = akappa * fmax_(std::fabs(w.ritz[k]), max_eig * ae);
             if (w.bnd[k] <= rel && k + 1 > js - neig) sig.push_back(k);
         }
         nsig = sig.size();
         size_t d = std::min(dimensions, nsig);
         for (size_t r = 0; r < d; ++r) {
             size_t k = sig[r];
-            std::vector<double> vec(cols, 0.0);
+            std::vector<real> vec(cols, 0.0);
             for (size_t i = 0; i < js; ++i) {
-                double c = s[k * js + i];
+                real c = s[k * js + i];
                 if (std::fabs(c) > ae) {
-                    const double* q = store.retrq(i);
+                    const real* q = store.retrq(i);
                     for (size_t j = 0; j < cols; ++j) vec[j] += c * q[j];
                 }
             }
@@ -997,7 +1006,7 @@ static Raw ritvec(const SMat& A, size_t dimensions, double kappa, Work& w, size_
                 for (size_t i = 0; i < js; ++i) {
                     idx -= js;
                     if (s[idx] != 0.0) {
-                        const double* q = store.retrq(i);
+                        const real* q = store.retrq(i);
                         for (size_t j = 0; j < cols; ++j) vt[j + off] += s[idx] * q[j];
                     }
                 }
@@ -1018,34 +1027,34 @@ static Raw ritvec(const SMat& A, size_t dimensions, double kappa, Work& w, size_
     R.s.assign(d, 0.0);
     R.ut.assign(d * w.nrows, 0.0);
     R.vt.assign(d * cols, 0.0);
-    std::vector<double> tmp(cols);
+    std::vector<real> tmp(cols);
     for (size_t i = 0; i < d; ++i) {
-        const double* v = rows[i].data();
-        double* ut = R.ut.data() + i * w.nrows;
+        const real* v = rows[i].data();
+        real* ut = R.ut.data() + i * w.nrows;
         svd_opb(A, v, tmp.data(), w.temp.data(), w.transposed);
         A.svd_opa(v, ut, w.transposed);
-        double t = svd_ddot(v, tmp.data(), cols);
+        real t = svd_ddot(v, tmp.data(), cols);
         if (!md.legacy) {
-            double sval = std::sqrt(fmax_(t, 0.0));
+            real sval = std::sqrt(fmax_(t, 0.0));
             R.s[i] = sval;
-            double ae = md.adaptive_eps;
+            real ae = md.adaptive_eps;
             if (sval > ae) svd_dscal(1.0 / sval, ut, w.nrows);
             else svd_dscal(1.0 / fmax_(sval, ae), ut, w.nrows);
         } else {
-            double sval = std::sqrt(t);
+            real sval = std::sqrt(t);
             R.s[i] = sval;
             svd_dscal(1.0 / sval, ut, w.nrows);
         }
-        std::memcpy(R.vt.data() + i * cols, v, cols * sizeof(double));
+        std::memcpy(R.vt.data() + i * cols, v, cols * sizeof(real));
     }
     return R;
 }
 
-static size_t lanso(const SMat& A, size_t dim, size_t iterations, double endl, double endr, Work& w,
+static size_t lanso(const SMat& A, size_t dim, size_t iterations, real endl, real endr, Work& w,
                     size_t& neig, Store& store, uint32_t seed, const Mode& md, Trace* tr) {
-    double rnm, tol;
+    real rnm, tol;
     stpone(A, w, store, seed, rnm, tol);
-    double eps1 = (md.legacy ? EPS : md.adaptive_eps) * std::sqrt((double)w.ncols);
+    real eps1 = (md.legacy ? EPS : md.adaptive_eps) * std::sqrt((real)w.ncols);
     w.eta[0] = eps1;
     w.oldeta[0] = eps1;
     size_t ll = 0, first = 1;
@@ -1102,13 +1111,13 @@ struct Las2Result {
     Raw raw;
     size_t dimensions = 0, iterations = 0, nnz = 0, steps = 0, neig = 0;
     bool transposed = false;
-    double kappa = 0.0;
+    real kappa = 0.0;
     uint32_t seed = 0;
 };
 
 // svd_las2: mod.rs:104-189 / legacy svdLAS2 legacy.rs:569-654
-static Las2Result svd_las2(const SMat& A, size_t dimensions, size_t iterations, double endl, double endr,
-                           double kappa, uint32_t seed, bool legacy, Trace* tr) {
+static Las2Result svd_las2(const SMat& A, size_t dimensions, size_t iterations, real endl, real endr,
+                           real kappa, uint32_t seed, bool legacy, Trace* tr) {
     if (seed == 0) seed = std::random_device{}();
     size_t mn = std::min(A.nrows(), A.ncols());
     if (dimensions == 0 || dimensions > mn) dimensions = mn;
@@ -1120,7 +1129,7 @@ static Las2Result svd_las2(const SMat& A, size_t dimensions, size_t iterations, 
                                          : "svdlibrs/svdLas2: svd_las2: insufficient dimensions: %zu", dimensions);
         throw Error(E_LAS2, buf);
     }
-    bool transposed = (double)A.ncols() >= (double)A.nrows() * 1.2;
+    bool transposed = (real)A.ncols() >= (real)A.nrows() * 1.2;
     size_t nrows = transposed ? A.ncols() : A.nrows();
     size_t ncols = transposed ? A.nrows() : A.ncols();
     Work w(nrows, ncols, transposed, iterations);
@@ -1137,7 +1146,7 @@ static Las2Result svd_las2(const SMat& A, size_t dimensions, size_t iterations, 
         tr->purges = g_purge_count;
         tr->sparsity = sparsity_of(A);
     }
-    double kap = fmax_(std::fabs(kappa), eps34());
+    real kap = fmax_(std::fabs(kappa), eps34());
     Las2Result res;
     res.raw = ritvec(A, dimensions, kap, w, steps, neig, store, md);
     if (transposed) {
@@ -1171,11 +1180,11 @@ static Las2Result svd_las2(const SMat& A, size_t dimensions, size_t iterations, 
 // ---------------------------------------------------------------------------
 struct DMatrix {
     size_t r = 0, c = 0;
-    std::vector<double> a;  // column-major
+    std::vector<real> a;  // column-major
     DMatrix() {}
     DMatrix(size_t r_, size_t c_) : r(r_), c(c_), a(r_ * c_, 0.0) {}
-    double& operator()(size_t i, size_t j) { return a[i + j * r]; }
-    double operator()(size_t i, size_t j) const { return a[i + j * r]; }
+    real& operator()(size_t i, size_t j) { return a[i + j * r]; }
+    real operator()(size_t i, size_t j) const { return a[i + j * r]; }
 };
 
 // masked multiply_with_dense, masked.rs:265-471.  compat_d3 reproduces the
@@ -1185,18 +1194,18 @@ static void masked_multiply_with_dense(const MaskedOp& M, const DMatrix& dense, 
     const Compressed* a = M.a;
     const uint64_t* p = a->ptr.data();
     const uint64_t* ci = a->idx.data();
-    const double* v = a->val.data();
+    const real* v = a->val.data();
     size_t l = dense.c;
     if (!transpose_self) {
         size_t rows = a->nmajor;
         result = DMatrix(rows, l);
 #pragma omp parallel for schedule(dynamic, 64) num_threads(g_threads) if (g_threads > 1)
         for (size_t row = 0; row < rows; ++row) {
-            std::vector<double> acc(l, 0.0);
+            std::vector<real> acc(l, 0.0);
             for (uint64_t j = p[row]; j < p[row + 1]; ++j) {
                 int64_t mc = M.o2m[ci[j]];
                 if (mc < 0) continue;
-                double val = v[j];
+                real val = v[j];
                 for (size_t c = 0; c < l; ++c) acc[c] += val * dense((size_t)mc, c);
             }
             for (size_t c = 0; c < l; ++c) result(row, c) = acc[c];
@@ -1207,12 +1216,12 @@ static void masked_multiply_with_dense(const MaskedOp& M, const DMatrix& dense, 
     result = DMatrix(nm, l);
     size_t cs = determine_chunk_size(nrows);
     size_t nch = (nrows + cs - 1) / cs;
-    std::vector<std::vector<double>> loc(nch);
+    std::vector<std::vector<real>> loc(nch);
 #pragma omp parallel for schedule(dynamic, 1) num_threads(g_threads) if (g_threads > 1)
     for (size_t ch = 0; ch < nch; ++ch) {
-        std::vector<double> lr(nm * l, 0.0);
+        std::vector<real> lr(nm * l, 0.0);
         size_t s = ch * cs, e = std::min(s + cs, nrows);
-        std::vector<double> drow(l);
+        std::vector<real> drow(l);
         for (size_t i = s; i < e; ++i) {
             for (size_t c = 0; c < l; ++c) {
                 if (compat_d3) {
@@ -1223,7 +1232,7 @@ static void masked_multiply_with_dense(const MaskedOp& M, const DMatrix& dense, 
             for (uint64_t j = p[i]; j < p[i + 1]; ++j) {
                 int64_t mc = M.o2m[ci[j]];
                 if (mc < 0) continue;
-                double val = v[j];
+                real val = v[j];
                 size_t base = (size_t)mc * l;
                 for (size_t c = 0; c < l; ++c) lr[base + c] += val * drow[c];
             }
@@ -1233,7 +1242,7 @@ static void masked_multiply_with_dense(const MaskedOp& M, const DMatrix& dense, 
     for (size_t ch = 0; ch < nch; ++ch)
         for (size_t r = 0; r < nm; ++r)
             for (size_t c = 0; c < l; ++c) {
-                double val = loc[ch][r * l + c];
+                real val = loc[ch][r * l + c];
                 if (val != 0.0) result(r, c) += val;
             }
 }
@@ -1243,21 +1252,21 @@ static void masked_multiply_transposed_by_dense(const MaskedOp& M, const DMatrix
     const Compressed* a = M.a;
     const uint64_t* p = a->ptr.data();
     const uint64_t* ci = a->idx.data();
-    const double* v = a->val.data();
+    const real* v = a->val.data();
     size_t qc = q.c, nm = M.ncols(), nrows = a->nmajor;
     result = DMatrix(qc, nm);
     size_t cs = determine_chunk_size(nrows);
     size_t nch = (nrows + cs - 1) / cs;
-    std::vector<std::vector<double>> loc(nch);
+    std::vector<std::vector<real>> loc(nch);
 #pragma omp parallel for schedule(dynamic, 1) num_threads(g_threads) if (g_threads > 1)
     for (size_t ch = 0; ch < nch; ++ch) {
-        std::vector<double> lr(qc * nm, 0.0);  // column-major qc x nm
+        std::vector<real> lr(qc * nm, 0.0);  // column-major qc x nm
         size_t s = ch * cs, e = std::min(s + cs, nrows);
         for (size_t row = s; row < e; ++row)
             for (uint64_t idx = p[row]; idx < p[row + 1]; ++idx) {
                 int64_t mc = M.o2m[ci[idx]];
                 if (mc < 0) continue;
-                double sv = v[idx];
+                real sv = v[idx];
                 for (size_t c = 0; c < qc; ++c) lr[c + (size_t)mc * qc] += q(row, c) * sv;
             }
         loc[ch].swap(lr);
@@ -1265,7 +1274,7 @@ static void masked_multiply_transposed_by_dense(const MaskedOp& M, const DMatrix
     for (size_t ch = 0; ch < nch; ++ch)
         for (size_t cc = 0; cc < nm; ++cc)
             for (size_t r = 0; r < qc; ++r) {
-                double val = loc[ch][r + cc * qc];
+                real val = loc[ch][r + cc * qc];
                 if (val != 0.0) result(r, cc) += val;
             }
 }
@@ -1275,22 +1284,22 @@ static void masked_multiply_transposed_by_dense(const MaskedOp& M, const DMatrix
 static DMatrix thin_q(const DMatrix& X) {
     size_t m = X.r, n = X.c, k = std::min(m, n);
     DMatrix A = X;
-    std::vector<std::vector<double>> vs(k);
-    std::vector<double> betas(k, 0.0);
+    std::vector<std::vector<real>> vs(k);
+    std::vector<real> betas(k, 0.0);
     for (size_t j = 0; j < k; ++j) {
-        double norm = 0.0;
+        real norm = 0.0;
         for (size_t i = j; i < m; ++i) norm += A(i, j) * A(i, j);
         norm = std::sqrt(norm);
-        std::vector<double> v(m - j, 0.0);
+        std::vector<real> v(m - j, 0.0);
         if (norm == 0.0) { vs[j] = v; betas[j] = 0.0; continue; }
-        double alpha = A(j, j) >= 0 ? -norm : norm;
+        real alpha = A(j, j) >= 0 ? -norm : norm;
         for (size_t i = j; i < m; ++i) v[i - j] = A(i, j);
         v[0] -= alpha;
-        double vn = 0.0;
-        for (double t : v) vn += t * t;
-        double beta = vn > 0 ? 2.0 / vn : 0.0;
+        real vn = 0.0;
+        for (real t : v) vn += t * t;
+        real beta = vn > 0 ? 2.0 / vn : 0.0;
         for (size_t c = j; c < n; ++c) {
-            double dot = 0.0;
+            real dot = 0.0;
             for (size_t i = j; i < m; ++i) dot += v[i - j] * A(i, c);
             dot *= beta;
             for (size_t i = j; i < m; ++i) A(i, c) -= dot * v[i - j];
@@ -1301,11 +1310,11 @@ static DMatrix thin_q(const DMatrix& X) {
     DMatrix Q(m, k);
     for (size_t j = 0; j < k; ++j) Q(j, j) = 1.0;
     for (size_t jj = k; jj-- > 0;) {
-        const std::vector<double>& v = vs[jj];
-        double beta = betas[jj];
+        const std::vector<real>& v = vs[jj];
+        real beta = betas[jj];
         if (beta == 0.0) continue;
         for (size_t c = 0; c < k; ++c) {
-            double dot = 0.0;
+            real dot = 0.0;
             for (size_t i = jj; i < m; ++i) dot += v[i - jj] * Q(i, c);
             dot *= beta;
             for (size_t i = jj; i < m; ++i) Q(i, c) -= dot * v[i - jj];
@@ -1317,11 +1326,11 @@ static DMatrix thin_q(const DMatrix& X) {
 // normalize_columns, randomized/mod.rs:239-293
 static void normalize_columns(DMatrix& M) {
     for (size_t j = 0; j < M.c; ++j) {
-        double norm = 0.0;
+        real norm = 0.0;
         for (size_t i = 0; i < M.r; ++i) norm += M(i, j) * M(i, j);
         norm = std::sqrt(norm);
         if (norm > 1e-10) {
-            double scale = 1.0 / norm;
+            real scale = 1.0 / norm;
             for (size_t i = 0; i < M.r; ++i) M(i, j) *= scale;
         }
     }
@@ -1330,7 +1339,7 @@ static void normalize_columns(DMatrix& M) {
 // One-sided Jacobi SVD of B (l x n): columns of B^T are orthogonalised.
 // Returns U_B (l x r), sigma (r, descending), V_B^T (r x n), r = min(l, n);
 // stands in for nalgebra's b.svd(true, true) (randomized/mod.rs:160).
-static void jacobi_svd(const DMatrix& B, DMatrix& U, std::vector<double>& sig, DMatrix& Vt) {
+static void jacobi_svd(const DMatrix& B, DMatrix& U, std::vector<real>& sig, DMatrix& Vt) {
     size_t l = B.r, n = B.c;
     bool wide = n >= l;
     // Work on W (p x q) with p >= q: W = B^T if wide else B
@@ -1340,38 +1349,38 @@ static void jacobi_svd(const DMatrix& B, DMatrix& U, std::vector<double>& sig, D
         for (size_t j = 0; j < q; ++j) W(i, j) = wide ? B(j, i) : B(i, j);
     for (size_t j = 0; j < q; ++j) V(j, j) = 1.0;
     for (int sweep = 0; sweep < 80; ++sweep) {
-        double off = 0.0;
+        real off = 0.0;
         for (size_t a = 0; a + 1 < q; ++a)
             for (size_t b = a + 1; b < q; ++b) {
-                double al = 0, be = 0, ga = 0;
+                real al = 0, be = 0, ga = 0;
                 for (size_t i = 0; i < p; ++i) {
                     al += W(i, a) * W(i, a);
                     be += W(i, b) * W(i, b);
                     ga += W(i, a) * W(i, b);
                 }
                 if (ga == 0.0) continue;
-                double conv = std::fabs(ga) / std::sqrt(al * be);
+                real conv = std::fabs(ga) / std::sqrt(al * be);
                 if (!(conv > 1e-15)) continue;
                 off = std::max(off, conv);
-                double zeta = (be - al) / (2.0 * ga);
-                double t = (zeta >= 0 ? 1.0 : -1.0) / (std::fabs(zeta) + std::sqrt(1.0 + zeta * zeta));
-                double c = 1.0 / std::sqrt(1.0 + t * t), s = c * t;
+                real zeta = (be - al) / (2.0 * ga);
+                real t = (zeta >= 0 ? 1.0 : -1.0) / (std::fabs(zeta) + std::sqrt(1.0 + zeta * zeta));
+                real c = 1.0 / std::sqrt(1.0 + t * t), s = c * t;
                 for (size_t i = 0; i < p; ++i) {
-                    double x = W(i, a), y = W(i, b);
+                    real x = W(i, a), y = W(i, b);
                     W(i, a) = c * x - s * y;
                     W(i, b) = s * x + c * y;
                 }
                 for (size_t i = 0; i < q; ++i) {
-                    double x = V(i, a), y = V(i, b);
+                    real x = V(i, a), y = V(i, b);
                     V(i, a) = c * x - s * y;
                     V(i, b) = s * x + c * y;
                 }
             }
         if (off < 1e-15) break;
     }
-    std::vector<double> nrm(q);
+    std::vector<real> nrm(q);
     for (size_t j = 0; j < q; ++j) {
-        double s2 = 0;
+        real s2 = 0;
         for (size_t i = 0; i < p; ++i) s2 += W(i, j) * W(i, j);
         nrm[j] = std::sqrt(s2);
     }
@@ -1403,9 +1412,9 @@ static void jacobi_svd(const DMatrix& B, DMatrix& U, std::vector<double>& sig, D
 
 struct RandResult {
     size_t d = 0, m = 0, n = 0;
-    std::vector<double> u;   // m x d row-major
-    std::vector<double> s;   // d
-    std::vector<double> vt;  // d x n row-major
+    std::vector<real> u;   // m x d row-major
+    std::vector<real> s;   // d
+    std::vector<real> vt;  // d x n row-major
     // wall time by what it scales with: sparse products (nnz), work on
     // m-row dense matrices (rows), work on n-row matrices and the small SVD (fixed)
     double t_sparse = 0, t_rows = 0, t_fixed = 0;
@@ -1417,32 +1426,32 @@ static double wall() {
 
 // compute_column_means (masked.rs:240-263): sums of the masked columns over
 // the rows, times 1/nrows
-static std::vector<double> column_means(const MaskedOp& M) {
+static std::vector<real> column_means(const MaskedOp& M) {
     const Compressed* a = M.a;
-    std::vector<double> mu(M.ncols(), 0.0);
+    std::vector<real> mu(M.ncols(), 0.0);
     for (size_t i = 0; i < a->nmajor; ++i)
         for (uint64_t j = a->ptr[i]; j < a->ptr[i + 1]; ++j) {
             int64_t mc = M.o2m[a->idx[j]];
             if (mc >= 0) mu[(size_t)mc] += a->val[j];
         }
-    const double rc = 1.0 / (double)a->nmajor;
-    for (double& v : mu) v *= rc;
+    const real rc = 1.0 / (real)a->nmajor;
+    for (real& v : mu) v *= rc;
     return mu;
 }
 
 // Products of the centred matrix A - 1 mu^T (mean_center, mod.rs:46-53), by
 // the rank-1 corrections A X - 1 (mu^T X) and A^T Y - mu (1^T Y).  The crate's
 // own adjustments (masked.rs:496-509, 793-809) differ from this algebra.
-static void center_rows(DMatrix& y, const DMatrix& x, const std::vector<double>& mu) {
+static void center_rows(DMatrix& y, const DMatrix& x, const std::vector<real>& mu) {
     for (size_t c = 0; c < y.c; ++c) {
-        double t = 0.0;
+        real t = 0.0;
         for (size_t j = 0; j < mu.size(); ++j) t += mu[j] * x(j, c);
         for (size_t i = 0; i < y.r; ++i) y(i, c) -= t;
     }
 }
-static void center_cols(DMatrix& z, const DMatrix& y, const std::vector<double>& mu) {
+static void center_cols(DMatrix& z, const DMatrix& y, const std::vector<real>& mu) {
     for (size_t c = 0; c < z.c; ++c) {
-        double t = 0.0;
+        real t = 0.0;
         for (size_t i = 0; i < y.r; ++i) t += y(i, c);
         for (size_t j = 0; j < z.r; ++j) z(j, c) -= mu[j] * t;
     }
@@ -1454,13 +1463,13 @@ static RandResult randomized_svd(const MaskedOp& M, size_t target_rank, size_t n
                                  bool mean_center = false) {
     RandResult R;
     size_t m = M.nrows(), n = M.ncols();
-    std::vector<double> mu;
+    std::vector<real> mu;
     if (mean_center) mu = column_means(M);
     size_t rank = std::min(target_rank, std::min(m, n));
     size_t l = rank + n_oversamples;
     DMatrix omega(n, l);
     for (size_t i = 0; i < n; ++i)
-        for (size_t c = 0; c < l; ++c) omega(i, c) = omega_rowmajor[i * l + c];
+        for (size_t c = 0; c < l; ++c) omega(i, c) = (real)omega_rowmajor[i * l + c];  // T::from_f64
     DMatrix y;
     double t = wall();
     auto lap = [&](double& acc) { double now = wall(); acc += now - t; t = now; };
@@ -1490,14 +1499,14 @@ static RandResult randomized_svd(const MaskedOp& M, size_t target_rank, size_t n
     masked_multiply_transposed_by_dense(M, Q, B);
     if (mean_center) {  // B = Q^T (A - 1 mu^T): row c of B loses (1^T Q e_c) mu^T
         for (size_t c = 0; c < B.r; ++c) {
-            double t = 0.0;
+            real t = 0.0;
             for (size_t i = 0; i < Q.r; ++i) t += Q(i, c);
             for (size_t j = 0; j < B.c; ++j) B(c, j) -= t * mu[j];
         }
     }
     lap(R.t_sparse);
     DMatrix Ub, Vt;
-    std::vector<double> sig;
+    std::vector<real> sig;
     jacobi_svd(B, Ub, sig, Vt);
     lap(R.t_fixed);
     size_t r = sig.size();
@@ -1506,7 +1515,7 @@ static RandResult randomized_svd(const MaskedOp& M, size_t target_rank, size_t n
     R.u.assign(m * actual, 0.0);
     for (size_t i = 0; i < m; ++i)
         for (size_t k = 0; k < actual; ++k) {
-            double acc = 0.0;
+            real acc = 0.0;
             for (size_t j = 0; j < Q.c; ++j) acc += Q(i, j) * Ub(j, k);
             R.u[i * actual + k] = acc;
         }
@@ -1541,8 +1550,16 @@ void orc_chacha_block(const uint8_t key[32], uint64_t counter, uint64_t stream, 
     orc::chacha_block(k, counter, stream, rounds, out);
 }
 
-void orc_start_vector(uint32_t seed, double* out, size_t n) { orc::start_vector(seed, out, n); }
+// sizeof(T): 8 for the f64 build, 4 for the f32 build (-DORC_F32)
+int orc_real_bytes() { return (int)sizeof(orc::real); }
 
+void orc_start_vector(uint32_t seed, double* out, size_t n) {
+    std::vector<orc::real> w(n);
+    orc::start_vector(seed, w.data(), n);
+    for (size_t i = 0; i < n; ++i) out[i] = w[i];
+}
+
+#ifndef ORC_F32
 double orc_pythag(double a, double b, int legacy) {
     return legacy ? orc::svd_pythag_legacy(a, b) : orc::svd_pythag_current(a, b);
 }
@@ -1563,6 +1580,7 @@ int orc_imtql2(size_t n, double* d, double* e, double* z, int legacy, size_t max
     try { orc::imtql2(n, n, d, e, z, md); return 0; }
     catch (orc::Error& ex) { g_orc_err = ex.what(); return ex.code; }
 }
+#endif
 
 struct orc_las2_out {
     uint64_t d, ut_rows, ut_cols, vt_rows, vt_cols;
@@ -1586,10 +1604,13 @@ struct orc_las2_out {
     int32_t masked_would_panic;
 };
 
-static double* dup_vec(const std::vector<double>& v) {
+extern "C++" {
+template <typename V>
+static double* dup_vec(const V& v) {
     double* p = (double*)std::malloc(std::max<size_t>(1, v.size()) * sizeof(double));
-    if (!v.empty()) std::memcpy(p, v.data(), v.size() * sizeof(double));
+    for (size_t i = 0; i < v.size(); ++i) p[i] = (double)v[i];
     return p;
+}
 }
 
 void orc_las2_free(orc_las2_out* o) {
@@ -1693,7 +1714,11 @@ int orc_opa(int kind, uint64_t nrows, uint64_t ncols, uint64_t nnz, const uint64
             coo->v.assign(val, val + nnz);
             op.reset(coo);
         } else return orc::E_UNSUPPORTED;
-        op->svd_opa(x, y, transposed != 0);
+        const size_t nx = transposed ? nrows : (kind == 3 ? op->ncols() : ncols);
+        const size_t ny = transposed ? (kind == 3 ? op->ncols() : ncols) : nrows;
+        std::vector<orc::real> xr(x, x + nx), yr(ny);
+        op->svd_opa(xr.data(), yr.data(), transposed != 0);
+        for (size_t i = 0; i < ny; ++i) y[i] = yr[i];
         return 0;
     } catch (std::exception& ex) { g_orc_err = ex.what(); return orc::E_PANIC; }
 }

@@ -8,18 +8,18 @@
 #include "svdb_internal.h"
 
 namespace svdb {
-svdb_matrix* create_csr(uint64_t, uint64_t, uint64_t, const uint64_t*, const uint64_t*, const double*);
-svdb_matrix* create_csc(uint64_t, uint64_t, uint64_t, const uint64_t*, const uint64_t*, const double*);
-svdb_matrix* create_coo(uint64_t, uint64_t, uint64_t, const uint64_t*, const uint64_t*, const double*);
+svdb_matrix* create_csr(uint64_t, uint64_t, uint64_t, const uint64_t*, const uint64_t*, const double*, const float*);
+svdb_matrix* create_csc(uint64_t, uint64_t, uint64_t, const uint64_t*, const uint64_t*, const double*, const float*);
+svdb_matrix* create_coo(uint64_t, uint64_t, uint64_t, const uint64_t*, const uint64_t*, const double*, const float*);
 svdb_matrix* create_csr_device(uint64_t, uint64_t, uint64_t, const int64_t*, const int32_t*, const double*);
 svdb_matrix* masked_new(const svdb_matrix*, const uint8_t*, uint64_t);
 void masked_maps(const svdb_matrix*, int64_t*, int64_t*);
 void destroy(svdb_matrix*);
 void las2(const svdb_matrix*, uint64_t, uint64_t, const double[2], double, uint32_t, bool, const svdb_options&,
-          svdb_rec*);
+          svdb_rec*, bool);
 int las2_plan(uint64_t, uint64_t, uint64_t, uint64_t, uint64_t, uint64_t*, uint64_t*, int32_t*, int32_t*);
 void randomized(const svdb_matrix*, uint64_t, uint64_t, uint64_t, int, int, int, uint64_t, int,
-                const svdb_options&, svdb_rec*);
+                const svdb_options&, svdb_rec*, bool);
 void svd_adjoint(const svdb_matrix*, int64_t, const double*, const double*, const double*, const double*,
                  const double*, const double*, svdb_adjoint_options&, double*);
 void sddmm_device(const svdb_matrix*, const void*, const void*, int64_t, void*, int, cudaStream_t);
@@ -101,21 +101,45 @@ int svdb_matrix_create_csr(uint64_t nrows, uint64_t ncols, uint64_t nnz, const u
                            const uint64_t* indices, const double* values, svdb_matrix** out) {
     return guarded([&] {
         if (!out) throw Error(SVDB_ERR_ARG, "null out");
-        *out = create_csr(nrows, ncols, nnz, indptr, indices, values);
+        *out = create_csr(nrows, ncols, nnz, indptr, indices, values, nullptr);
+    });
+}
+int svdb_matrix_create_csr_f32(uint64_t nrows, uint64_t ncols, uint64_t nnz, const uint64_t* indptr,
+                               const uint64_t* indices, const float* values,
+                               svdb_matrix** out) {
+    return guarded([&] {
+        if (!out) throw Error(SVDB_ERR_ARG, "null out");
+        *out = create_csr(nrows, ncols, nnz, indptr, indices, nullptr, values);
     });
 }
 int svdb_matrix_create_csc(uint64_t nrows, uint64_t ncols, uint64_t nnz, const uint64_t* colptr,
                            const uint64_t* rowidx, const double* values, svdb_matrix** out) {
     return guarded([&] {
         if (!out) throw Error(SVDB_ERR_ARG, "null out");
-        *out = create_csc(nrows, ncols, nnz, colptr, rowidx, values);
+        *out = create_csc(nrows, ncols, nnz, colptr, rowidx, values, nullptr);
+    });
+}
+int svdb_matrix_create_csc_f32(uint64_t nrows, uint64_t ncols, uint64_t nnz, const uint64_t* colptr,
+                               const uint64_t* rowidx, const float* values,
+                               svdb_matrix** out) {
+    return guarded([&] {
+        if (!out) throw Error(SVDB_ERR_ARG, "null out");
+        *out = create_csc(nrows, ncols, nnz, colptr, rowidx, nullptr, values);
     });
 }
 int svdb_matrix_create_coo(uint64_t nrows, uint64_t ncols, uint64_t nnz, const uint64_t* rows, const uint64_t* cols,
                            const double* values, svdb_matrix** out) {
     return guarded([&] {
         if (!out) throw Error(SVDB_ERR_ARG, "null out");
-        *out = create_coo(nrows, ncols, nnz, rows, cols, values);
+        *out = create_coo(nrows, ncols, nnz, rows, cols, values, nullptr);
+    });
+}
+int svdb_matrix_create_coo_f32(uint64_t nrows, uint64_t ncols, uint64_t nnz, const uint64_t* rows,
+                               const uint64_t* cols, const float* values,
+                               svdb_matrix** out) {
+    return guarded([&] {
+        if (!out) throw Error(SVDB_ERR_ARG, "null out");
+        *out = create_coo(nrows, ncols, nnz, rows, cols, nullptr, values);
     });
 }
 int svdb_matrix_create_csr_device(uint64_t nrows, uint64_t ncols, uint64_t nnz, const int64_t* d_indptr,
@@ -355,7 +379,7 @@ static int las2_common(const svdb_matrix* a, uint64_t dimensions, uint64_t itera
         svdb_matrix* am = const_cast<svdb_matrix*>(a);
         std::lock_guard<std::mutex> lk(am->mu);
         DeviceGuard g(a->device);
-        las2(a, dimensions, iterations, ei, kappa, seed, legacy, o, out);
+        las2(a, dimensions, iterations, ei, kappa, seed, legacy, o, out, false);
     });
 }
 
@@ -417,8 +441,115 @@ int svdb_randomized_svd(const svdb_matrix* a, uint64_t target_rank, uint64_t n_o
         std::lock_guard<std::mutex> lk(am->mu);
         DeviceGuard g(a->device);
         randomized(a, target_rank, n_oversamples, n_power_iters, normalizer, mean_center, has_seed, seed, verbose,
-                   o, out);
+                   o, out, false);
     });
+}
+
+// ---- T = f32 entry points: the solver runs with its results in HBM, which
+// are then narrowed to f32 (round to nearest) into the caller's record.
+extern "C++" {
+template <typename Solve>
+static int solve_f32(const svdb_matrix* a, const svdb_options* opts, svdb_rec_f32* out, Solve&& solve) {
+    return guarded([&] {
+        check_handle(a);
+        if (!out) throw Error(SVDB_ERR_ARG, "null out");
+        svdb_options o = opts_or_default(opts);
+        const bool host = !o.result_on_device;
+        o.result_on_device = 1;
+        cudaStream_t s = o.stream ? (cudaStream_t)o.stream : a->stream;
+        svdb_rec r;
+        std::memset(&r, 0, sizeof r);
+        std::memset(out, 0, sizeof(*out));
+        svdb_matrix* am = const_cast<svdb_matrix*>(a);
+        std::lock_guard<std::mutex> lk(am->mu);
+        DeviceGuard g(a->device);
+        solve(o, &r);
+        struct Owned {  // the f64 device record, released stream-ordered on every path
+            svdb_rec* r;
+            cudaStream_t s;
+            ~Owned() {
+                for (double* q : {r->u, r->s, r->vt})
+                    if (q) cudaFreeAsync(q, s);
+            }
+        } owned{&r, s};
+        const int64_t nu = (int64_t)(r.u_rows * r.u_cols), nv = (int64_t)(r.vt_rows * r.vt_cols), ns = (int64_t)r.d;
+        DevBuf<float> u(std::max<int64_t>(nu, 1), s), sv(std::max<int64_t>(ns, 1), s), vt(std::max<int64_t>(nv, 1), s);
+        narrow(r.u, u.p, nu, s);
+        narrow(r.s, sv.p, ns, s);
+        narrow(r.vt, vt.p, nv, s);
+        out->d = r.d;
+        out->u_rows = r.u_rows; out->u_cols = r.u_cols;
+        out->vt_rows = r.vt_rows; out->vt_cols = r.vt_cols;
+        out->diagnostics = r.diagnostics;
+        out->origin = r.origin;
+        out->time_ms_total = r.time_ms_total;
+        out->time_ms_spmv = r.time_ms_spmv;
+        out->time_ms_ortho = r.time_ms_ortho;
+        out->time_ms_tridiag = r.time_ms_tridiag;
+        out->time_ms_ritvec = r.time_ms_ritvec;
+        if (!host) {
+            SVDB_CUDA(cudaStreamSynchronize(s));
+            out->u = u.detach(); out->s = sv.detach(); out->vt = vt.detach();
+            out->on_device = 1;
+            return;
+        }
+        out->u = (float*)malloc(std::max<int64_t>(nu, 1) * sizeof(float));
+        out->s = (float*)malloc(std::max<int64_t>(ns, 1) * sizeof(float));
+        out->vt = (float*)malloc(std::max<int64_t>(nv, 1) * sizeof(float));
+        if (!out->u || !out->s || !out->vt) {
+            free(out->u); free(out->s); free(out->vt);
+            std::memset(out, 0, sizeof(*out));
+            throw std::bad_alloc();
+        }
+        if (nu) SVDB_CUDA(cudaMemcpyAsync(out->u, u.p, nu * sizeof(float), cudaMemcpyDeviceToHost, s));
+        if (ns) SVDB_CUDA(cudaMemcpyAsync(out->s, sv.p, ns * sizeof(float), cudaMemcpyDeviceToHost, s));
+        if (nv) SVDB_CUDA(cudaMemcpyAsync(out->vt, vt.p, nv * sizeof(float), cudaMemcpyDeviceToHost, s));
+        SVDB_CUDA(cudaStreamSynchronize(s));
+        out->on_device = 0;
+    });
+}
+}  // extern "C++"
+
+int svdb_las2_f32(const svdb_matrix* a, uint64_t dimensions, uint64_t iterations, const float end_interval[2],
+                  float kappa, uint32_t random_seed, const svdb_options* opts, svdb_rec_f32* out) {
+    return solve_f32(a, opts, out, [&](const svdb_options& o, svdb_rec* r) {
+        if (o.algorithm == SVDB_LEGACY) throw Error(SVDB_ERR_UNSUPPORTED, "legacy::svdLAS2 is f64-only");
+        const double ei[2] = {end_interval ? (double)end_interval[0] : (double)-1.0e-30f,
+                              end_interval ? (double)end_interval[1] : (double)1.0e-30f};
+        las2(a, dimensions, iterations, ei, (double)kappa, random_seed, false, o, r, true);
+    });
+}
+int svdb_svd_f32(const svdb_matrix* a, svdb_rec_f32* out) {
+    return svdb_las2_f32(a, 0, 0, nullptr, 1.0e-6f, 0, nullptr, out);
+}
+int svdb_svd_dim_f32(const svdb_matrix* a, uint64_t dimensions, svdb_rec_f32* out) {
+    return svdb_las2_f32(a, dimensions, 0, nullptr, 1.0e-6f, 0, nullptr, out);
+}
+int svdb_svd_dim_seed_f32(const svdb_matrix* a, uint64_t dimensions, uint32_t random_seed, svdb_rec_f32* out) {
+    return svdb_las2_f32(a, dimensions, 0, nullptr, 1.0e-6f, random_seed, nullptr, out);
+}
+int svdb_randomized_svd_f32(const svdb_matrix* a, uint64_t target_rank, uint64_t n_oversamples,
+                            uint64_t n_power_iters, int normalizer, int mean_center, int has_seed, uint64_t seed,
+                            int verbose, const svdb_options* opts, svdb_rec_f32* out) {
+    return solve_f32(a, opts, out, [&](const svdb_options& o, svdb_rec* r) {
+        if (normalizer < 0 || normalizer > 2) throw Error(SVDB_ERR_ARG, "bad normalizer");
+        randomized(a, target_rank, n_oversamples, n_power_iters, normalizer, mean_center, has_seed, seed, verbose,
+                   o, r, true);
+    });
+}
+
+void svdb_rec_f32_free(svdb_rec_f32* r) {
+    if (!r) return;
+    if (r->on_device) {
+        cudaFree(r->u);
+        cudaFree(r->s);
+        cudaFree(r->vt);
+    } else {
+        free(r->u);
+        free(r->s);
+        free(r->vt);
+    }
+    std::memset(r, 0, sizeof(*r));
 }
 
 void svdb_rec_free(svdb_rec* r) {

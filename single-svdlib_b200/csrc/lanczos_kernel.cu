@@ -17,7 +17,6 @@
 namespace svdb {
 
 constexpr double kEps = 2.220446049250313e-16;
-constexpr double kSqrtEps = 1.4901161193847656e-08;  // sqrt(f64::EPSILON)
 constexpr int kThreads = 512;
 
 __device__ __forceinline__ bool cmp_eq(double a, double b) { return fabs(b - a) < kEps; }
@@ -90,6 +89,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_lanczos_block(const __grid_cons
     bool resume = a.resume != 0;
     int64_t j = a.first;
     const double eps1 = a.eps1;
+    const double sqrt_eps = a.sqrt_eps;  // of the run's scalar T
 
 #define WV(k) (a.W[perm[k]])
 
@@ -199,7 +199,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_lanczos_block(const __grid_cons
             rnm = sqrt(s2);
         }
         if (leader) { a.alf[j] = alf_j; a.bet[j] = bet_j; }
-        tol = kSqrtEps * (bet_j + fabs(alf_j) + rnm);
+        tol = sqrt_eps * (bet_j + fabs(alf_j) + rnm);
 
         // ---- ortbnd (mod.rs:815-838) and the purge test (mod.rs:768-770) in block 0
         if (blockIdx.x == 0) {
@@ -251,7 +251,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_lanczos_block(const __grid_cons
                     int64_t i2 = shi[0];
                     for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
                         if (shb[w] > b2 || (shb[w] == b2 && shi[w] < i2)) { b2 = shb[w]; i2 = shi[w]; }
-                    a.st->purge_flag = fabs(etaC[i2 + ll]) > kSqrtEps;
+                    a.st->purge_flag = fabs(etaC[i2 + ll]) > sqrt_eps;
                 }
             } else if (threadIdx.x == 0) {
                 a.st->purge_flag = 0;
@@ -267,7 +267,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_lanczos_block(const __grid_cons
             // ---- purge (mod.rs:760-813): <= 2 sweeps of classical Gram-Schmidt
             // of q (w1, via w3) and r (w0, via w4) against q_ll .. q_{j-1}.
             ++npurge;
-            const double reps1 = eps1 / kSqrtEps;
+            const double reps1 = eps1 / sqrt_eps;
             const int64_t cnt = j - ll;
             int64_t nsplit = (n + 2047) / 2048;
             int64_t maxsplit = a.part_cap / (2 * cnt);

@@ -53,6 +53,7 @@ struct LzArgs {
     int64_t first, last;
     int32_t resume;    // 1: the host performed startv for step `first`
     double eps1;       // eps * sqrt(n), lanczos_step / purge (mod.rs:685,774)
+    double sqrt_eps;   // sqrt(eps): lanczos_step's tol and purge's reps (mod.rs:745,773)
 };
 
 void launch_lanczos_block(const LzArgs& a, int blocks, int threads, cudaStream_t s);

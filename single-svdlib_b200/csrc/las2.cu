@@ -25,7 +25,18 @@
 
 namespace svdb {
 
-static const double EPS = std::numeric_limits<double>::epsilon();
+// SvdFloat::eps of the run's scalar T (src/utils.rs:87-113): f64::EPSILON,
+// or f32::EPSILON while a T = f32 run holds a ScalarEps on this thread.  The
+// tolerances, pythag's and compare's thresholds all follow it; the arithmetic
+// stays FP64.
+static thread_local double EPS = std::numeric_limits<double>::epsilon();
+struct ScalarEps {
+    double saved;
+    explicit ScalarEps(bool f32) : saved(EPS) {
+        EPS = f32 ? (double)std::numeric_limits<float>::epsilon() : std::numeric_limits<double>::epsilon();
+    }
+    ~ScalarEps() { EPS = saved; }
+};
 static double eps34() { return std::pow(EPS, 0.75); }
 static inline bool compare(double a, double b) { return std::fabs(b - a) < EPS; }  // src/utils.rs:110-112
 
@@ -385,7 +396,10 @@ struct Las2Out {
 
 class Las2Run {
   public:
-    Las2Run(const svdb_matrix* A, bool legacy, bool fp32, cudaStream_t s) : A_(A), s_(s), fp32_(fp32) {
+    // f32: the crate's T = f32 run (f32 tolerances and start vector; FP32
+    // operands in the products).  fp32: FP32 operands only (SVDB_MIXED).
+    Las2Run(const svdb_matrix* A, bool legacy, bool fp32, bool f32, cudaStream_t s)
+        : A_(A), s_(s), fp32_(fp32 || f32), f32_(f32) {
         legacy_ = legacy;
     }
 
@@ -396,7 +410,7 @@ class Las2Run {
   private:
     const svdb_matrix* A_;
     cudaStream_t s_;
-    bool fp32_ = false, legacy_ = false, transposed_ = false;
+    bool fp32_ = false, f32_ = false, legacy_ = false, transposed_ = false;
     int64_t m_ = 0, n_ = 0;  // internal nrows / ncols
     const DevCompressed* op1_ = nullptr;
     const DevCompressed* op2_ = nullptr;
@@ -438,7 +452,7 @@ void Las2Run::ensure_q(int64_t rows) {
 double Las2Run::startv(int64_t step, uint32_t seed) {
     double rnm2 = ddot(w(0), w(0));
     for (int id = 0; id < 3; ++id) {
-        if (id > 0 || step > 0 || compare(rnm2, 0.0)) start_vector(seed, w(0), n_, s_);
+        if (id > 0 || step > 0 || compare(rnm2, 0.0)) start_vector(seed, w(0), n_, s_, f32_);
         copy(w(0), w(3), n_, s_);
         opb(w(3), w(0));
         copy(w(0), w(3), n_, s_);
@@ -517,6 +531,7 @@ int64_t Las2Run::lanczos_step(int64_t first, int64_t last, int64_t& ll, bool& en
         a.st = st_.p; a.bar = bar_.p;
         a.first = j; a.last = last; a.resume = resume ? 1 : 0;
         a.eps1 = EPS * std::sqrt((double)n_);
+        a.sqrt_eps = std::sqrt(EPS);
         launch_lanczos_block(a, lz_blocks_, 512, s_);
         GridBarrier hb;
         SVDB_CUDA(cudaMemcpyAsync(&hs, st_.p, sizeof hs, cudaMemcpyDeviceToHost, s_));
@@ -749,6 +764,7 @@ void Las2Run::run(int64_t dimensions, int64_t iterations, double endl, double en
     out.neig = neig;
     SVDB_CUDA(cudaEventRecord(t1, s_));
     double kap = std::fmax(std::fabs(kappa), eps34());
+    if (f32_) kap = (double)(float)kap;  // Float::max(|kappa|, eps34) in f32 (mod.rs:162)
     ritvec(dimensions, kap, steps, neig, out);
     SVDB_CUDA(cudaEventRecord(t2, s_));
     SVDB_CUDA(cudaStreamSynchronize(s_));
@@ -792,13 +808,16 @@ void Las2Run::fill_trace(svdb_trace* t, int64_t steps) const {
     put(t->bnd, bnd_, steps + 1);
 }
 
-// Entry used by the C ABI.
+// Entry used by the C ABI.  f32: the crate's lanczos at T = f32 (f32
+// epsilon in every tolerance, f32 start vector, FP32 operands).
 void las2(const svdb_matrix* A, uint64_t dimensions, uint64_t iterations, const double end_interval[2],
-          double kappa, uint32_t seed, bool legacy, const svdb_options& o, svdb_rec* rec) {
+          double kappa, uint32_t seed, bool legacy, const svdb_options& o, svdb_rec* rec, bool f32) {
     cudaStream_t s = o.stream ? (cudaStream_t)o.stream : A->stream;
+    if (f32 && legacy) throw Error(SVDB_ERR_UNSUPPORTED, "legacy::svdLAS2 is f64-only");
+    ScalarEps scalar_eps(f32);
     Las2Out out;
     {
-        Las2Run run(A, legacy, o.precision == SVDB_MIXED, s);
+        Las2Run run(A, legacy, o.precision == SVDB_MIXED, f32, s);
         try {
             run.run((int64_t)dimensions, (int64_t)iterations, end_interval[0], end_interval[1], kappa, seed, out);
         } catch (Error&) {

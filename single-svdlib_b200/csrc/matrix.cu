@@ -188,10 +188,11 @@ const DevCompressed& csc_of(const svdb_matrix* a) {
     return a->csc;
 }
 
-// Upload a compressed structure given with usize offsets / indices.
+// Upload a compressed structure given with usize offsets / indices and f64
+// values, or f32 values (val32, kept as the FP32 copy and widened exactly).
 static void upload_compressed(DevCompressed& c, int64_t nmajor, int64_t nminor, uint64_t nnz, const uint64_t* ptr,
-                              const uint64_t* idx, const double* val, cudaStream_t s) {
-    if (!ptr || (nnz && (!idx || !val))) throw Error(SVDB_ERR_ARG, "null array");
+                              const uint64_t* idx, const double* val, const float* val32, cudaStream_t s) {
+    if (!ptr || (nnz && (!idx || (!val && !val32)))) throw Error(SVDB_ERR_ARG, "null array");
     if (nminor > INT32_MAX) throw Error(SVDB_ERR_UNSUPPORTED, "minor dimension above 2^31-1");
     c.nmajor = nmajor;
     c.nminor = nminor;
@@ -205,7 +206,13 @@ static void upload_compressed(DevCompressed& c, int64_t nmajor, int64_t nminor, 
     SVDB_CUDA(cudaMemcpyAsync(tptr.p, ptr, (nmajor + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
     if (nnz) {
         SVDB_CUDA(cudaMemcpyAsync(tidx.p, idx, nnz * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
-        SVDB_CUDA(cudaMemcpyAsync(c.val.p, val, nnz * sizeof(double), cudaMemcpyHostToDevice, s));
+        if (val32) {
+            c.val32.alloc(nnz, s);
+            SVDB_CUDA(cudaMemcpyAsync(c.val32.p, val32, nnz * sizeof(float), cudaMemcpyHostToDevice, s));
+            widen(c.val32.p, c.val.p, (int64_t)nnz, s);
+        } else {
+            SVDB_CUDA(cudaMemcpyAsync(c.val.p, val, nnz * sizeof(double), cudaMemcpyHostToDevice, s));
+        }
     }
     k_check_convert_ptr<<<grid_for(nmajor + 1), 256, 0, s>>>(tptr.p, c.ptr.p, nmajor, nnz, bad.p);
     if (nnz) k_check_convert_idx<<<grid_for(nnz), 256, 0, s>>>(tidx.p, c.idx.p, nnz, (uint64_t)nminor, bad.p);
@@ -259,12 +266,12 @@ static svdb_matrix* new_handle() {
 }
 
 svdb_matrix* create_csr(uint64_t nrows, uint64_t ncols, uint64_t nnz, const uint64_t* indptr,
-                        const uint64_t* indices, const double* values) {
+                        const uint64_t* indices, const double* values, const float* values32) {
     svdb_matrix* a = new_handle();
     try {
         a->kind = KIND_CSR;
         a->nrows = nrows; a->ncols = ncols; a->nnz = nnz;
-        upload_compressed(a->csr, nrows, ncols, nnz, indptr, indices, values, a->stream);
+        upload_compressed(a->csr, nrows, ncols, nnz, indptr, indices, values, values32, a->stream);
         transpose(a->csr, a->csc, a->stream);
         build_plans(a, a->stream);
         SVDB_CUDA(cudaStreamSynchronize(a->stream));
@@ -277,13 +284,13 @@ svdb_matrix* create_csr(uint64_t nrows, uint64_t ncols, uint64_t nnz, const uint
 }
 
 svdb_matrix* create_csc(uint64_t nrows, uint64_t ncols, uint64_t nnz, const uint64_t* colptr,
-                        const uint64_t* rowidx, const double* values) {
+                        const uint64_t* rowidx, const double* values, const float* values32) {
     svdb_matrix* a = new_handle();
     try {
         a->kind = KIND_CSC;
         a->nrows = nrows; a->ncols = ncols; a->nnz = nnz;
         if (nrows > INT32_MAX) throw Error(SVDB_ERR_UNSUPPORTED, "nrows above 2^31-1");
-        upload_compressed(a->csc, ncols, nrows, nnz, colptr, rowidx, values, a->stream);
+        upload_compressed(a->csc, ncols, nrows, nnz, colptr, rowidx, values, values32, a->stream);
         transpose(a->csc, a->csr, a->stream);
         build_plans(a, a->stream);
         SVDB_CUDA(cudaStreamSynchronize(a->stream));
@@ -298,7 +305,7 @@ svdb_matrix* create_csc(uint64_t nrows, uint64_t ncols, uint64_t nnz, const uint
 // COO: entries stay in push order inside each row (stable sort by row), and
 // duplicates remain separate entries, as the crate's triplet loops use them.
 svdb_matrix* create_coo(uint64_t nrows, uint64_t ncols, uint64_t nnz, const uint64_t* rows, const uint64_t* cols,
-                        const double* values) {
+                        const double* values, const float* values32) {
     svdb_matrix* a = new_handle();
     try {
         a->kind = KIND_COO;
@@ -315,10 +322,16 @@ svdb_matrix* create_coo(uint64_t nrows, uint64_t ncols, uint64_t nnz, const uint
         DevBuf<int> bad(1, s);
         SVDB_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), s));
         if (nnz) {
-            if (!rows || !cols || !values) throw Error(SVDB_ERR_ARG, "null array");
+            if (!rows || !cols || (!values && !values32)) throw Error(SVDB_ERR_ARG, "null array");
             SVDB_CUDA(cudaMemcpyAsync(tr.p, rows, nnz * 8, cudaMemcpyHostToDevice, s));
             SVDB_CUDA(cudaMemcpyAsync(tc.p, cols, nnz * 8, cudaMemcpyHostToDevice, s));
-            SVDB_CUDA(cudaMemcpyAsync(v.p, values, nnz * 8, cudaMemcpyHostToDevice, s));
+            if (values32) {
+                DevBuf<float> v32(nnz, s);
+                SVDB_CUDA(cudaMemcpyAsync(v32.p, values32, nnz * 4, cudaMemcpyHostToDevice, s));
+                widen(v32.p, v.p, (int64_t)nnz, s);
+            } else {
+                SVDB_CUDA(cudaMemcpyAsync(v.p, values, nnz * 8, cudaMemcpyHostToDevice, s));
+            }
             k_check_convert_idx<<<grid_for(nnz), 256, 0, s>>>(tr.p, r32.p, nnz, nrows, bad.p);
             k_check_convert_idx<<<grid_for(nnz), 256, 0, s>>>(tc.p, c32.p, nnz, ncols, bad.p);
             SVDB_CHECK_LAUNCH_N(2);

@@ -144,6 +144,34 @@ void copy(const double* x, double* y, int64_t n, cudaStream_t s) {
     SVDB_CUDA(cudaMemcpyAsync(y, x, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
 }
 
+__global__ void k_narrow(const double* __restrict__ x, float* __restrict__ y, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        y[i] = __double2float_rn(x[i]);
+}
+__global__ void k_widen(const float* __restrict__ x, double* __restrict__ y, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        y[i] = (double)x[i];
+}
+__global__ void k_round_f32(double* __restrict__ x, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        x[i] = (double)__double2float_rn(x[i]);
+}
+void narrow(const double* x, float* y, int64_t n, cudaStream_t s) {
+    if (n <= 0) return;
+    k_narrow<<<blocks_for(n, 256), 256, 0, s>>>(x, y, n);
+    SVDB_CHECK_LAUNCH();
+}
+void widen(const float* x, double* y, int64_t n, cudaStream_t s) {
+    if (n <= 0) return;
+    k_widen<<<blocks_for(n, 256), 256, 0, s>>>(x, y, n);
+    SVDB_CHECK_LAUNCH();
+}
+void round_f32(double* x, int64_t n, cudaStream_t s) {
+    if (n <= 0) return;
+    k_round_f32<<<blocks_for(n, 256), 256, 0, s>>>(x, n);
+    SVDB_CHECK_LAUNCH();
+}
+
 // ------------------------------------------------------- CGS helpers ----
 // t[i] = Q[i0+i] . x; block (split, i) partials then an ordered reduction.
 __global__ void __launch_bounds__(256) k_gemv_t_part(const double* __restrict__ Q, int64_t n, int64_t i0,
@@ -201,8 +229,9 @@ void gemv_sub(const double* Q, int64_t n, int64_t i0, int64_t cnt, const double*
 // ------------------------------------------------------ start vector ----
 // Value v uses u64 draw v = words (2v, 2v+1) of the ChaCha12 keystream with
 // key = seed bytes (u32 little endian, rest zero), counter from 0, stream 0:
-// one thread per 64-byte block, 8 values each.
-__global__ void k_start_vector(uint32_t seed, double* __restrict__ w, int64_t n) {
+// one thread per 64-byte block, 8 values each.  round_f32: each value is
+// rounded to f32, as T::from_f64 does for T = f32 (src/lanczos/mod.rs:604-606).
+__global__ void k_start_vector(uint32_t seed, double* __restrict__ w, int64_t n, int round_f32) {
     const int64_t nblk = (n + 7) / 8;
     uint32_t key[8] = {seed, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
     for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < nblk; b += (int64_t)gridDim.x * blockDim.x) {
@@ -213,15 +242,16 @@ __global__ void k_start_vector(uint32_t seed, double* __restrict__ w, int64_t n)
             const int64_t i = b * 8 + q;
             if (i < n) {
                 const uint64_t u = (uint64_t)out[2 * q] | ((uint64_t)out[2 * q + 1] << 32);
-                w[i] = uniform_pm1_dev(u);
+                const double v = uniform_pm1_dev(u);
+                w[i] = round_f32 ? (double)__double2float_rn(v) : v;
             }
         }
     }
 }
 
-void start_vector(uint32_t seed, double* w, int64_t n, cudaStream_t s) {
+void start_vector(uint32_t seed, double* w, int64_t n, cudaStream_t s, bool round_f32) {
     if (n <= 0) return;
-    k_start_vector<<<blocks_for((n + 7) / 8, 128), 128, 0, s>>>(seed, w, n);
+    k_start_vector<<<blocks_for((n + 7) / 8, 128), 128, 0, s>>>(seed, w, n, round_f32 ? 1 : 0);
     SVDB_CHECK_LAUNCH();
 }
 

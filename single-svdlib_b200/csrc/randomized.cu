@@ -476,9 +476,11 @@ void gram_device(const double* X, int64_t rows, int c, double* G, int precision,
 
 void randomized(const svdb_matrix* A, uint64_t target_rank, uint64_t n_oversamples, uint64_t n_power_iters,
                 int normalizer, int mean_center, int has_seed, uint64_t seed, int verbose, const svdb_options& o,
-                svdb_rec* rec) {
+                svdb_rec* rec, bool f32) {
     cudaStream_t s = o.stream ? (cudaStream_t)o.stream : A->stream;
-    const bool mixed = o.precision == SVDB_MIXED;
+    // f32: the crate's T = f32 run: Omega's f64 draws rounded to f32
+    // (T::from_f64, randomized/mod.rs:299-313) and FP32 operands
+    const bool mixed = f32 || o.precision == SVDB_MIXED;
     const int64_t m = A->nrows, n = A->ncols;
     const int64_t rank = std::min<int64_t>((int64_t)target_rank, std::min(m, n));
     int l = (int)(rank + (int64_t)n_oversamples);
@@ -506,9 +508,13 @@ void randomized(const svdb_matrix* A, uint64_t target_rank, uint64_t n_oversampl
 
     // Omega (n x l)
     DevBuf<double> Om(std::max<int64_t>(n * l, 1), s);
-    if (o.omega) SVDB_CUDA(cudaMemcpyAsync(Om.p, o.omega, n * l * 8, cudaMemcpyHostToDevice, s));
-    else k_omega<double><<<nb(n * l, 256), 256, 0, s>>>(has_seed ? seed : 0, n * l, Om.p);
-    SVDB_CHECK_LAUNCH();
+    if (o.omega) {
+        SVDB_CUDA(cudaMemcpyAsync(Om.p, o.omega, n * l * 8, cudaMemcpyHostToDevice, s));
+    } else {
+        k_omega<double><<<nb(n * l, 256), 256, 0, s>>>(has_seed ? seed : 0, n * l, Om.p);
+        SVDB_CHECK_LAUNCH();
+    }
+    if (f32) round_f32(Om.p, n * l, s);
 
     // Sparse products: FP64 operands, or under SVDB_MIXED FP32 values and an
     // FP32 copy of the dense operand (half the gathered bytes), FP64 sums and output.

@@ -159,10 +159,14 @@ double dot_host(const double* x, const double* y, int64_t n, double* scratch, cu
 void axpy(double a, const double* x, double* y, int64_t n, cudaStream_t s);   // y += a*x (unfused mul then add)
 void scal(double a, double* x, int64_t n, cudaStream_t s);                    // x *= a
 void copy(const double* x, double* y, int64_t n, cudaStream_t s);
+void narrow(const double* x, float* y, int64_t n, cudaStream_t s);  // y = (float)x, round to nearest
+void widen(const float* x, double* y, int64_t n, cudaStream_t s);   // y = (double)x
+void round_f32(double* x, int64_t n, cudaStream_t s);               // x = (double)(float)x
 size_t reduce_scratch_doubles();
 
-// Start vector: rand 0.9 StdRng::from_seed(seed bytes) + random_range(-1.0..1.0).
-void start_vector(uint32_t seed, double* w, int64_t n, cudaStream_t s);
+// Start vector: rand 0.9 StdRng::from_seed(seed bytes) + random_range(-1.0..1.0),
+// rounded to f32 when round_f32 (T = f32).
+void start_vector(uint32_t seed, double* w, int64_t n, cudaStream_t s, bool round_f32 = false);
 
 // y[e] = y[e] - t[i] * Q[i0+i][e], sequentially over i (the crate's axpy order)
 void gemv_sub(const double* Q, int64_t n, int64_t i0, int64_t cnt, const double* t, double* y, cudaStream_t s);

@@ -46,6 +46,15 @@ class svdb_rec(C.Structure):
                 ("time_ms_tridiag", C.c_double), ("time_ms_ritvec", C.c_double)]
 
 
+class svdb_rec_f32(C.Structure):
+    _fields_ = [("d", C.c_uint64), ("u_rows", C.c_uint64), ("u_cols", C.c_uint64),
+                ("u", C.POINTER(C.c_float)), ("s", C.POINTER(C.c_float)),
+                ("vt_rows", C.c_uint64), ("vt_cols", C.c_uint64), ("vt", C.POINTER(C.c_float)),
+                ("diagnostics", svdb_diagnostics), ("on_device", C.c_int32), ("origin", C.c_int32),
+                ("time_ms_total", C.c_double), ("time_ms_spmv", C.c_double), ("time_ms_ortho", C.c_double),
+                ("time_ms_tridiag", C.c_double), ("time_ms_ritvec", C.c_double)]
+
+
 class svdb_trace(C.Structure):
     _fields_ = [("alf", C.POINTER(C.c_double)), ("bet", C.POINTER(C.c_double)), ("ritz", C.POINTER(C.c_double)),
                 ("bnd", C.POINTER(C.c_double)), ("cap", C.c_uint64), ("steps", C.c_uint64),
@@ -84,6 +93,9 @@ SIGNATURES = {
     "svdb_matrix_create_csc": (C.c_int, [u64, u64, u64, vp, vp, vp, P(vp)]),
     "svdb_matrix_create_coo": (C.c_int, [u64, u64, u64, vp, vp, vp, P(vp)]),
     "svdb_matrix_create_csr_device": (C.c_int, [u64, u64, u64, vp, vp, vp, P(vp)]),
+    "svdb_matrix_create_csr_f32": (C.c_int, [u64, u64, u64, vp, vp, vp, P(vp)]),
+    "svdb_matrix_create_csc_f32": (C.c_int, [u64, u64, u64, vp, vp, vp, P(vp)]),
+    "svdb_matrix_create_coo_f32": (C.c_int, [u64, u64, u64, vp, vp, vp, P(vp)]),
     "svdb_matrix_destroy": (None, [vp]),
     "svdb_matrix_nrows": (u64, [vp]),
     "svdb_matrix_ncols": (u64, [vp]),
@@ -114,6 +126,13 @@ SIGNATURES = {
     "svdb_las2_plan": (C.c_int, [u64, u64, u64, u64, u64, P(u64), P(u64), P(i32), P(i32)]),
     "svdb_randomized_svd": (C.c_int, [vp, u64, u64, u64, C.c_int, C.c_int, C.c_int, u64, C.c_int,
                                       P(svdb_options), P(svdb_rec)]),
+    "svdb_las2_f32": (C.c_int, [vp, u64, u64, P(C.c_float), C.c_float, u32, P(svdb_options), P(svdb_rec_f32)]),
+    "svdb_svd_f32": (C.c_int, [vp, P(svdb_rec_f32)]),
+    "svdb_svd_dim_f32": (C.c_int, [vp, u64, P(svdb_rec_f32)]),
+    "svdb_svd_dim_seed_f32": (C.c_int, [vp, u64, u32, P(svdb_rec_f32)]),
+    "svdb_randomized_svd_f32": (C.c_int, [vp, u64, u64, u64, C.c_int, C.c_int, C.c_int, u64, C.c_int,
+                                          P(svdb_options), P(svdb_rec_f32)]),
+    "svdb_rec_f32_free": (None, [P(svdb_rec_f32)]),
     "svdb_batch_options_default": (None, [P(svdb_batch_options)]),
     "svdb_batch_create": (C.c_int, [vp, vp, vp, u64, u64, u64, u64, C.c_int, C.c_int, u64, P(svdb_batch_options),
                                     P(vp)]),

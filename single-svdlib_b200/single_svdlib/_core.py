@@ -133,13 +133,15 @@ class SvdRec:
         return (self.u * self.s) @ self.vt
 
 
-def rec_from_c(r: _abi.svdb_rec) -> SvdRec:
+def rec_from_c(r) -> SvdRec:
+    """SvdRec from an svdb_rec (T = f64) or an svdb_rec_f32 (T = f32, float32 arrays)."""
     d = int(r.d)
     ur, uc, vr, vc = int(r.u_rows), int(r.u_cols), int(r.vt_rows), int(r.vt_cols)
+    dtype = np.float32 if isinstance(r, _abi.svdb_rec_f32) else np.float64
 
     def arr(ptr, count, shape):
         if count == 0:
-            return np.zeros(shape)
+            return np.zeros(shape, dtype=dtype)
         return np.ctypeslib.as_array(ptr, (count,)).copy().reshape(shape)
 
     u = arr(r.u, ur * uc, (ur, uc))
@@ -176,10 +178,22 @@ def _f64(a):
     return np.ascontiguousarray(a, dtype=np.float64)
 
 
+def _values(data, kind):
+    """(values, T, constructor): float32 values make a T = f32 matrix, anything
+    else is taken as f64."""
+    data = np.asarray(data)
+    if data.dtype == np.float32:
+        return np.ascontiguousarray(data), np.float32, getattr(_abi.lib(), f"svdb_matrix_create_{kind}_f32")
+    return _f64(data), np.float64, getattr(_abi.lib(), f"svdb_matrix_create_{kind}")
+
+
 class _Handle:
-    """Owns an svdb_matrix handle (the SMat trait object)."""
+    """Owns an svdb_matrix handle (the SMat trait object).  ``dtype`` is the
+    crate's scalar T of the matrix: float64, or float32 for matrices built
+    from float32 values (the solvers then run at T = f32)."""
 
     _h = None
+    dtype = np.float64
 
     def _take(self, h):
         self._h = h
@@ -280,10 +294,10 @@ class CsrMatrix(_Handle):
     """nalgebra_sparse::CsrMatrix<f64>, uploaded to the current CUDA device."""
 
     def __init__(self, nrows, ncols, indptr, indices, data):
-        indptr, indices, data = _u64(indptr), _u64(indices), _f64(data)
+        indptr, indices = _u64(indptr), _u64(indices)
+        data, self.dtype, fn = _values(data, "csr")
         h = C.c_void_p()
-        check(_abi.lib().svdb_matrix_create_csr(nrows, ncols, len(data), indptr.ctypes.data, indices.ctypes.data,
-                                                data.ctypes.data, C.byref(h)))
+        check(fn(nrows, ncols, len(data), indptr.ctypes.data, indices.ctypes.data, data.ctypes.data, C.byref(h)))
         self._take(h)
 
     @classmethod
@@ -296,10 +310,10 @@ class CscMatrix(_Handle):
     """nalgebra_sparse::CscMatrix<f64>."""
 
     def __init__(self, nrows, ncols, indptr, indices, data):
-        indptr, indices, data = _u64(indptr), _u64(indices), _f64(data)
+        indptr, indices = _u64(indptr), _u64(indices)
+        data, self.dtype, fn = _values(data, "csc")
         h = C.c_void_p()
-        check(_abi.lib().svdb_matrix_create_csc(nrows, ncols, len(data), indptr.ctypes.data, indices.ctypes.data,
-                                                data.ctypes.data, C.byref(h)))
+        check(fn(nrows, ncols, len(data), indptr.ctypes.data, indices.ctypes.data, data.ctypes.data, C.byref(h)))
         self._take(h)
 
     @classmethod
@@ -312,10 +326,10 @@ class CooMatrix(_Handle):
     """nalgebra_sparse::CooMatrix<f64>: triplets in push order, duplicates kept."""
 
     def __init__(self, nrows, ncols, rows, cols, data):
-        rows, cols, data = _u64(rows), _u64(cols), _f64(data)
+        rows, cols = _u64(rows), _u64(cols)
+        data, self.dtype, fn = _values(data, "coo")
         h = C.c_void_p()
-        check(_abi.lib().svdb_matrix_create_coo(nrows, ncols, len(data), rows.ctypes.data, cols.ctypes.data,
-                                                data.ctypes.data, C.byref(h)))
+        check(fn(nrows, ncols, len(data), rows.ctypes.data, cols.ctypes.data, data.ctypes.data, C.byref(h)))
         self._take(h)
 
 
@@ -331,6 +345,7 @@ class MaskedCSRMatrix(_Handle):
         h = C.c_void_p()
         check(_abi.lib().svdb_masked_new(matrix.handle, mask.ctypes.data, len(mask), C.byref(h)))
         self._parent = matrix
+        self.dtype = matrix.dtype
         self._take(h)
 
     @classmethod
@@ -344,6 +359,7 @@ class MaskedCSRMatrix(_Handle):
         h = C.c_void_p()
         check(_abi.lib().svdb_masked_with_columns(matrix.handle, cols.ctypes.data, len(cols), C.byref(h)))
         obj._parent = matrix
+        obj.dtype = matrix.dtype
         obj._take(h)
         return obj
 

@@ -10,22 +10,31 @@ from .._core import SvdRec, as_smat, check, options, rec_from_c
 from .masked import MaskedCSRMatrix  # noqa: F401  (lanczos::masked)
 
 
-def _run(fn, a, *args, opts=None):
-    r = _abi.svdb_rec()
+def _run(fn, a, *args, opts=None, f32=False):
+    r = _abi.svdb_rec_f32() if f32 else _abi.svdb_rec()
     try:
         check(fn(a.handle, *args, C.byref(opts) if opts is not None else None, C.byref(r)))
         return rec_from_c(r)
     finally:
-        _abi.lib().svdb_rec_free(C.byref(r))
+        (_abi.lib().svdb_rec_f32_free if f32 else _abi.lib().svdb_rec_free)(C.byref(r))
+
+
+def _las2_fn(a, algorithm):
+    """(entry point, end_interval array type, T = f32?) for the matrix's scalar T."""
+    if a.dtype == np.float32:
+        return _abi.lib().svdb_las2_f32, C.c_float * 2, True
+    fn = _abi.lib().svdb_legacy_svd_las2 if algorithm == "legacy" else _abi.lib().svdb_las2
+    return fn, C.c_double * 2, False
 
 
 def svd_las2(a, dimensions=0, iterations=0, end_interval=(-1.0e-30, 1.0e-30), kappa=1.0e-6, random_seed=0,
              precision="f64") -> SvdRec:
-    """lanczos::svd_las2 (mod.rs:104-189)."""
+    """lanczos::svd_las2 (mod.rs:104-189), at the matrix's T (f64, or f32 for
+    float32 matrices: f32 tolerances, float32 results; precision is ignored)."""
     a = as_smat(a)
-    ei = (C.c_double * 2)(*end_interval)
-    return _run(_abi.lib().svdb_las2, a, dimensions, iterations, ei, kappa, random_seed,
-                opts=options(precision=precision, algorithm="lanczos"))
+    fn, eit, f32 = _las2_fn(a, "lanczos")
+    return _run(fn, a, dimensions, iterations, eit(*end_interval), kappa, random_seed,
+                opts=options(precision=precision, algorithm="lanczos"), f32=f32)
 
 
 def svd(a) -> SvdRec:
@@ -74,11 +83,10 @@ def las2_traced(a, dimensions=0, iterations=0, end_interval=(-1.0e-30, 1.0e-30),
     tr.cap = cap
     o = options(precision=precision, algorithm=algorithm)
     o.trace = C.pointer(tr)
-    ei = (C.c_double * 2)(*end_interval)
-    fn = _abi.lib().svdb_legacy_svd_las2 if algorithm == "legacy" else _abi.lib().svdb_las2
+    fn, eit, f32 = _las2_fn(a, algorithm)
     out = {"rec": None, "error": None}
     try:
-        out["rec"] = _run(fn, a, dimensions, iterations, ei, kappa, random_seed, opts=o)
+        out["rec"] = _run(fn, a, dimensions, iterations, eit(*end_interval), kappa, random_seed, opts=o, f32=f32)
     except Exception as e:  # noqa: BLE001 - returned to the caller with the trace
         out["error"] = e
     st = int(tr.steps)

@@ -31,15 +31,15 @@ def randomized_svd(m, target_rank, n_oversamples, n_power_iters, power_iteration
         norm = norm.value
     om = None if omega is None else np.ascontiguousarray(omega, dtype=np.float64)
     o = options(precision=precision, verbose=verbose, omega=om)
-    r = _abi.svdb_rec()
+    f32 = a.dtype == np.float32  # T = f32: float32 results, precision ignored
+    r = _abi.svdb_rec_f32() if f32 else _abi.svdb_rec()
+    fn = _abi.lib().svdb_randomized_svd_f32 if f32 else _abi.lib().svdb_randomized_svd
     try:
-        check(_abi.lib().svdb_randomized_svd(a.handle, target_rank, n_oversamples, n_power_iters,
-                                             _abi.NORMALIZER[norm], int(mean_center), int(seed is not None),
-                                             0 if seed is None else int(seed), int(verbose), C.byref(o),
-                                             C.byref(r)))
+        check(fn(a.handle, target_rank, n_oversamples, n_power_iters, _abi.NORMALIZER[norm], int(mean_center),
+                 int(seed is not None), 0 if seed is None else int(seed), int(verbose), C.byref(o), C.byref(r)))
         return rec_from_c(r)
     finally:
-        _abi.lib().svdb_rec_free(C.byref(r))
+        (_abi.lib().svdb_rec_f32_free if f32 else _abi.lib().svdb_rec_free)(C.byref(r))
 
 
 def svd_flip(u=None, v=None, u_based_decision=True):

@@ -6,17 +6,19 @@ from single_svdlib import CooMatrix, CscMatrix, CsrMatrix, MaskedCSRMatrix
 import matrices as M
 
 
-def upload(kind, A, mask=None):
+def upload(kind, A, mask=None, dtype=np.float64):
+    """The matrix as a device handle; dtype=np.float32 makes a T = f32 matrix."""
+    v = lambda d: np.asarray(d, dtype=dtype)  # noqa: E731
     if kind == "csr":
-        return CsrMatrix(A["nrows"], A["ncols"], A["indptr"], A["indices"], A["data"])
+        return CsrMatrix(A["nrows"], A["ncols"], A["indptr"], A["indices"], v(A["data"]))
     if kind == "csc":
         C = M.to_csc(A)
-        return CscMatrix(C["nrows"], C["ncols"], C["indptr"], C["indices"], C["data"])
+        return CscMatrix(C["nrows"], C["ncols"], C["indptr"], C["indices"], v(C["data"]))
     if kind == "coo":
         C = M.to_coo(A)
-        return CooMatrix(C["nrows"], C["ncols"], C["row"], C["col"], C["data"])
+        return CooMatrix(C["nrows"], C["ncols"], C["row"], C["col"], v(C["data"]))
     if kind == "masked":
-        parent = CsrMatrix(A["nrows"], A["ncols"], A["indptr"], A["indices"], A["data"])
+        parent = CsrMatrix(A["nrows"], A["ncols"], A["indptr"], A["indices"], v(A["data"]))
         return MaskedCSRMatrix(parent, mask)
     raise ValueError(kind)
 

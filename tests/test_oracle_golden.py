@@ -202,6 +202,27 @@ def test_randomized_checker_mean_center_is_the_centred_svd(masked):
     assert r0["s"][0] > 2 * r["s"][0]
 
 
+def test_f32_checker_is_the_crate_at_t_f32():
+    # the same restatement built with T = f32 (impl SvdFloat for f32, src/utils.rs:87-99):
+    # start vector = the f64 draws rounded to f32 (mod.rs:604-606), kappa clamped to f32 eps34
+    sv = O.start_vector(11, 1000, scalar="f32")
+    np.testing.assert_array_equal(sv, O.start_vector(11, 1000).astype(np.float32).astype(np.float64))
+    U, _ = np.linalg.qr(np.random.default_rng(1).standard_normal((120, 6)))
+    V, _ = np.linalg.qr(np.random.default_rng(2).standard_normal((80, 6)))
+    D = ((U * np.geomspace(100, 1, 6)) @ V.T).astype(np.float32)
+    A = M.dense(D)
+    r = O.las2("csr", A, 3, 0, seed=3, scalar="f32")
+    assert r["diagnostics"]["kappa"] == float(np.float32(np.finfo(np.float32).eps) ** np.float32(0.75))
+    assert r["d"] == 3
+    # randomized at T = f32 against the dense spectrum
+    truth = np.linalg.svd(D.astype(np.float64), compute_uv=False)
+    om = M.omega(80, 12, 3)
+    rr = O.randomized(A, 6, 6, 1, "QR", omega=om, scalar="f32")
+    np.testing.assert_allclose(rr["s"], truth[:6], rtol=2e-6)
+    with pytest.raises(ValueError):
+        O.las2("csr", A, 3, 0, legacy=True, scalar="f32")
+
+
 def test_poisson_workload_fixture_shape():
     f = FIX["poisson_5000x2000_seed42_dim10"]
     A = M.poisson_rows(5000, 2000, 20, 42)
