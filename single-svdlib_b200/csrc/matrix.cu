@@ -25,6 +25,7 @@ const DeviceProps& device_props() {
         props.sms = p.multiProcessorCount;
         props.coop = p.cooperativeLaunch;
         props.l2 = p.l2CacheSize;
+        props.smem_optin = p.sharedMemPerBlockOptin > 1024 ? p.sharedMemPerBlockOptin - 1024 : 0;
         cached_dev = dev;
     }
     return props;
@@ -175,6 +176,8 @@ void ensure_fp32(const svdb_matrix* a) {
 
 // SpMM load-balancing plans for both orientations (spmm.cu)
 static void build_plans(svdb_matrix* a, cudaStream_t s) {
+    a->csr.owner_stream = a->stream;
+    a->csc.owner_stream = a->stream;
     build_seg_plan(a->csr, s);
     build_seg_plan(a->csc, s);
 }

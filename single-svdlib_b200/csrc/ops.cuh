@@ -19,6 +19,14 @@ template <typename XT, typename OT>
 void spmm_dev(const DevCompressed& m, bool fp32, const XT* X, int l, OT* Y, cudaStream_t s);
 // Raises the error a TMA gather wait of an earlier SpMM recorded (synchronises).
 void spmm_tma_check();
+// FP32 SpMM by panels of X in shared memory (spmm_panel.cu); the plan is
+// built on the first call for a structure.  spmm_panel returns false when the
+// plan does not suit the matrix; spmm_panel_check raises a recorded timeout.
+bool spmm_panel_eligible(const DevCompressed& m, int l, const void* X);
+bool spmm_panel(DevCompressed& m, const float* X, int l, double* Y, cudaStream_t s,
+                void (*heavy_segments)(const DevCompressed&, const int32_t*, const int64_t*, const int64_t*, int64_t,
+                                       const float*, int, double*, double*, cudaStream_t));
+void spmm_panel_check();
 // X^T X on the tensor cores (gram_tc.cu): part gets one c x c FP64 partial per
 // block (gram_tc_blocks(rows) of them); gram_tc_check raises a recorded timeout.
 int gram_tc_launch(const double* X, int64_t rows, int c, double* part, int64_t part_cap, const int* cond,

@@ -647,6 +647,7 @@ void randomized(const svdb_matrix* A, uint64_t target_rank, uint64_t n_oversampl
         cudaEventDestroy(ev.second);
     }
     spmm_tma_check();
+    spmm_panel_check();
     gram_tc_check();
     if (verbose) printf("SVD | Randomized | Jacobi sweeps on R: %d%s\n", hjac >> 8, (hjac & 2) ? " (limit)" : "");
     if (hflags & 2) throw Error(SVDB_ERR_LAS2, "randomized_svd: CholeskyQR broke down even with a shift");

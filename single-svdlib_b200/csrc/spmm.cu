@@ -568,9 +568,31 @@ void spmm_tma_check() {
     }
 }
 
+// The rows the panel kernel leaves to the segment kernel: an explicit list
+// of segments (row < 0: partial k of the list, at part[k * l]).
+static void heavy_segments_f32(const DevCompressed& m, const int32_t* row, const int64_t* beg, const int64_t* end,
+                               int64_t n, const float* X, int l, double* Y, double* part, cudaStream_t s) {
+    if (n <= 0) return;
+    const uintptr_t align = 16;
+    const bool vec = (l % 4 == 0) && ((reinterpret_cast<uintptr_t>(X) % align) == 0);
+    const int blocks = nblk(n * 32, 256, 16);
+    if (l <= 32)
+        k_spmm_seg<float, float, double, 2, 2, 4><<<blocks, 256, 0, s>>>(m.idx.p, m.val32.p, row, beg, end, n, X, l,
+                                                                         l, vec, Y, l, part);
+    else
+        k_spmm_seg<float, float, double, 4, 2, 4><<<blocks, 256, 0, s>>>(m.idx.p, m.val32.p, row, beg, end, n, X, l,
+                                                                         l, vec, Y, l, part);
+    SVDB_CHECK_LAUNCH();
+}
+
 template <typename XT, typename OT>
 void spmm_dev(const DevCompressed& m, bool fp32, const XT* X, int l, OT* Y, cudaStream_t s) {
     if (m.nmajor == 0 || l == 0) return;
+    if constexpr (std::is_same<XT, float>::value && std::is_same<OT, double>::value) {
+        if (fp32 && spmm_panel_eligible(m, l, X) &&
+            spmm_panel(const_cast<DevCompressed&>(m), X, l, Y, s, heavy_segments_f32))
+            return;
+    }
     if constexpr (std::is_same<XT, float>::value) {
         if (fp32 && m.val32.p && m.nnz > 0 && tma_eligible(X, l, l)) {
             DevBuf<double> part;

@@ -104,6 +104,27 @@ struct SegPlan {
     DevBuf<int32_t> multi_rows;
 };
 
+// Panel plan of the FP32 SpMM (spmm_panel.cu), built on first use.  Rows
+// up to `heavy` nonzeros are dealt to (virtual CTA, warp, slot); their entries
+// are copied grouped by (virtual CTA, panel of the dense operand) -- a "CTA
+// panel", padded to an even count -- and inside it by (warp, slot).  Longer
+// rows keep the segment kernel: their segments of `plan`, compacted into
+// hseg_*, and hmulti rows merged from partials.
+struct PanelPlan {
+    bool tried = false, usable = false;
+    int rw = 0, vctas = 0, npanels = 0, sstride = 0;
+    int64_t heavy = 0, nlight = 0, ecap = 0;
+    DevBuf<uint64_t> ent;      // row within the panel (low 32 bits) | FP32 value bits (high 32)
+    DevBuf<int64_t> cbase;     // vctas * npanels + 1: first entry of each CTA panel
+    DevBuf<int32_t> soff;      // per CTA panel, stride sstride: warps * rw + 1 slot offsets in it
+    DevBuf<int32_t> slot_row;  // vctas * warps * rw rows, -1 for an empty slot
+    int64_t nhseg = 0, nhmulti = 0;
+    DevBuf<int32_t> hseg_row;  // negative: a partial at the list position; else the row
+    DevBuf<int64_t> hseg_beg, hseg_end;
+    DevBuf<int32_t> hmulti_row;
+    DevBuf<int64_t> hmulti_first, hmulti_count;
+};
+
 struct DevCompressed {
     int64_t nmajor = 0, nminor = 0, nnz = 0;
     DevBuf<int64_t> ptr;
@@ -111,6 +132,10 @@ struct DevCompressed {
     DevBuf<double> val;
     DevBuf<float> val32;  // FP32 copy of val, made on first mixed-precision use
     SegPlan plan;         // built when the handle is created
+    PanelPlan panel;      // built on the first panel SpMM
+    // stream of the handle that owns this structure: buffers made after
+    // creation (the panel plan) are allocated, and so freed, on it
+    cudaStream_t owner_stream = nullptr;
     double avg_per_major() const { return nmajor ? double(nnz) / double(nmajor) : 0.0; }
 };
 
@@ -146,6 +171,7 @@ struct DeviceProps {
     int sms = 148;
     int coop = 1;
     size_t l2 = 0;
+    size_t smem_optin = 0;  // dynamic shared memory a block may opt into (less 1 KB for static use)
 };
 const DeviceProps& device_props();
 

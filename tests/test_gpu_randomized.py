@@ -71,6 +71,51 @@ def test_mixed_precision_error_is_stated():
     assert rel < 1e-5, rel
 
 
+@pytest.mark.parametrize("fmt", ["csr", "masked"])
+def test_mixed_panel_spmm_matches_segment_spmm(fmt, monkeypatch):
+    """The FP32 products through the panel kernel (X staged in shared memory by
+    panels of 384 rows) against the segment kernel, on a matrix with rows and
+    columns long enough to be left to the segment kernel (more than 2048
+    entries) and an empty row."""
+    rng = np.random.default_rng(77)
+    m, n = 6000, 2600
+    lens = np.minimum(n, rng.lognormal(np.log(50), 0.7, m).astype(int))
+    lens[3], lens[9], lens[10] = n, 0, 2500
+    rows = np.repeat(np.arange(m), lens)
+    cols = np.concatenate([rng.choice(n, k, replace=False) for k in lens])
+    dense_col = np.arange(0, m, 2)  # column 7: 3000 entries
+    rows = np.concatenate([rows, dense_col])
+    cols = np.concatenate([cols, np.full(len(dense_col), 7)])
+    import scipy.sparse as sp
+    S = sp.csr_matrix((rng.random(len(rows)) + 0.5, (rows, cols)), shape=(m, n))
+    S.sum_duplicates()
+    S.sort_indices()
+    A = M.from_scipy(S)
+    mask = (np.arange(n) % 5 != 2).astype(np.uint8) if fmt == "masked" else None
+    nc = int(mask.sum()) if mask is not None else n
+    om = M.omega(nc, 16, 4)
+    mat = lambda: MaskedCSRMatrix(upload("csr", A), mask) if mask is not None else upload("csr", A)  # noqa: E731
+    res = {}
+    for impl in ("seg", "panel"):
+        monkeypatch.setenv("SVDB_SPMM", impl)
+        res[impl] = randomized.randomized_svd(mat(), 10, 6, 2, PIN.QR, False, 1, False, omega=om,
+                                              precision="mixed")
+    f64 = randomized.randomized_svd(mat(), 10, 6, 2, PIN.QR, False, 1, False, omega=om)
+    assert np.max(np.abs(res["panel"].s - res["seg"].s) / res["seg"].s) < 2e-6
+    assert np.max(np.abs(res["panel"].s - f64.s) / f64.s) < 1e-5
+    assert np.all(subspace_cos(res["panel"].u[:, :5], f64.u[:, :5]) > 1 - 1e-6)
+
+    # the plan built through a view belongs to the parent: the view may go first
+    monkeypatch.setenv("SVDB_SPMM", "panel")
+    parent = upload("csr", A)
+    view = MaskedCSRMatrix(parent, np.ones(n, np.uint8))
+    r = randomized.randomized_svd(view, 10, 6, 2, PIN.QR, False, 1, False, omega=M.omega(n, 16, 4),
+                                  precision="mixed")
+    assert np.all(np.isfinite(r.s))
+    view.close()
+    parent.close()
+
+
 def test_device_omega_is_seeded():
     A = M.uniform(200, 80, 0.1, 44)
     r1 = randomized.randomized_svd(upload("csr", A), 5, 5, 1, PIN.QR, False, 9, False)
