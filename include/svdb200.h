@@ -275,8 +275,10 @@ int svdb_opa_device(const svdb_matrix* a, const double* d_x, double* d_y, int tr
 int svdb_gram_device(const double* d_x, uint64_t rows, uint64_t c, double* d_g, int precision, void* stream);
 
 /* Device buffers come from the device's stream-ordered pool, which the
- * library keeps cached between calls; this returns the cached memory of the
- * current device to the driver (after a device synchronisation). */
+ * library keeps cached between calls, and host results of 64 KB and more
+ * are page-locked buffers that svdb_rec_free keeps for reuse; this returns
+ * both caches (of the current device) to the driver, after a device
+ * synchronisation. */
 int svdb_release_cached_memory(void);
 
 /* Number of kernels this library has launched in the process so far. */
@@ -459,7 +461,9 @@ int svdb_svd_flip(double* u, uint64_t u_rows, uint64_t u_cols, double* v, uint64
 
 /* ---- results ---- */
 
-/* Frees u, s, vt (host or device) and zeroes the record. */
+/* Frees u, s, vt (host or device) and zeroes the record.  Host results are
+ * library memory (page-locked from 64 KB up): release them with this call,
+ * never with free(). */
 void svdb_rec_free(svdb_rec* rec);
 /* SvdRec::recompose: out (u_rows x vt_cols, host) = u diag(s) vt as the crate
  * writes it (src/lanczos/mod.rs:1408-1413), which needs u_cols == d

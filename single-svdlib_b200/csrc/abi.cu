@@ -493,14 +493,9 @@ static int solve_f32(const svdb_matrix* a, const svdb_options* opts, svdb_rec_f3
             out->on_device = 1;
             return;
         }
-        out->u = (float*)malloc(std::max<int64_t>(nu, 1) * sizeof(float));
-        out->s = (float*)malloc(std::max<int64_t>(ns, 1) * sizeof(float));
-        out->vt = (float*)malloc(std::max<int64_t>(nv, 1) * sizeof(float));
-        if (!out->u || !out->s || !out->vt) {
-            free(out->u); free(out->s); free(out->vt);
-            std::memset(out, 0, sizeof(*out));
-            throw std::bad_alloc();
-        }
+        out->u = (float*)host_result_alloc(std::max<int64_t>(nu, 1) * sizeof(float));
+        out->s = (float*)host_result_alloc(std::max<int64_t>(ns, 1) * sizeof(float));
+        out->vt = (float*)host_result_alloc(std::max<int64_t>(nv, 1) * sizeof(float));
         if (nu) SVDB_CUDA(cudaMemcpyAsync(out->u, u.p, nu * sizeof(float), cudaMemcpyDeviceToHost, s));
         if (ns) SVDB_CUDA(cudaMemcpyAsync(out->s, sv.p, ns * sizeof(float), cudaMemcpyDeviceToHost, s));
         if (nv) SVDB_CUDA(cudaMemcpyAsync(out->vt, vt.p, nv * sizeof(float), cudaMemcpyDeviceToHost, s));
@@ -545,9 +540,9 @@ void svdb_rec_f32_free(svdb_rec_f32* r) {
         cudaFree(r->s);
         cudaFree(r->vt);
     } else {
-        free(r->u);
-        free(r->s);
-        free(r->vt);
+        host_result_free(r->u);
+        host_result_free(r->s);
+        host_result_free(r->vt);
     }
     std::memset(r, 0, sizeof(*r));
 }
@@ -559,9 +554,9 @@ void svdb_rec_free(svdb_rec* r) {
         cudaFree(r->s);
         cudaFree(r->vt);
     } else {
-        free(r->u);
-        free(r->s);
-        free(r->vt);
+        host_result_free(r->u);
+        host_result_free(r->s);
+        host_result_free(r->vt);
     }
     std::memset(r, 0, sizeof(*r));
 }

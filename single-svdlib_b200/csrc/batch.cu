@@ -782,9 +782,9 @@ void batch_run(svdb_batch* B, svdb_rec* outs) {
             SVDB_CUDA(cudaMemcpyAsync(r->vt, dvt, d * nb * 8, cudaMemcpyDeviceToDevice, s));
             r->on_device = 1;
         } else {
-            r->u = (double*)malloc(std::max<int64_t>(m * d, 1) * 8);
-            r->s = (double*)malloc(std::max<int64_t>(d, 1) * 8);
-            r->vt = (double*)malloc(std::max<int64_t>(d * nb, 1) * 8);
+            r->u = (double*)host_result_alloc(std::max<int64_t>(m * d, 1) * 8);
+            r->s = (double*)host_result_alloc(std::max<int64_t>(d, 1) * 8);
+            r->vt = (double*)host_result_alloc(std::max<int64_t>(d * nb, 1) * 8);
             if (!r->u || !r->s || !r->vt) throw std::bad_alloc();
             SVDB_CUDA(cudaMemcpyAsync(r->u, du, m * d * 8, cudaMemcpyDeviceToHost, s));
             std::memcpy(r->s, sig.data() + b * B->l, d * 8);

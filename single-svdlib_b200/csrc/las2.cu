@@ -840,9 +840,9 @@ void las2(const svdb_matrix* A, uint64_t dimensions, uint64_t iterations, const 
         rec->on_device = 1;
         SVDB_CUDA(cudaStreamSynchronize(s));
     } else {
-        rec->u = (double*)malloc(std::max<size_t>(nu, 1) * sizeof(double));
-        rec->s = (double*)malloc(std::max<size_t>(out.d, 1) * sizeof(double));
-        rec->vt = (double*)malloc(std::max<size_t>(nv, 1) * sizeof(double));
+        rec->u = (double*)host_result_alloc(std::max<size_t>(nu, 1) * sizeof(double));
+        rec->s = (double*)host_result_alloc(std::max<size_t>(out.d, 1) * sizeof(double));
+        rec->vt = (double*)host_result_alloc(std::max<size_t>(nv, 1) * sizeof(double));
         if (nu) SVDB_CUDA(cudaMemcpyAsync(rec->u, out.Ut.p, nu * 8, cudaMemcpyDeviceToHost, s));
         if (out.d) SVDB_CUDA(cudaMemcpyAsync(rec->s, out.S.p, out.d * 8, cudaMemcpyDeviceToHost, s));
         if (nv) SVDB_CUDA(cudaMemcpyAsync(rec->vt, out.Vt.p, nv * 8, cudaMemcpyDeviceToHost, s));

@@ -258,6 +258,7 @@ void release_cached_memory() {
     SVDB_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
     SVDB_CUDA(cudaDeviceSynchronize());
     SVDB_CUDA(cudaMemPoolTrimTo(pool, 0));
+    host_result_release();
 }
 
 static svdb_matrix* new_handle() {

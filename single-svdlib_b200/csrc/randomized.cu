@@ -660,9 +660,9 @@ void randomized(const svdb_matrix* A, uint64_t target_rank, uint64_t n_oversampl
         rec->u = U.detach(); rec->s = S.detach(); rec->vt = Vt.detach();
         rec->on_device = 1;
     } else {
-        rec->u = (double*)malloc(std::max<int64_t>(m * actual, 1) * 8);
-        rec->s = (double*)malloc(std::max<int64_t>(actual, 1) * 8);
-        rec->vt = (double*)malloc(std::max<int64_t>(actual * n, 1) * 8);
+        rec->u = (double*)host_result_alloc(std::max<int64_t>(m * actual, 1) * 8);
+        rec->s = (double*)host_result_alloc(std::max<int64_t>(actual, 1) * 8);
+        rec->vt = (double*)host_result_alloc(std::max<int64_t>(actual * n, 1) * 8);
         if (actual) {
             SVDB_CUDA(cudaMemcpyAsync(rec->u, U.p, m * actual * 8, cudaMemcpyDeviceToHost, s));
             SVDB_CUDA(cudaMemcpyAsync(rec->s, S.p, actual * 8, cudaMemcpyDeviceToHost, s));

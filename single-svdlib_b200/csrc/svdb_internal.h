@@ -190,6 +190,13 @@ void widen(const float* x, double* y, int64_t n, cudaStream_t s);   // y = (doub
 void round_f32(double* x, int64_t n, cudaStream_t s);               // x = (double)(float)x
 size_t reduce_scratch_doubles();
 
+// Host result buffers (hostmem.cu): page-locked and reused from 64 KB up,
+// malloc below; host_result_free takes either kind, host_result_release
+// returns the idle page-locked buffers to the driver.
+void* host_result_alloc(size_t bytes);
+void host_result_free(void* p);
+void host_result_release();
+
 // Start vector: rand 0.9 StdRng::from_seed(seed bytes) + random_range(-1.0..1.0),
 // rounded to f32 when round_f32 (T = f32).
 void start_vector(uint32_t seed, double* w, int64_t n, cudaStream_t s, bool round_f32 = false);
