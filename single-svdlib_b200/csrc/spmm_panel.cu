@@ -7,9 +7,9 @@
 // Here each CTA streams X once through shared memory instead, in panels of
 // kPanelRows rows, and applies its rows' nonzeros to the panel there:
 //   - a warp owns up to RW rows (slots) with FP32 accumulators in registers;
-//     its two half-warps take alternate nonzeros of a slot, lane q of a half
-//     holding columns 4q .. 4q+3 (one 16-byte shared-memory read and four FMAs
-//     per nonzero), and the halves are added when a slot is written;
+//     its four quarter-warps work on four slots at once, lane ql of a
+//     quarter holding float4 columns ql and 8 + ql (two conflict-free 16-byte
+//     shared-memory reads and eight FMAs per nonzero);
 //   - the plan dealt rows to (virtual CTA, warp, slot) in snake order of
 //     their lengths, so every warp gets about the same number of nonzeros, and
 //     copied the nonzeros grouped by (virtual CTA, panel) -- a CTA panel --
@@ -37,7 +37,7 @@ namespace svdb {
 
 constexpr int kPanelRows = 256;   // rows of X per panel
 constexpr int kPanelWarps = 16;   // warps per CTA
-constexpr int kPanelMaxRw = 16;   // slots per warp (4 FP32 accumulators each, within 128 registers)
+constexpr int kPanelMaxRw = 24;   // slots per warp: 6 per quarter-warp, 8 FP32 accumulators each per lane
 constexpr int kPanelFlush = 512;  // FP32 terms of a slot before it is added into Y
 constexpr uint64_t kPanelWaitNs = 2000000000ull;
 
@@ -118,27 +118,25 @@ __device__ __forceinline__ void pn_issue(const PanelArgs& a, const PanelStage& s
     pn_bulk(st.o(b), a.soff + cp * a.sstride, ob, bar);
 }
 
-// Writes (first) or adds a slot's sums into its FP64 row of Y: lane q of the
-// first half-warp owns columns 4q .. 4q+3.
-__device__ __forceinline__ void pn_store(double* Y, int l, int row, bool first, int q, int hq, const float4& t) {
-    if (row < 0 || q >= hq) return;
-    double2* y = reinterpret_cast<double2*>(Y + (int64_t)row * l + 4 * q);
+// Writes (first) or adds a slot's columns 4 ql .. 4 ql + 3 and 32 + 4 ql ..
+// 32 + 4 ql + 3 (those below l) into its FP64 row of Y.
+__device__ __forceinline__ void pn_store4(double* Y, int l, int row, bool first, int c, const float4& v) {
+    if (c >= l) return;  // l % 4 == 0: a float4 column is wholly inside or outside
+    double2* y = reinterpret_cast<double2*>(Y + (int64_t)row * l + c);
     double2 u = first ? make_double2(0.0, 0.0) : y[0];
-    double2 v = first ? make_double2(0.0, 0.0) : y[1];
-    u.x += (double)t.x;
-    u.y += (double)t.y;
-    v.x += (double)t.z;
-    v.y += (double)t.w;
+    double2 w = first ? make_double2(0.0, 0.0) : y[1];
+    u.x += (double)v.x;
+    u.y += (double)v.y;
+    w.x += (double)v.z;
+    w.y += (double)v.w;
     y[0] = u;
-    y[1] = v;
+    y[1] = w;
 }
-
-__device__ __forceinline__ float4 pn_halves(float4 t) {
-    t.x += __shfl_xor_sync(0xffffffffu, t.x, 16);
-    t.y += __shfl_xor_sync(0xffffffffu, t.y, 16);
-    t.z += __shfl_xor_sync(0xffffffffu, t.z, 16);
-    t.w += __shfl_xor_sync(0xffffffffu, t.w, 16);
-    return t;
+__device__ __forceinline__ void pn_store8(double* Y, int l, int row, bool first, int ql, const float4& c0,
+                                          const float4& c1) {
+    if (row < 0) return;
+    pn_store4(Y, l, row, first, 4 * ql, c0);
+    pn_store4(Y, l, row, first, 32 + 4 * ql, c1);
 }
 
 __device__ __forceinline__ void pn_fma(float4& ac, float v, const float4& x) {
@@ -148,8 +146,9 @@ __device__ __forceinline__ void pn_fma(float4& ac, float v, const float4& x) {
     ac.w = fmaf(v, x.w, ac.w);
 }
 
-template <int RW>
+template <int RQ>
 __global__ void __launch_bounds__(kPanelWarps * 32, 1) k_spmm_panel(const __grid_constant__ PanelArgs a) {
+    constexpr int RW = 4 * RQ;  // slots per warp
     extern __shared__ __align__(128) unsigned char sm_raw[];
     __shared__ int s_abort;
     PanelStage st;
@@ -158,10 +157,10 @@ __global__ void __launch_bounds__(kPanelWarps * 32, 1) k_spmm_panel(const __grid
     st.esz = (uint32_t)a.ecap * 8;
     st.osz = (uint32_t)a.sstride * 4;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    const unsigned full = 0xffffffffu;
-    const int half = lane >> 4, q = lane & 15;
-    const int hq = a.l >> 2;                // float4 columns of a row of X
-    const int qc = q < hq ? q : hq - 1;     // lanes past the row read a valid column and discard it
+    const int qt = lane >> 3, ql = lane & 7;  // quarter of the warp, lane in it
+    const int hq = a.l >> 2;                  // float4 columns of a row of X
+    // float4 columns ql and 8 + ql of a row, kept inside the row (lanes past l read and discard)
+    const int cq0 = min(ql, hq - 1), cq1 = min(8 + ql, hq - 1);
     const int nmine = (a.vctas - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
     const int total = nmine * a.npanels;
     if (total <= 0) return;
@@ -189,18 +188,24 @@ __global__ void __launch_bounds__(kPanelWarps * 32, 1) k_spmm_panel(const __grid
     }
     __syncthreads();
 
-    float4 acc[RW];
-    int rowreg = -1, cntreg = 0, flreg = 0;  // lane r: row, FP32 terms and "flushed" of slot r
+    // slot s = 4 t + q belongs to quarter q (lanes 8q .. 8q+7); lane ql of a
+    // quarter holds float4 columns ql and 8 + ql of its RQ slots (each quarter
+    // reads 128 contiguous bytes of a row per instruction: no bank conflicts)
+    float4 acc[RQ][2];
+    int row[RQ], cnt[RQ];
+    unsigned flushed = 0;  // bit t: slot 4 t + q was written to Y before
     for (int it = 0; it < total; ++it) {
         if (s_abort) break;
         const int p = it % a.npanels;
         if (p == 0) {
             const int64_t vc = (int64_t)blockIdx.x + (int64_t)(it / a.npanels) * gridDim.x;
 #pragma unroll
-            for (int r = 0; r < RW; ++r) acc[r] = make_float4(0.f, 0.f, 0.f, 0.f);
-            rowreg = lane < RW ? __ldg(a.slot_row + (vc * kPanelWarps + w) * RW + lane) : -1;
-            cntreg = 0;
-            flreg = 0;
+            for (int t = 0; t < RQ; ++t) {
+                acc[t][0] = acc[t][1] = make_float4(0.f, 0.f, 0.f, 0.f);
+                row[t] = __ldg(a.slot_row + (vc * kPanelWarps + w) * RW + 4 * t + qt);
+                cnt[t] = 0;
+            }
+            flushed = 0;
         }
         const int b = it & 1;
         // every thread acquires the stage the barrier announced as complete
@@ -210,49 +215,45 @@ __global__ void __launch_bounds__(kPanelWarps * 32, 1) k_spmm_panel(const __grid
         }
         const float4* X4 = reinterpret_cast<const float4*>(st.x(b));
         const uint2* E = st.e(b);
-        const int offreg = lane <= RW ? st.o(b)[w * RW + lane] : 0;
+        const int32_t* O = st.o(b) + w * RW + qt;
 #pragma unroll
-        for (int r = 0; r < RW; ++r) {
-            const int o = __shfl_sync(full, offreg, r), o1 = __shfl_sync(full, offreg, r + 1);
-            if (o1 > o) {
-                float4 ac = acc[r];
-                int j = o + half;
-                for (; j + 2 < o1; j += 4) {
-                    const uint2 e0 = E[j], e1 = E[j + 2];
-                    const float4 x0 = X4[(int)e0.x * hq + qc];
-                    const float4 x1 = X4[(int)e1.x * hq + qc];
-                    pn_fma(ac, __uint_as_float(e0.y), x0);
-                    pn_fma(ac, __uint_as_float(e1.y), x1);
-                }
-                if (j < o1) {
-                    const uint2 e0 = E[j];
-                    pn_fma(ac, __uint_as_float(e0.y), X4[(int)e0.x * hq + qc]);
-                }
-                const int c2 = __shfl_sync(full, cntreg, r) + (o1 - o);
-                if (c2 >= kPanelFlush) {
-                    const float4 t = pn_halves(ac);
-                    const bool first = __shfl_sync(full, flreg, r) == 0;
-                    const int row = __shfl_sync(full, rowreg, r);
-                    if (half == 0) pn_store(a.Y, a.l, row, first, q, hq, t);
-                    ac = make_float4(0.f, 0.f, 0.f, 0.f);
-                    if (lane == r) {
-                        cntreg = 0;
-                        flreg = 1;
-                    }
-                } else if (lane == r) {
-                    cntreg = c2;
-                }
-                acc[r] = ac;
+        for (int t = 0; t < RQ; ++t) {
+            const int o = O[4 * t], o1 = O[4 * t + 1];
+            float4 c0 = acc[t][0], c1 = acc[t][1];
+            int j = o;
+            for (; j + 1 < o1; j += 2) {
+                const uint2 e0 = E[j], e1 = E[j + 1];
+                const float4* x0 = X4 + (int)e0.x * hq;
+                const float4* x1 = X4 + (int)e1.x * hq;
+                const float4 x00 = x0[cq0], x01 = x0[cq1], x10 = x1[cq0], x11 = x1[cq1];
+                const float v0 = __uint_as_float(e0.y), v1 = __uint_as_float(e1.y);
+                pn_fma(c0, v0, x00);
+                pn_fma(c1, v0, x01);
+                pn_fma(c0, v1, x10);
+                pn_fma(c1, v1, x11);
             }
+            if (j < o1) {
+                const uint2 e0 = E[j];
+                const float4* x0 = X4 + (int)e0.x * hq;
+                const float v0 = __uint_as_float(e0.y);
+                pn_fma(c0, v0, x0[cq0]);
+                pn_fma(c1, v0, x0[cq1]);
+            }
+            cnt[t] += o1 - o;
+            if (cnt[t] >= kPanelFlush) {  // this quarter only
+                pn_store8(a.Y, a.l, row[t], !(flushed >> t & 1u), ql, c0, c1);
+                c0 = c1 = make_float4(0.f, 0.f, 0.f, 0.f);
+                cnt[t] = 0;
+                flushed |= 1u << t;
+            }
+            acc[t][0] = c0;
+            acc[t][1] = c1;
         }
         if (p == a.npanels - 1) {  // the virtual CTA's last panel: write every slot
 #pragma unroll
-            for (int r = 0; r < RW; ++r) {
-                const bool first = __shfl_sync(full, flreg, r) == 0;
-                const int c = __shfl_sync(full, cntreg, r);
-                const int row = __shfl_sync(full, rowreg, r);
-                const float4 t = pn_halves(acc[r]);
-                if (half == 0 && (first || c > 0)) pn_store(a.Y, a.l, row, first, q, hq, t);
+            for (int t = 0; t < RQ; ++t) {
+                const bool first = !(flushed >> t & 1u);
+                if (first || cnt[t] > 0) pn_store8(a.Y, a.l, row[t], first, ql, acc[t][0], acc[t][1]);
             }
         }
         if (tid == 0 && it + 1 < total && !s_abort) {
@@ -440,7 +441,7 @@ int pn_blocks(int64_t work, int threads) {
     return (int)std::max<int64_t>(1, std::min<int64_t>(b, (int64_t)device_props().sms * 16));
 }
 
-int pn_rw_template(int64_t rw) { return rw <= 8 ? 8 : 16; }
+int pn_rw_template(int64_t rw) { return rw <= 8 ? 8 : rw <= 16 ? 16 : 24; }
 
 }  // namespace
 
@@ -585,13 +586,14 @@ void build_panel_plan(DevCompressed& m, cudaStream_t s) {
     pp.usable = true;
 }
 
-// Opt-in (SVDB_SPMM=panel, read on every call).  On B200 for the 100,000 x
-// 30,000 count-like matrix (65 M nonzeros, l = 60) the products took 17.6 ms
-// per solve against 18.0 ms for the segment kernel, and building the plan
-// took 8.3 ms per structure: a row has only 5-8 nonzeros per panel, so the
-// fixed cost of visiting a (row, panel) pair -- offsets, counts, moving the
-// accumulators -- outweighs the four instructions per nonzero (15.7 warp
-// instructions per nonzero measured, issue-bound at 16 warps per SM).
+// Opt-in (SVDB_SPMM=panel, read on every call).  On B200, for the 100,000 x
+// 30,000 count-like matrix (65 M nonzeros, l = 60), one product took 1.47 ms
+// for A Z and 2.77 ms for A^T Y, against 2.25 ms with the segment kernel.
+// The staging alone (copies and barriers, compute left out) took 0.35 and
+// 0.54 ms.  A^T Y is held by per-panel imbalance: its rows (columns of A)
+// have very skewed lengths, and a panel step waits for the warp whose long
+// row occupies one quarter.  Building the plan takes about 4 ms per
+// structure, which a call on a new handle pays.
 bool spmm_panel_eligible(const DevCompressed& m, int l, const void* X) {
     const char* e = getenv("SVDB_SPMM");
     if (!e || std::string(e) != "panel") return false;
@@ -625,13 +627,14 @@ bool spmm_panel(DevCompressed& m, const float* X, int l, double* Y, cudaStream_t
     a.Y = Y;
     const int grid = std::min(pp.vctas, device_props().sms);
     switch (pp.rw) {
-#define SVDB_PANEL_LAUNCH(RW)                                                                                   \
-    case RW:                                                                                                    \
-        SVDB_CUDA(cudaFuncSetAttribute(k_spmm_panel<RW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
-        k_spmm_panel<RW><<<grid, kPanelWarps * 32, smem, s>>>(a);                                               \
+#define SVDB_PANEL_LAUNCH(RQ)                                                                                   \
+    case 4 * RQ:                                                                                                \
+        SVDB_CUDA(cudaFuncSetAttribute(k_spmm_panel<RQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+        k_spmm_panel<RQ><<<grid, kPanelWarps * 32, smem, s>>>(a);                                               \
         break;
-        SVDB_PANEL_LAUNCH(8)
-        SVDB_PANEL_LAUNCH(16)
+        SVDB_PANEL_LAUNCH(2)
+        SVDB_PANEL_LAUNCH(4)
+        SVDB_PANEL_LAUNCH(6)
 #undef SVDB_PANEL_LAUNCH
         default:
             throw Error(SVDB_ERR_CUDA, "panel SpMM: unexpected slot count");
