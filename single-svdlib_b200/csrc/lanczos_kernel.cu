@@ -60,19 +60,61 @@ __device__ __forceinline__ double spmv_rows(const LzOperand& op, const double* x
     return dotacc;
 }
 
-// Grid-wide sum of one value per thread: block partial -> barrier -> every
-// block reduces the partials in the same order.
-__device__ __forceinline__ bool grid_sum(double v, double* part, GridBarrier* bar, double* sh, double& out) {
-    double b = block_sum(v, sh);
-    if (threadIdx.x == 0) part[blockIdx.x] = b;
-    if (!grid_sync(bar)) return false;
-    out = reduce_partials(part, gridDim.x, sh);
-    return true;
+namespace cg = cooperative_groups;
+
+// Barrier over all blocks: the bounded grid barrier of a cooperative launch,
+// or (CL) the hardware barrier of a thread-block cluster that holds the whole
+// grid.  Cluster mode needs control flow uniform over the blocks, which holds
+// here: every branch depends on values all blocks compute identically.
+template <bool CL>
+__device__ __forceinline__ bool lz_sync(GridBarrier* bar) {
+    if constexpr (CL) {
+        cg::this_cluster().sync();
+        return true;
+    } else {
+        return grid_sync(bar);
+    }
 }
 
-template <bool FP32>
+// Sum over all blocks of one value per thread: block partial -> barrier ->
+// every block adds the partials in the same order.  `par` alternates between
+// two sets of partial slots, so a block that starts the next sum never
+// overwrites a partial another block is still reading.  Cluster mode keeps
+// the partials in each block's shared memory (cl_slot) and reads them across
+// the cluster.
+template <bool CL>
+__device__ __forceinline__ bool lz_sum(double v, double* part, GridBarrier* bar, double* sh, double* cl_slot,
+                                       double* cl_out, int& par, double& out) {
+    const double b = block_sum(v, sh);
+    const int p = par;
+    par ^= 1;
+    if constexpr (CL) {
+        cg::cluster_group cl = cg::this_cluster();
+        if (threadIdx.x == 0) cl_slot[p] = b;
+        cl.sync();
+        if (threadIdx.x == 0) {
+            double acc = 0.0;
+            for (unsigned r = 0; r < cl.num_blocks(); ++r) acc += *cl.map_shared_rank(cl_slot + p, r);
+            *cl_out = acc;
+        }
+        __syncthreads();
+        out = *cl_out;
+        __syncthreads();
+        return true;
+    } else {
+        double* pp = part + (size_t)p * gridDim.x;
+        if (threadIdx.x == 0) pp[blockIdx.x] = b;
+        if (!grid_sync(bar)) return false;
+        out = reduce_partials(pp, gridDim.x, sh);
+        return true;
+    }
+}
+
+template <bool FP32, bool CL>
 __global__ void __launch_bounds__(kThreads, 2) k_lanczos_block(const __grid_constant__ LzArgs a) {
     __shared__ double sh[32];
+    __shared__ double cl_slot[2], cl_out;
+    int par = 0;
     const int64_t n = a.n;
     const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const int64_t nth = (int64_t)gridDim.x * blockDim.x;
@@ -116,6 +158,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_lanczos_block(const __grid_cons
                     a.st->rnm = rnm; a.st->tol = tol; a.st->ll = ll;
                     a.st->eta_sel = eta_sel; a.st->npurge = npurge;
                 }
+                if constexpr (CL) cg::this_cluster().sync();  // no block leaves while others may read its slots
                 return;
             }
         } else {
@@ -143,13 +186,13 @@ __global__ void __launch_bounds__(kThreads, 2) k_lanczos_block(const __grid_cons
             int t = perm[3]; perm[3] = perm[6]; perm[6] = t;
         }
         resume = false;
-        if (!grid_sync(a.bar)) return;
+        if (!lz_sync<CL>(a.bar)) return;
 
         // ---- phase 2: w0 = op2 temp - rnm w2; alf[j] = w0 . w3
         double alf_j;
         {
             double part = spmv_rows<FP32, false, true>(a.op2, a.temp, 1.0, WV(0), -rnm, WV(2), WV(3), sh);
-            if (!grid_sum(part, a.part, a.bar, sh, alf_j)) return;
+            if (!lz_sum<CL>(part, a.part, a.bar, sh, cl_slot, &cl_out, par, alf_j)) return;
         }
 
         // orthogonalise against the initial Lanczos vectors (mod.rs:722-731)
@@ -171,7 +214,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_lanczos_block(const __grid_cons
                 acc = fma(v, dv[e], acc);
             }
             double t;
-            if (!grid_sum(acc, a.part, a.bar, sh, t)) return;
+            if (!lz_sum<CL>(acc, a.part, a.bar, sh, cl_slot, &cl_out, par, t)) return;
             if (step < nloc) {
                 if (leader) { etaC[step] = eps1; etaO[step] = eps1; }
                 axv = a.Q + step * n;
@@ -195,7 +238,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_lanczos_block(const __grid_cons
                 acc = fma(v, v, acc);
             }
             double s2;
-            if (!grid_sum(acc, a.part, a.bar, sh, s2)) return;
+            if (!lz_sum<CL>(acc, a.part, a.bar, sh, cl_slot, &cl_out, par, s2)) return;
             rnm = sqrt(s2);
         }
         if (leader) { a.alf[j] = alf_j; a.bet[j] = bet_j; }
@@ -260,7 +303,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_lanczos_block(const __grid_cons
             double* t = etaC; etaC = etaO; etaO = t;
         }
         eta_sel ^= 1;
-        if (!grid_sync(a.bar)) return;
+        if (!lz_sync<CL>(a.bar)) return;
         const int do_purge = *(volatile int*)&a.st->purge_flag;
 
         if (do_purge) {
@@ -295,7 +338,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_lanczos_block(const __grid_cons
                     sr = warp_sum(sr);
                     if (lane == 0) { a.part[2 * task] = sq; a.part[2 * task + 1] = sr; }
                 }
-                if (!grid_sync(a.bar)) return;
+                if (!lz_sync<CL>(a.bar)) return;
                 for (int64_t i = gwarp; i < cnt; i += nwarps) {
                     double sq = 0.0, sr = 0.0;
                     for (int64_t c = lane; c < nsplit; c += 32) {
@@ -306,7 +349,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_lanczos_block(const __grid_cons
                     sr = warp_sum(sr);
                     if (lane == 0) { a.tq[ll + i] = sq; a.tr[ll + i] = sr; }
                 }
-                if (!grid_sync(a.bar)) return;
+                if (!lz_sync<CL>(a.bar)) return;
                 // tq = sum |t_q|, tr = sum |t_r|
                 double aq = 0.0, ar = 0.0;
                 for (int64_t i = threadIdx.x; i < cnt; i += blockDim.x) {
@@ -333,7 +376,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_lanczos_block(const __grid_cons
                     acc = fma(v0, v1, acc);
                 }
                 double t;
-                if (!grid_sum(acc, a.part, a.bar, sh, t)) return;
+                if (!lz_sum<CL>(acc, a.part, a.bar, sh, cl_slot, &cl_out, par, t)) return;
                 tr_sum += fabs(t);
                 double* w4w = WV(4);
                 double acc2 = 0.0;
@@ -344,7 +387,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_lanczos_block(const __grid_cons
                     acc2 = fma(v, v, acc2);
                 }
                 double s2;
-                if (!grid_sum(acc2, a.part, a.bar, sh, s2)) return;
+                if (!lz_sum<CL>(acc2, a.part, a.bar, sh, cl_slot, &cl_out, par, s2)) return;
                 rnm = sqrt(s2);
                 if (tq_sum <= reps1 && tr_sum <= rnm * reps1) break;
             }
@@ -362,25 +405,64 @@ __global__ void __launch_bounds__(kThreads, 2) k_lanczos_block(const __grid_cons
         a.st->rnm = rnm; a.st->tol = tol; a.st->ll = ll;
         a.st->eta_sel = eta_sel; a.st->npurge = npurge;
     }
+    if constexpr (CL) cg::this_cluster().sync();  // no block leaves while others may read its slots
 #undef WV
 }
 
 int lanczos_max_blocks(int threads) {
     int per_sm = 0;
-    SVDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lanczos_block<false>, threads, 0));
+    SVDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lanczos_block<false, false>, threads, 0));
     int per_sm32 = 0;
-    SVDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm32, k_lanczos_block<true>, threads, 0));
+    SVDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm32, k_lanczos_block<true, false>, threads, 0));
     per_sm = per_sm < per_sm32 ? per_sm : per_sm32;
     if (per_sm < 1) per_sm = 1;
     return per_sm * device_props().sms;
 }
 
-void launch_lanczos_block(const LzArgs& a, int blocks, int threads, cudaStream_t s) {
-    void* args[] = {(void*)&a};
+void launch_lanczos_block(const LzArgs& a, int blocks, int threads, int cluster, cudaStream_t s) {
     const bool fp32 = a.op1.vf != nullptr;
-    const void* fn = fp32 ? (const void*)k_lanczos_block<true> : (const void*)k_lanczos_block<false>;
-    SVDB_CUDA(cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(threads), args, 0, s));
+    if (cluster > 0) {  // the whole grid is one cluster of `cluster` blocks
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(cluster);
+        cfg.blockDim = dim3(threads);
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = cluster;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        if (fp32) SVDB_CUDA(cudaLaunchKernelEx(&cfg, k_lanczos_block<true, true>, a));
+        else SVDB_CUDA(cudaLaunchKernelEx(&cfg, k_lanczos_block<false, true>, a));
+    } else {
+        void* args[] = {(void*)&a};
+        const void* fn = fp32 ? (const void*)k_lanczos_block<true, false> : (const void*)k_lanczos_block<false, false>;
+        SVDB_CUDA(cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(threads), args, 0, s));
+    }
     count_launches(1);
+}
+
+// Whether a cluster of `cluster` blocks of `threads` threads can be resident.
+bool lanczos_cluster_ok(int cluster, int threads) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cluster);
+    cfg.blockDim = dim3(threads);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int n = 0, n32 = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, k_lanczos_block<false, true>, &cfg) != cudaSuccess ||
+        cudaOccupancyMaxActiveClusters(&n32, k_lanczos_block<true, true>, &cfg) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return n >= 1 && n32 >= 1;
 }
 
 }  // namespace svdb

@@ -56,7 +56,9 @@ struct LzArgs {
     double sqrt_eps;   // sqrt(eps): lanczos_step's tol and purge's reps (mod.rs:745,773)
 };
 
-void launch_lanczos_block(const LzArgs& a, int blocks, int threads, cudaStream_t s);
+// blocks: a cooperative grid; cluster > 0: one thread-block cluster of that many blocks instead.
+void launch_lanczos_block(const LzArgs& a, int blocks, int threads, int cluster, cudaStream_t s);
 int lanczos_max_blocks(int threads);
+bool lanczos_cluster_ok(int cluster, int threads);
 
 }  // namespace svdb

@@ -92,6 +92,11 @@ static void insert_sort(size_t n, double* a1, double* a2) {
         }
 }
 
+// Lanczos blocks on operators of at most kLzClusterNnz nonzeros run as one
+// cluster of kLzCluster blocks (portable cluster size).
+constexpr int kLzCluster = 8;
+constexpr int64_t kLzClusterNnz = 1 << 20;
+
 struct Mode {
     bool legacy = false;
     double sparsity = 0.0;
@@ -422,7 +427,7 @@ class Las2Run {
     int perm_[7] = {0, 1, 2, 3, 4, 5, 6};
     int eta_sel_ = 0;
     int64_t npurge_ = 0;
-    int lz_blocks_ = 0;
+    int lz_blocks_ = 0, lz_cluster_ = 0;
     std::vector<double> alf_h_, bet_h_, ritz_, bnd_, w5_;
 
     double* w(int k) { return W_[perm_[k]].p; }
@@ -532,7 +537,7 @@ int64_t Las2Run::lanczos_step(int64_t first, int64_t last, int64_t& ll, bool& en
         a.first = j; a.last = last; a.resume = resume ? 1 : 0;
         a.eps1 = EPS * std::sqrt((double)n_);
         a.sqrt_eps = std::sqrt(EPS);
-        launch_lanczos_block(a, lz_blocks_, 512, s_);
+        launch_lanczos_block(a, lz_blocks_, 512, lz_cluster_, s_);
         GridBarrier hb;
         SVDB_CUDA(cudaMemcpyAsync(&hs, st_.p, sizeof hs, cudaMemcpyDeviceToHost, s_));
         SVDB_CUDA(cudaMemcpyAsync(&hb, bar_.p, sizeof hb, cudaMemcpyDeviceToHost, s_));
@@ -754,8 +759,18 @@ void Las2Run::run(int64_t dimensions, int64_t iterations, double endl, double en
                                       op2_->nmajor * group_for(op2_->avg_per_major()), n_}) / 512 + 1;
     if (const char* env = getenv("SVDB_LZ_BLOCKS")) want = atoi(env);
     lz_blocks_ = (int)std::max<int64_t>(1, std::min<int64_t>(want, maxb));
+    // Small operators: one cluster of kLzCluster blocks, whose hardware barrier
+    // and shared-memory partials replace the grid barrier (SVDB_LZ_CLUSTER=0
+    // keeps the cooperative grid, =1 forces the cluster).
+    {
+        const char* env = getenv("SVDB_LZ_CLUSTER");
+        const bool small = op1_->nnz <= kLzClusterNnz && op2_->nnz <= kLzClusterNnz;
+        const bool want_cl = env ? atoi(env) != 0 : small;
+        lz_cluster_ = (want_cl && lanczos_cluster_ok(kLzCluster, 512)) ? kLzCluster : 0;
+        if (lz_cluster_) lz_blocks_ = lz_cluster_;
+    }
     const int64_t nsplit_max = (n_ + 2047) / 2048;
-    part_cap_ = std::max<int64_t>({(int64_t)lz_blocks_, 2 * cap * nsplit_max, 2 * cap});
+    part_cap_ = std::max<int64_t>({2 * (int64_t)lz_blocks_, 2 * cap * nsplit_max, 2 * cap});
     part_.alloc(part_cap_, s_);
 
     int64_t neig = 0;

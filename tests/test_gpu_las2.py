@@ -203,3 +203,25 @@ def test_poisson_5000x2000_lanczos_as_written_fails_like_the_crate():
     assert isinstance(got["error"], Imtql2Error)
     assert str(got["error"]).endswith(f["message"].split(": ", 1)[1])
     assert got["steps"] + 1 == f["lanczos_steps"]
+
+
+@pytest.mark.parametrize("algorithm", ["lanczos", "legacy"])
+def test_cluster_and_grid_lanczos_blocks_agree(algorithm, monkeypatch):
+    """Small operators run the Lanczos blocks as one thread-block cluster (hardware
+    barrier, partials in shared memory); larger ones as a cooperative grid.  Both
+    follow the same steps: decisions equal, sigma within 1e-12."""
+    A = M.poisson_rows(3000, 1200, 10, 21)
+    out = {}
+    for mode in ("0", "1"):
+        monkeypatch.setenv("SVDB_LZ_CLUSTER", mode)
+        out[mode] = lanczos.las2_traced(upload("csr", A), 8, 0, random_seed=5, algorithm=algorithm)
+    g, c = out["0"], out["1"]
+    assert c["lanczos_blocks"] == 8
+    # the as-written path may end in the crate's Imtql2Error: then both modes must
+    assert type(g["error"]) is type(c["error"]), (g["error"], c["error"])
+    assert g["steps"] == c["steps"] and g["purges"] == c["purges"]
+    np.testing.assert_allclose(c["alf"], g["alf"], rtol=0, atol=1e-12 * np.abs(g["alf"]).max())
+    np.testing.assert_allclose(c["bet"], g["bet"], rtol=0, atol=1e-12 * np.abs(g["bet"]).max())
+    if g["error"] is None:
+        assert g["rec"].d == c["rec"].d
+        np.testing.assert_allclose(c["rec"].s, g["rec"].s, rtol=0, atol=1e-12 * g["rec"].s.max())
