@@ -92,10 +92,11 @@ __device__ __forceinline__ bool lz_sum(double v, double* part, GridBarrier* bar,
         cg::cluster_group cl = cg::this_cluster();
         if (threadIdx.x == 0) cl_slot[p] = b;
         cl.sync();
-        if (threadIdx.x == 0) {
-            double acc = 0.0;
-            for (unsigned r = 0; r < cl.num_blocks(); ++r) acc += *cl.map_shared_rank(cl_slot + p, r);
-            *cl_out = acc;
+        if (threadIdx.x < 32) {  // lane r reads rank r's partial; a fixed shuffle tree adds them
+            const unsigned nb = cl.num_blocks();
+            double acc = threadIdx.x < nb ? *cl.map_shared_rank(cl_slot + p, threadIdx.x) : 0.0;
+            acc = warp_sum(acc);
+            if (threadIdx.x == 0) *cl_out = acc;
         }
         __syncthreads();
         out = *cl_out;
@@ -329,6 +330,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_lanczos_block(const __grid_cons
                     const int64_t e0 = c * chunk, e1 = (e0 + chunk < n) ? e0 + chunk : n;
                     const double* q = a.Q + i * n;
                     double sq = 0.0, sr = 0.0;
+#pragma unroll 4
                     for (int64_t e = e0 + lane; e < e1; e += 32) {
                         const double qv = q[e];
                         sq = fma(qv, w3[e], sq);
@@ -365,7 +367,24 @@ __global__ void __launch_bounds__(kThreads, 2) k_lanczos_block(const __grid_cons
                 double acc = 0.0;
                 for (int64_t e = tid; e < n; e += nth) {
                     double v1 = w1[e], v0 = w0[e];
-                    for (int64_t i = ll; i < j; ++i) {
+                    // the crate's order over i (unfused multiply, then add); the
+                    // loads of eight vectors are issued before their updates
+                    int64_t i = ll;
+                    for (; i + 8 <= j; i += 8) {
+                        double qv[8], t1[8], t0[8];
+#pragma unroll
+                        for (int u = 0; u < 8; ++u) {
+                            qv[u] = a.Q[(i + u) * n + e];
+                            t1[u] = a.tq[i + u];
+                            t0[u] = a.tr[i + u];
+                        }
+#pragma unroll
+                        for (int u = 0; u < 8; ++u) {
+                            v1 = add_rn(v1, mul_rn(-t1[u], qv[u]));
+                            v0 = add_rn(v0, mul_rn(-t0[u], qv[u]));
+                        }
+                    }
+                    for (; i < j; ++i) {
                         const double qv = a.Q[i * n + e];
                         v1 = add_rn(v1, mul_rn(-a.tq[i], qv));
                         v0 = add_rn(v0, mul_rn(-a.tr[i], qv));
@@ -444,8 +463,18 @@ void launch_lanczos_block(const LzArgs& a, int blocks, int threads, int cluster,
     count_launches(1);
 }
 
-// Whether a cluster of `cluster` blocks of `threads` threads can be resident.
+// Whether a cluster of `cluster` blocks of `threads` threads can be resident
+// (sizes above 8 are opted into per kernel).
 bool lanczos_cluster_ok(int cluster, int threads) {
+    if (cluster > 8) {
+        if (cudaFuncSetAttribute(k_lanczos_block<false, true>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+                cudaSuccess ||
+            cudaFuncSetAttribute(k_lanczos_block<true, true>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+                cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+    }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(cluster);
     cfg.blockDim = dim3(threads);

@@ -93,7 +93,8 @@ static void insert_sort(size_t n, double* a1, double* a2) {
 }
 
 // Lanczos blocks on operators of at most kLzClusterNnz nonzeros run as one
-// cluster of kLzCluster blocks (portable cluster size).
+// cluster of 2 * kLzCluster blocks where the device allows it, else of
+// kLzCluster (the portable size).
 constexpr int kLzCluster = 8;
 constexpr int64_t kLzClusterNnz = 1 << 20;
 
@@ -766,7 +767,11 @@ void Las2Run::run(int64_t dimensions, int64_t iterations, double endl, double en
         const char* env = getenv("SVDB_LZ_CLUSTER");
         const bool small = op1_->nnz <= kLzClusterNnz && op2_->nnz <= kLzClusterNnz;
         const bool want_cl = env ? atoi(env) != 0 : small;
-        lz_cluster_ = (want_cl && lanczos_cluster_ok(kLzCluster, 512)) ? kLzCluster : 0;
+        lz_cluster_ = 0;
+        if (want_cl) {  // the widest cluster that fits: 16 blocks (non-portable), else 8
+            for (int c : {2 * kLzCluster, kLzCluster})
+                if (lanczos_cluster_ok(c, 512)) { lz_cluster_ = c; break; }
+        }
         if (lz_cluster_) lz_blocks_ = lz_cluster_;
     }
     const int64_t nsplit_max = (n_ + 2047) / 2048;

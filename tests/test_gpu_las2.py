@@ -208,7 +208,8 @@ def test_poisson_5000x2000_lanczos_as_written_fails_like_the_crate():
 @pytest.mark.parametrize("algorithm", ["lanczos", "legacy"])
 def test_cluster_and_grid_lanczos_blocks_agree(algorithm, monkeypatch):
     """Small operators run the Lanczos blocks as one thread-block cluster (hardware
-    barrier, partials in shared memory); larger ones as a cooperative grid.  Both
+    barrier, partials in shared memory) of 16 or 8 blocks; larger ones as a
+    cooperative grid.  Both
     follow the same steps: decisions equal, sigma within 1e-12."""
     A = M.poisson_rows(3000, 1200, 10, 21)
     out = {}
@@ -216,7 +217,7 @@ def test_cluster_and_grid_lanczos_blocks_agree(algorithm, monkeypatch):
         monkeypatch.setenv("SVDB_LZ_CLUSTER", mode)
         out[mode] = lanczos.las2_traced(upload("csr", A), 8, 0, random_seed=5, algorithm=algorithm)
     g, c = out["0"], out["1"]
-    assert c["lanczos_blocks"] == 8
+    assert c["lanczos_blocks"] in (8, 16)  # 16 where the device allows the non-portable cluster size
     # the as-written path may end in the crate's Imtql2Error: then both modes must
     assert type(g["error"]) is type(c["error"]), (g["error"], c["error"])
     assert g["steps"] == c["steps"] and g["purges"] == c["purges"]
