@@ -65,11 +65,13 @@ __device__ __forceinline__ void chol_inv_body(const double* __restrict__ G, int 
                     if (threadIdx.x == 0) s_fail = 1;
                     break;
                 }
-                const int rem = c - k - 1;
                 const double inv = 1.0 / d;
-                for (int t = threadIdx.x; t < rem * rem; t += 128) {
-                    const int i = k + 1 + t / rem, j = k + 1 + t % rem;
-                    if (i <= j) sm[i * c + j] -= sm[k * c + i] * sm[k * c + j] * inv;
+                // upper triangle i <= j of the trailing block: 8 rows x 16 columns of
+                // threads, no index division
+                const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
+                for (int i = k + 1 + ty; i < c; i += 8) {
+                    const double aki = sm[k * c + i];
+                    for (int j = i + tx; j < c; j += 16) sm[i * c + j] -= aki * sm[k * c + j] * inv;
                 }
                 asm volatile("bar.sync 1, 128;" ::: "memory");
             }
@@ -177,10 +179,16 @@ __device__ __forceinline__ void jacobi_svd_body(const double* __restrict__ R, in
                 al = warp_sum(al);
                 be = warp_sum(be);
                 ga = warp_sum(ga);
-                if (ga != 0.0 && fabs(ga) > tol * sqrt(al * be)) {
-                    const double zeta = (be - al) / (2.0 * ga);
-                    const double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-                    const double cs = 1.0 / sqrt(1.0 + t * t), sn = cs * t;
+                // |ga| > tol sqrt(al be), compared in squares.  The rotation of the
+                // usual zeta = (be - al) / (2 ga), t = sign(zeta) / (|zeta| +
+                // sqrt(1 + zeta^2)), cs = 1 / sqrt(1 + t^2), with numerator and
+                // denominator of t scaled by |2 ga|: one sqrt, one division, one
+                // reciprocal square root on the dependent path.
+                if (ga != 0.0 && ga * ga > (tol * tol) * (al * be)) {
+                    const double d = be - al, g2 = 2.0 * ga;
+                    const bool pos = (d >= 0.0) == (ga > 0.0) || d == 0.0;  // sign(zeta) >= 0
+                    const double t = (pos ? fabs(g2) : -fabs(g2)) / (fabs(d) + sqrt(fma(d, d, g2 * g2)));
+                    const double cs = rsqrt(fma(t, t, 1.0)), sn = cs * t;
                     for (int i = lane; i < c; i += 32) {
                         const double x = W[p * c + i], y = W[q * c + i];
                         W[p * c + i] = cs * x - sn * y;
