@@ -114,17 +114,37 @@ __device__ __forceinline__ void chol_inv_body(const double* __restrict__ G, int 
         ri[t] = 0.0;
     }
     __syncthreads();
-    // R^-1 column j by back substitution, one warp per column: the inner sums
-    // run across the lanes (a fixed tree), the rows in turn
+    // R^-1 row i, one warp per row: x^T R = e_i^T by forward substitution in
+    // axpy form.  Lane l holds x_l, x_{l+32}, x_{l+64}, x_{l+96}; step k scales
+    // x_k by 1 / R_kk and subtracts x_k R[k, k+1..] from the later entries,
+    // reading row k of R (contiguous, no bank conflicts).  No reductions: the
+    // dependent path of a step is one shuffle, one multiply and one FMA.
+    for (int k = threadIdx.x; k < c; k += blockDim.x) s_rd[k] = 1.0 / sm[k * c + k];
+    __syncthreads();
     {
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-        for (int j = warp; j < c; j += nwarps) {
-            for (int i = j; i >= 0; --i) {
-                double s = 0.0;
-                for (int k = i + 1 + lane; k <= j; k += 32) s = fma(sm[i * c + k], ri[k * c + j], s);
-                s = warp_sum(s);
-                if (lane == 0) ri[i * c + j] = ((i == j ? 1.0 : 0.0) - s) / sm[i * c + i];
-                __syncwarp();
+        for (int i = warp; i < c; i += nwarps) {
+            double x[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) x[q] = (lane + 32 * q == i) ? 1.0 : 0.0;
+            for (int k = i; k < c; ++k) {
+                const int ks = k >> 5, kl = k & 31;
+                double own = x[0];
+#pragma unroll
+                for (int q = 1; q < 4; ++q)
+                    if (ks == q) own = x[q];
+                const double xk = __shfl_sync(0xffffffffu, own, kl) * s_rd[k];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int e = lane + 32 * q;
+                    if (e == k) x[q] = xk;
+                    else if (e > k && e < c) x[q] = fma(-xk, sm[k * c + e], x[q]);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int e = lane + 32 * q;
+                if (e < c) ri[i * c + e] = e >= i ? x[q] : 0.0;
             }
         }
     }
