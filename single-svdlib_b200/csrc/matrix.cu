@@ -54,20 +54,6 @@ __global__ void k_check_convert_idx(const uint64_t* in, int32_t* out, uint64_t n
     }
 }
 
-// row id of every entry: binary search of the offsets
-__global__ void k_expand_major(const int64_t* ptr, int64_t nmajor, int64_t nnz, int32_t* major_of) {
-    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (; k < nnz; k += stride) {
-        int64_t lo = 0, hi = nmajor;  // find last r with ptr[r] <= k
-        while (hi - lo > 1) {
-            int64_t mid = (lo + hi) >> 1;
-            if (ptr[mid] <= k) lo = mid; else hi = mid;
-        }
-        major_of[k] = (int32_t)lo;
-    }
-}
-
 template <typename IT>
 __global__ void k_iota(IT* v, int64_t n) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -75,16 +61,29 @@ __global__ void k_iota(IT* v, int64_t n) {
     for (; k < n; k += stride) v[k] = (IT)k;
 }
 
+// row id of every entry, one warp per row (writes stay inside [0, nnz) for any offsets)
+__global__ void k_fill_major(const int64_t* __restrict__ ptr, int64_t nmajor, int64_t nnz,
+                             int32_t* __restrict__ major_of) {
+    const int lane = threadIdx.x & 31;
+    const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t r = gwarp; r < nmajor; r += nwarps) {
+        const int64_t b = ptr[r] < 0 ? 0 : ptr[r], e = ptr[r + 1] > nnz ? nnz : ptr[r + 1];
+        for (int64_t k = b + lane; k < e; k += 32) major_of[k] = (int32_t)r;
+    }
+}
+
 template <typename IT>
-__global__ void k_gather_transpose(const IT* perm, const int32_t* major_of, const double* val, int32_t* out_idx,
-                                   double* out_val, int64_t nnz) {
+__global__ void k_gather_idx(const IT* perm, const int32_t* major_of, int32_t* out_idx, int64_t nnz) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (; k < nnz; k += stride) {
-        IT p = perm[k];
-        out_idx[k] = major_of[p];
-        out_val[k] = val[p];
-    }
+    for (; k < nnz; k += stride) out_idx[k] = major_of[perm[k]];
+}
+template <typename IT>
+__global__ void k_gather_val(const IT* perm, const double* val, double* out_val, int64_t nnz) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (; k < nnz; k += stride) out_val[k] = val[perm[k]];
 }
 
 // out_ptr[c] = first position with key >= c (keys sorted ascending), c in [0, nminor]
@@ -121,8 +120,11 @@ static int bits_for(int64_t n) {
 
 // Stable sort of entry positions by minor index: the transpose keeps majors
 // ascending inside every minor slice (CSR rows ascending inside each column).
+// The structure (offsets, indices) needs only in.ptr and in.idx; the values
+// follow through the returned permutation, so an upload can still be copying
+// in.val while the structure is built.
 template <typename IT>
-static void transpose_impl(const DevCompressed& in, DevCompressed& out, cudaStream_t s) {
+static DevBuf<IT> transpose_structure(const DevCompressed& in, DevCompressed& out, cudaStream_t s) {
     const int64_t nnz = in.nnz;
     out.nmajor = in.nminor;
     out.nminor = in.nmajor;
@@ -130,31 +132,43 @@ static void transpose_impl(const DevCompressed& in, DevCompressed& out, cudaStre
     out.ptr.alloc(out.nmajor + 1, s);
     out.idx.alloc(std::max<int64_t>(nnz, 1), s);
     out.val.alloc(std::max<int64_t>(nnz, 1), s);
+    DevBuf<IT> perm(std::max<int64_t>(nnz, 1), s);
     if (nnz == 0) {
         SVDB_CUDA(cudaMemsetAsync(out.ptr.p, 0, (out.nmajor + 1) * sizeof(int64_t), s));
-        return;
+        return perm;
     }
     DevBuf<int32_t> major_of(nnz, s), keys_out(nnz, s);
-    DevBuf<IT> vals_in(nnz, s), vals_out(nnz, s);
-    k_expand_major<<<grid_for(nnz), 256, 0, s>>>(in.ptr.p, in.nmajor, nnz, major_of.p);
+    DevBuf<IT> vals_in(nnz, s);
+    k_fill_major<<<grid_for(in.nmajor * 32), 256, 0, s>>>(in.ptr.p, in.nmajor, nnz, major_of.p);
     k_iota<IT><<<grid_for(nnz), 256, 0, s>>>(vals_in.p, nnz);
     SVDB_CHECK_LAUNCH_N(2);
     size_t tmp_bytes = 0;
     int end_bit = bits_for(std::max<int64_t>(in.nminor, 2));
-    SVDB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, in.idx.p, keys_out.p, vals_in.p, vals_out.p,
+    SVDB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, in.idx.p, keys_out.p, vals_in.p, perm.p,
                                               nnz, 0, end_bit, s));
     DevBuf<uint8_t> tmp(std::max<size_t>(tmp_bytes, 1), s);
-    SVDB_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tmp_bytes, in.idx.p, keys_out.p, vals_in.p, vals_out.p, nnz,
+    SVDB_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tmp_bytes, in.idx.p, keys_out.p, vals_in.p, perm.p, nnz,
                                               0, end_bit, s));
-    k_gather_transpose<IT><<<grid_for(nnz), 256, 0, s>>>(vals_out.p, major_of.p, in.val.p, out.idx.p, out.val.p,
-                                                         nnz);
+    k_gather_idx<IT><<<grid_for(nnz), 256, 0, s>>>(perm.p, major_of.p, out.idx.p, nnz);
     k_offsets_from_sorted<<<grid_for(out.nmajor + 1), 256, 0, s>>>(keys_out.p, nnz, out.nmajor, out.ptr.p);
     SVDB_CHECK_LAUNCH_N(2);
+    return perm;
+}
+template <typename IT>
+static void transpose_values(const DevCompressed& in, DevCompressed& out, const DevBuf<IT>& perm, cudaStream_t s) {
+    if (in.nnz == 0) return;
+    k_gather_val<IT><<<grid_for(in.nnz), 256, 0, s>>>(perm.p, in.val.p, out.val.p, in.nnz);
+    SVDB_CHECK_LAUNCH();
 }
 
 void transpose(const DevCompressed& in, DevCompressed& out, cudaStream_t s) {
-    if (in.nnz <= INT32_MAX) transpose_impl<int32_t>(in, out, s);
-    else transpose_impl<int64_t>(in, out, s);
+    if (in.nnz <= INT32_MAX) {
+        DevBuf<int32_t> perm = transpose_structure<int32_t>(in, out, s);
+        transpose_values(in, out, perm, s);
+    } else {
+        DevBuf<int64_t> perm = transpose_structure<int64_t>(in, out, s);
+        transpose_values(in, out, perm, s);
+    }
 }
 
 // The FP32 copies belong to the handle that owns the arrays (the parent of an
@@ -191,10 +205,39 @@ const DevCompressed& csc_of(const svdb_matrix* a) {
     return a->csc;
 }
 
-// Upload a compressed structure given with usize offsets / indices and f64
-// values, or f32 values (val32, kept as the FP32 copy and widened exactly).
-static void upload_compressed(DevCompressed& c, int64_t nmajor, int64_t nminor, uint64_t nnz, const uint64_t* ptr,
-                              const uint64_t* idx, const double* val, const float* val32, cudaStream_t s) {
+// A second stream for the value upload of a new handle, synchronised and
+// destroyed on every exit (so no buffer it writes is freed under it).
+struct SideStream {
+    cudaStream_t s = nullptr;
+    cudaEvent_t e = nullptr;
+    SideStream() {
+        SVDB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        SVDB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    ~SideStream() {
+        if (s) {
+            cudaStreamSynchronize(s);
+            cudaStreamDestroy(s);
+        }
+        if (e) cudaEventDestroy(e);
+    }
+};
+
+static void build_plans(svdb_matrix* a, cudaStream_t s);
+
+// Uploads a compressed structure `c` given with usize offsets / indices and f64
+// values, or f32 values (val32, kept as the FP32 copy and widened exactly),
+// builds its transpose `t` and both segment plans.  The offsets are checked
+// first (the plans size their buffers from them).  The values then travel on a
+// second stream after the indices, while this stream converts the indices,
+// sorts the transpose's structure and builds the plans: only the last step,
+// placing the values in the transpose, waits for them.  Out-of-range indices
+// are read as 0 on the device (every step stays in bounds) and reported at
+// the end.
+static void upload_and_transpose(svdb_matrix* a, DevCompressed& c, DevCompressed& t, int64_t nmajor, int64_t nminor,
+                                 uint64_t nnz, const uint64_t* ptr, const uint64_t* idx, const double* val,
+                                 const float* val32) {
+    cudaStream_t s = a->stream;
     if (!ptr || (nnz && (!idx || (!val && !val32)))) throw Error(SVDB_ERR_ARG, "null array");
     if (nminor > INT32_MAX) throw Error(SVDB_ERR_UNSUPPORTED, "minor dimension above 2^31-1");
     c.nmajor = nmajor;
@@ -205,32 +248,49 @@ static void upload_compressed(DevCompressed& c, int64_t nmajor, int64_t nminor, 
     c.ptr.alloc(nmajor + 1, s);
     c.idx.alloc(std::max<uint64_t>(nnz, 1), s);
     c.val.alloc(std::max<uint64_t>(nnz, 1), s);
+    if (val32 && nnz) c.val32.alloc(nnz, s);
     SVDB_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), s));
     SVDB_CUDA(cudaMemcpyAsync(tptr.p, ptr, (nmajor + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
-    if (nnz) {
-        SVDB_CUDA(cudaMemcpyAsync(tidx.p, idx, nnz * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
-        if (val32) {
-            c.val32.alloc(nnz, s);
-            SVDB_CUDA(cudaMemcpyAsync(c.val32.p, val32, nnz * sizeof(float), cudaMemcpyHostToDevice, s));
-            widen(c.val32.p, c.val.p, (int64_t)nnz, s);
-        } else {
-            SVDB_CUDA(cudaMemcpyAsync(c.val.p, val, nnz * sizeof(double), cudaMemcpyHostToDevice, s));
-        }
-    }
     k_check_convert_ptr<<<grid_for(nmajor + 1), 256, 0, s>>>(tptr.p, c.ptr.p, nmajor, nnz, bad.p);
-    if (nnz) k_check_convert_idx<<<grid_for(nnz), 256, 0, s>>>(tidx.p, c.idx.p, nnz, (uint64_t)nminor, bad.p);
-    SVDB_CHECK_LAUNCH_N(nnz ? 2 : 1);
+    SVDB_CHECK_LAUNCH();
     int hbad = 0;
     SVDB_CUDA(cudaMemcpyAsync(&hbad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     SVDB_CUDA(cudaStreamSynchronize(s));
-    if (hbad) {
+    auto report = [&](int b) {
         std::string m = "invalid compressed sparse input:";
-        if (hbad & 1) m += " offsets[0] != 0;";
-        if (hbad & 2) m += " offsets[last] != nnz;";
-        if (hbad & 4) m += " offsets not monotone;";
-        if (hbad & 8) m += " index out of bounds;";
+        if (b & 1) m += " offsets[0] != 0;";
+        if (b & 2) m += " offsets[last] != nnz;";
+        if (b & 4) m += " offsets not monotone;";
+        if (b & 8) m += " index out of bounds;";
         throw Error(SVDB_ERR_SHAPE, m);
+    };
+    if (hbad) report(hbad);
+    SideStream side;
+    if (nnz) {
+        SVDB_CUDA(cudaMemcpyAsync(tidx.p, idx, nnz * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+        // the values follow the indices on the link, on the side stream
+        SVDB_CUDA(cudaEventRecord(side.e, s));
+        SVDB_CUDA(cudaStreamWaitEvent(side.s, side.e, 0));
+        if (val32) {
+            SVDB_CUDA(cudaMemcpyAsync(c.val32.p, val32, nnz * sizeof(float), cudaMemcpyHostToDevice, side.s));
+            widen(c.val32.p, c.val.p, (int64_t)nnz, side.s);
+        } else {
+            SVDB_CUDA(cudaMemcpyAsync(c.val.p, val, nnz * sizeof(double), cudaMemcpyHostToDevice, side.s));
+        }
+        SVDB_CUDA(cudaEventRecord(side.e, side.s));
+        k_check_convert_idx<<<grid_for(nnz), 256, 0, s>>>(tidx.p, c.idx.p, nnz, (uint64_t)nminor, bad.p);
+        SVDB_CHECK_LAUNCH();
     }
+    auto finish = [&](auto perm) {
+        build_plans(a, s);
+        if (nnz) SVDB_CUDA(cudaStreamWaitEvent(s, side.e, 0));
+        transpose_values(c, t, perm, s);
+    };
+    if (c.nnz <= INT32_MAX) finish(transpose_structure<int32_t>(c, t, s));
+    else finish(transpose_structure<int64_t>(c, t, s));
+    SVDB_CUDA(cudaMemcpyAsync(&hbad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    SVDB_CUDA(cudaStreamSynchronize(s));
+    if (hbad) report(hbad);
 }
 
 // Device buffers come from the device's default stream-ordered pool.  With
@@ -275,10 +335,7 @@ svdb_matrix* create_csr(uint64_t nrows, uint64_t ncols, uint64_t nnz, const uint
     try {
         a->kind = KIND_CSR;
         a->nrows = nrows; a->ncols = ncols; a->nnz = nnz;
-        upload_compressed(a->csr, nrows, ncols, nnz, indptr, indices, values, values32, a->stream);
-        transpose(a->csr, a->csc, a->stream);
-        build_plans(a, a->stream);
-        SVDB_CUDA(cudaStreamSynchronize(a->stream));
+        upload_and_transpose(a, a->csr, a->csc, nrows, ncols, nnz, indptr, indices, values, values32);
     } catch (...) {
         cudaStreamSynchronize(a->stream);
         delete a;
@@ -294,10 +351,7 @@ svdb_matrix* create_csc(uint64_t nrows, uint64_t ncols, uint64_t nnz, const uint
         a->kind = KIND_CSC;
         a->nrows = nrows; a->ncols = ncols; a->nnz = nnz;
         if (nrows > INT32_MAX) throw Error(SVDB_ERR_UNSUPPORTED, "nrows above 2^31-1");
-        upload_compressed(a->csc, ncols, nrows, nnz, colptr, rowidx, values, values32, a->stream);
-        transpose(a->csc, a->csr, a->stream);
-        build_plans(a, a->stream);
-        SVDB_CUDA(cudaStreamSynchronize(a->stream));
+        upload_and_transpose(a, a->csc, a->csr, ncols, nrows, nnz, colptr, rowidx, values, values32);
     } catch (...) {
         cudaStreamSynchronize(a->stream);
         delete a;
@@ -359,10 +413,10 @@ svdb_matrix* create_coo(uint64_t nrows, uint64_t ncols, uint64_t nnz, const uint
             SVDB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, r32.p, keys_out.p, pin.p, pout.p, nnz, 0, eb, s));
             DevBuf<uint8_t> t(std::max<size_t>(tb, 1), s);
             SVDB_CUDA(cub::DeviceRadixSort::SortPairs(t.p, tb, r32.p, keys_out.p, pin.p, pout.p, nnz, 0, eb, s));
-            k_gather_transpose<int64_t><<<grid_for(nnz), 256, 0, s>>>(pout.p, c32.p, v.p, a->csr.idx.p,
-                                                                      a->csr.val.p, nnz);
+            k_gather_idx<int64_t><<<grid_for(nnz), 256, 0, s>>>(pout.p, c32.p, a->csr.idx.p, nnz);
+            k_gather_val<int64_t><<<grid_for(nnz), 256, 0, s>>>(pout.p, v.p, a->csr.val.p, nnz);
             k_offsets_from_sorted<<<grid_for(nrows + 1), 256, 0, s>>>(keys_out.p, nnz, nrows, a->csr.ptr.p);
-            SVDB_CHECK_LAUNCH_N(3);
+            SVDB_CHECK_LAUNCH_N(4);
         }
         transpose(a->csr, a->csc, s);
         build_plans(a, s);
