@@ -144,25 +144,44 @@ __global__ void k_small_gemm(const double* __restrict__ A, const double* __restr
     }
 }
 
-// Out (rows x cout) = X (rows x c) S (c x lds, first cout columns).  S and a
-// 64-row tile of X are staged in shared memory; a 16 x 16 thread grid gives
+// Out (rows x cout) = X (rows x c) S (c x lds, first cout columns).  S and
+// 64-row tiles of X are staged in shared memory; a 16 x 16 thread grid gives
 // every thread a 4 x NJ register tile (rows ty + 16 i, columns tx + 16 j).
+// With nbuf = 2 the next tile of X is copied (cp.async) while the current one
+// is multiplied; nbuf = 1 when two tiles do not fit.
 constexpr int kRmRows = 64;
+__device__ __forceinline__ void rm_cp_async(void* dst, const void* src, int bytes) {
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+    if (bytes == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+    else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+}
 template <typename TI, typename TO, int NJ>
 __global__ void __launch_bounds__(256) k_right_mul(const TI* __restrict__ X, int64_t rows, int c,
                                                    const double* __restrict__ S, int lds, int cout,
-                                                   TO* __restrict__ Out, const int* __restrict__ cond) {
+                                                   TO* __restrict__ Out, const int* __restrict__ cond, int nbuf) {
     if (cond && *cond == 0) return;
-    extern __shared__ double sm[];  // S: c*cout | X tile: kRmRows*c
+    extern __shared__ double sm[];  // S: c*cout doubles | nbuf X tiles of kRmRows*c TI
     double* ss = sm;
-    double* xs = sm + c * cout;
+    TI* xbuf = reinterpret_cast<TI*>(sm + c * cout);
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     for (int t = threadIdx.x; t < c * cout; t += blockDim.x) ss[t] = S[(t / cout) * lds + t % cout];
-    for (int64_t r0 = (int64_t)blockIdx.x * kRmRows; r0 < rows; r0 += (int64_t)gridDim.x * kRmRows) {
+    auto load = [&](int64_t r0, int b) {  // tile at row r0 into buffer b (asynchronous)
         const int nr = (int)std::min<int64_t>(kRmRows, rows - r0);
+        TI* xs = xbuf + (size_t)b * kRmRows * c;
+        for (int t = threadIdx.x; t < nr * c; t += blockDim.x) rm_cp_async(xs + t, X + r0 * c + t, (int)sizeof(TI));
+    };
+    const int64_t step = (int64_t)gridDim.x * kRmRows;
+    int64_t r0 = (int64_t)blockIdx.x * kRmRows;
+    if (r0 < rows) load(r0, 0);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    for (int it = 0; r0 < rows; r0 += step, ++it) {
+        const int b = nbuf == 2 ? (it & 1) : 0;
+        if (nbuf == 2 && r0 + step < rows) load(r0 + step, b ^ 1);
+        asm volatile("cp.async.commit_group;" ::: "memory");  // possibly empty: one group per iteration
+        asm volatile("cp.async.wait_group 1;" ::: "memory");  // this tile's group has landed
         __syncthreads();
-        for (int t = threadIdx.x; t < nr * c; t += blockDim.x) xs[t] = (double)X[r0 * c + t];
-        __syncthreads();
+        const TI* xs = xbuf + (size_t)b * kRmRows * c;
+        const int nr = (int)std::min<int64_t>(kRmRows, rows - r0);
         double acc[4][NJ];
 #pragma unroll
         for (int i = 0; i < 4; ++i)
@@ -171,7 +190,7 @@ __global__ void __launch_bounds__(256) k_right_mul(const TI* __restrict__ X, int
         for (int k = 0; k < c; ++k) {
             double xv[4], sv[NJ];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) xv[i] = (ty + 16 * i < nr) ? xs[(ty + 16 * i) * c + k] : 0.0;
+            for (int i = 0; i < 4; ++i) xv[i] = (ty + 16 * i < nr) ? (double)xs[(ty + 16 * i) * c + k] : 0.0;
 #pragma unroll
             for (int j = 0; j < NJ; ++j) sv[j] = (tx + 16 * j < cout) ? ss[k * cout + tx + 16 * j] : 0.0;
 #pragma unroll
@@ -189,7 +208,13 @@ __global__ void __launch_bounds__(256) k_right_mul(const TI* __restrict__ X, int
                 if (col < cout) Out[(r0 + rr) * cout + col] = (TO)acc[i][j];
             }
         }
+        __syncthreads();  // this buffer is read; it may be refilled
+        if (nbuf == 1 && r0 + step < rows) {
+            load(r0 + step, 0);
+            asm volatile("cp.async.commit_group;" ::: "memory");  // older than the next iteration's group
+        }
     }
+    asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
 __global__ void k_copy_cond(const double* __restrict__ src, double* __restrict__ dst, int64_t n,
@@ -376,14 +401,20 @@ static void gram(RandCtx& cx, const double* X, int64_t rows, int c, double* G, c
 
 static void right_mul(const double* X, int64_t rows, int c, const double* S, int lds, int cout, double* Out,
                       cudaStream_t s, const int* cond = nullptr) {
-    const size_t smem = ((size_t)c * cout + (size_t)kRmRows * c) * sizeof(double);
-    if (smem > 220 * 1024 || cout > 128) throw Error(SVDB_ERR_UNSUPPORTED, "dense factor wider than the shared-memory tile");
-    const int blocks = (int)std::max<int64_t>(
-        1, std::min<int64_t>((rows + kRmRows - 1) / kRmRows, (int64_t)device_props().sms * 4));
+    const size_t s_bytes = (size_t)c * cout * sizeof(double), tile = (size_t)kRmRows * c * sizeof(double);
+    if (s_bytes + tile > 220 * 1024 || cout > 128)
+        throw Error(SVDB_ERR_UNSUPPORTED, "dense factor wider than the shared-memory tile");
+    const int nbuf = (s_bytes + 2 * tile <= 220 * 1024) ? 2 : 1;
+    const size_t smem = s_bytes + nbuf * tile;
+    const int64_t tiles = (rows + kRmRows - 1) / kRmRows;
     auto go = [&](auto kern) {
         if (smem > 48 * 1024)
             SVDB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        kern<<<blocks, 256, smem, s>>>(X, rows, c, S, lds, cout, Out, cond);
+        int per_sm = 0;  // one wave of resident blocks, each looping over tiles
+        SVDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem));
+        const int blocks = (int)std::max<int64_t>(
+            1, std::min<int64_t>(tiles, (int64_t)device_props().sms * std::max(per_sm, 1)));
+        kern<<<blocks, 256, smem, s>>>(X, rows, c, S, lds, cout, Out, cond, nbuf);
     };
     if (cout <= 16) go(k_right_mul<double, double, 1>);
     else if (cout <= 32) go(k_right_mul<double, double, 2>);
