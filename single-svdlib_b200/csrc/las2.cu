@@ -681,17 +681,19 @@ void Las2Run::ritvec(int64_t dimensions, double kappa, int64_t steps, int64_t ne
     SVDB_CUDA(cudaEventCreate(&e1));
     SVDB_CUDA(cudaEventRecord(e0, s_));
     const int64_t nrot = (int64_t)R.i.size();
-    DevBuf<int32_t> ri(std::max<int64_t>(nrot, 1), s_), dperm(js, s_), drowk(d_out, s_);
-    DevBuf<double> rc(std::max<int64_t>(nrot, 1), s_), rs(std::max<int64_t>(nrot, 1), s_), Z(js * js, s_),
-        C(d_out * js, s_);
+    std::vector<double> hcs;
+    std::vector<int32_t> hil;
+    rot_pack(R.i.data(), R.c.data(), R.s.data(), nrot, js, hcs, hil);
+    const int64_t npad = rot_padded(nrot);
+    DevBuf<int32_t> dil(2 * npad, s_), dperm(js, s_), drowk(d_out, s_);
+    DevBuf<double> dcs(2 * npad, s_), Z(js * js, s_), C(d_out * js, s_);
     if (nrot) {
-        SVDB_CUDA(cudaMemcpyAsync(ri.p, R.i.data(), nrot * 4, cudaMemcpyHostToDevice, s_));
-        SVDB_CUDA(cudaMemcpyAsync(rc.p, R.c.data(), nrot * 8, cudaMemcpyHostToDevice, s_));
-        SVDB_CUDA(cudaMemcpyAsync(rs.p, R.s.data(), nrot * 8, cudaMemcpyHostToDevice, s_));
+        SVDB_CUDA(cudaMemcpyAsync(dcs.p, hcs.data(), nrot * 16, cudaMemcpyHostToDevice, s_));
+        SVDB_CUDA(cudaMemcpyAsync(dil.p, hil.data(), nrot * 8, cudaMemcpyHostToDevice, s_));
     }
     SVDB_CUDA(cudaMemcpyAsync(dperm.p, R.perm.data(), js * 4, cudaMemcpyHostToDevice, s_));
     SVDB_CUDA(cudaMemcpyAsync(drowk.p, rowk.data(), d_out * 4, cudaMemcpyHostToDevice, s_));
-    rot_apply(Z.p, js, ri.p, rc.p, rs.p, nrot, s_);
+    rot_apply(Z.p, js, dcs.p, dil.p, nrot, s_);
     build_coef(Z.p, js, dperm.p, drowk.p, d_out, md_.legacy, ae, C.p, s_);
     SVDB_CUDA(cudaEventRecord(e1, s_));
     backtransform(C.p, Q_.p, js, n_, d_out, out.Vt.p, s_);

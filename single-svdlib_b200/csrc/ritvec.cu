@@ -17,15 +17,15 @@
 namespace svdb {
 
 // Z is column-major: Z(row k, col i) at z[i * js + k]; thread k walks row k.
-__global__ void __launch_bounds__(128) k_rot_apply(double* __restrict__ z, int64_t js,
-                                                   const int32_t* __restrict__ ri, const double* __restrict__ rc,
-                                                   const double* __restrict__ rs, int64_t nrot) {
+// Rotation t is (c, s) = cs[t] and index il[t].x (rot_pack).
+__global__ void __launch_bounds__(128) k_rot_apply(double* __restrict__ z, int64_t js, const double2* __restrict__ cs,
+                                                   const int2* __restrict__ il, int64_t nrot) {
     const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= js) return;
     for (int64_t i = 0; i < js; ++i) z[i * js + k] = (i == k) ? 1.0 : 0.0;
     for (int64_t t = 0; t < nrot; ++t) {
-        const int64_t i = ri[t];
-        const double c = rc[t], s = rs[t];
+        const int64_t i = il[t].x;
+        const double c = cs[t].x, s = cs[t].y;
         double* zi = z + i * js + k;
         double* zi1 = z + (i + 1) * js + k;
         const double f = *zi1;
@@ -36,49 +36,141 @@ __global__ void __launch_bounds__(128) k_rot_apply(double* __restrict__ z, int64
 }
 
 // The same in shared memory: block b owns rows b*ROWS .. +ROWS of Z, stored
-// as zs[i * ROWS + local row]; the rotation list is staged in chunks that
-// every thread reads (a broadcast).  Within a QL sweep the rotations walk i
-// downwards, and rotation i - 1 reads as f the z[i] that rotation i has just
-// written: it is handed over in a register.  Each element still sees the
-// crate's operations in order (unfused), so Z is bit-identical.
-constexpr int kRotChunk = 1024;
-__global__ void __launch_bounds__(64) k_rot_apply_smem(double* __restrict__ z, int64_t js,
-                                                       const int32_t* __restrict__ ri,
-                                                       const double* __restrict__ rc,
-                                                       const double* __restrict__ rs, int64_t nrot) {
-    extern __shared__ double zs[];  // js x blockDim.x
-    __shared__ int32_t sri[kRotChunk];
-    __shared__ double src_[kRotChunk], srs[kRotChunk];
-    const int rows = blockDim.x, tid = threadIdx.x;
-    const int64_t k = blockIdx.x * (int64_t)rows + tid;
-    for (int64_t i = 0; i < js; ++i) zs[i * rows + tid] = (i == k) ? 1.0 : 0.0;
-    int64_t prev = -2;
-    double carry = 0.0;
-    for (int64_t t0 = 0; t0 < nrot; t0 += kRotChunk) {
-        const int cnt = (int)min((int64_t)kRotChunk, nrot - t0);
-        __syncthreads();
-        for (int u = tid; u < cnt; u += rows) {
-            sri[u] = ri[t0 + u];
-            src_[u] = rc[t0 + u];
-            srs[u] = rs[t0 + u];
-        }
-        __syncthreads();
-        for (int u = 0; u < cnt; ++u) {
-            const int64_t i = sri[u];
-            const double c = src_[u], s = srs[u];
-            const double f = (i + 1 == prev) ? carry : zs[(i + 1) * rows + tid];
-            const double a = zs[i * rows + tid];
-            const double hi = add_rn(mul_rn(s, a), mul_rn(c, f));
-            const double lo = sub_rn(mul_rn(c, a), mul_rn(s, f));
-            zs[(i + 1) * rows + tid] = hi;
-            zs[i * rows + tid] = lo;
-            carry = lo;
-            prev = i;
-        }
+// as zs[i * ROWS + local row].  The rotation list arrives in segments
+// (rot_pack): runs of consecutive rotations whose index falls by one, as a
+// QL sweep makes them.  Inside a segment every z[i] is read (as a) before it
+// is written (as the hi of rotation i - 1), and rotation i - 1 reads as f the
+// lo that rotation i has just made, which stays in a register and is stored
+// once, at the segment's end.  So the a values and (c, s) of the next group
+// of kRotGroup rotations are read while the current group computes (two
+// register sets in turn), and what remains in sequence is f <- c*a - s*f.
+// With ROWS a compile-time constant every z access is an immediate offset
+// from the group's base, and (c, s) is one 16-byte broadcast read: about ten
+// instructions per rotation, against a 16-cycle chain.  Each element still
+// sees the crate's operations in order (unfused), so Z is bit-identical.  The
+// lists are staged by chunks of kRotChunk in two shared-memory buffers: the
+// next chunk is copied (cp.async) while the current one is applied.
+constexpr int kRotGroup = 8;
+
+__device__ __forceinline__ void rot_cp16(void* dst, const void* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+
+struct RotStage {
+    double2* cs;
+    int2* il;
+};
+
+__device__ __forceinline__ RotStage rot_stage(unsigned char* base, int b) {
+    unsigned char* p = base + (size_t)b * kRotChunk * kRotStageBytes;
+    return RotStage{reinterpret_cast<double2*>(p), reinterpret_cast<int2*>(p + kRotChunk * 16)};
+}
+
+// Copies rotations t0 .. t0 + cnt (cnt rounded up to 4: the device lists are
+// padded to a multiple of 4 entries) into stage st.
+__device__ __forceinline__ void rot_stage_load(const RotStage& st, const double2* cs, const int2* il, int64_t t0,
+                                               int cnt) {
+    const int c4 = (cnt + 3) & ~3;
+    const int ni = c4 / 2;  // 16-byte units of il (cs has c4)
+    for (int u = threadIdx.x; u < c4 + ni; u += blockDim.x) {
+        if (u < c4) rot_cp16(st.cs + u, cs + t0 + u);
+        else rot_cp16(st.il + 2 * (u - c4), il + t0 + 2 * (u - c4));
     }
-    __syncthreads();
+}
+
+// Group of kRotGroup rotations at indices top', top' - 1, ...: zg points at
+// z[top'] of this thread's row, pg at the group's (c, s).
+template <int ROWS>
+__device__ __forceinline__ void rot_group_load(const double* zg, const double2* pg, double (&A)[kRotGroup],
+                                               double2 (&C)[kRotGroup]) {
+#pragma unroll
+    for (int q = 0; q < kRotGroup; ++q) {
+        A[q] = zg[-q * ROWS];
+        C[q] = pg[q];
+    }
+}
+
+template <int ROWS>
+__device__ __forceinline__ void rot_group_apply(double* zg, const double (&A)[kRotGroup],
+                                                const double2 (&C)[kRotGroup], double& f) {
+#pragma unroll
+    for (int q = 0; q < kRotGroup; ++q) {
+        const double hi = add_rn(mul_rn(C[q].y, A[q]), mul_rn(C[q].x, f));
+        f = sub_rn(mul_rn(C[q].x, A[q]), mul_rn(C[q].y, f));
+        zg[-(q - 1) * ROWS] = hi;  // z[i + 1]
+    }
+}
+
+template <int ROWS>
+__global__ void __launch_bounds__(ROWS) k_rot_apply_smem(double* __restrict__ z, int64_t js,
+                                                         const double2* __restrict__ cs,
+                                                         const int2* __restrict__ il, int64_t nrot) {
+    extern __shared__ __align__(16) unsigned char rot_smem[];
+    double* zs = reinterpret_cast<double*>(rot_smem + 2 * kRotChunk * kRotStageBytes);  // js x ROWS
+    const int tid = threadIdx.x;
+    const int64_t k = blockIdx.x * (int64_t)ROWS + tid;
+    for (int64_t i = 0; i < js; ++i) zs[i * ROWS + tid] = (i == k) ? 1.0 : 0.0;
+    constexpr int G = kRotGroup;
+    const int64_t nchunk = (nrot + kRotChunk - 1) / kRotChunk;
+    if (nchunk > 0) rot_stage_load(rot_stage(rot_smem, 0), cs, il, 0, (int)(nrot < kRotChunk ? nrot : kRotChunk));
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    for (int64_t ch = 0; ch < nchunk; ++ch) {
+        const int64_t t1 = (ch + 1) * kRotChunk;
+        if (t1 < nrot)
+            rot_stage_load(rot_stage(rot_smem, (int)((ch + 1) & 1)), cs, il, t1,
+                           (int)(nrot - t1 < kRotChunk ? nrot - t1 : kRotChunk));
+        asm volatile("cp.async.commit_group;" ::: "memory");  // possibly empty: one group per chunk
+        asm volatile("cp.async.wait_group 1;" ::: "memory");  // this chunk's copies have landed
+        __syncthreads();
+        const RotStage st = rot_stage(rot_smem, (int)(ch & 1));
+        const int cnt = (int)(nrot - ch * kRotChunk < kRotChunk ? nrot - ch * kRotChunk : kRotChunk);
+        for (int u = 0; u < cnt;) {
+            const int2 h = st.il[u];  // (top index, segment length)
+            const int len = h.y;
+            double* zp = zs + h.x * ROWS + tid;  // z[top]
+            const double2* p = st.cs + u;
+            double f = zp[ROWS];
+            const int nfull = len / G, rem = len - nfull * G;
+            double A0[G], A1[G];
+            double2 C0[G], C1[G];
+            int g = 0;
+            if (nfull > 0) rot_group_load<ROWS>(zp, p, A0, C0);
+            for (; g + 2 <= nfull; g += 2) {  // the next group is untouched by this one
+                rot_group_load<ROWS>(zp - (g + 1) * G * ROWS, p + (g + 1) * G, A1, C1);
+                rot_group_apply<ROWS>(zp - g * G * ROWS, A0, C0, f);
+                if (g + 2 < nfull) rot_group_load<ROWS>(zp - (g + 2) * G * ROWS, p + (g + 2) * G, A0, C0);
+                rot_group_apply<ROWS>(zp - (g + 1) * G * ROWS, A1, C1, f);
+            }
+            if (g < nfull) {
+                rot_group_apply<ROWS>(zp - g * G * ROWS, A0, C0, f);
+                ++g;
+            }
+            if (rem) {
+                double* zt = zp - nfull * G * ROWS;
+                const double2* pt = p + nfull * G;
+#pragma unroll
+                for (int q = 0; q < G; ++q)
+                    if (q < rem) {
+                        A1[q] = zt[-q * ROWS];
+                        C1[q] = pt[q];
+                    }
+#pragma unroll
+                for (int q = 0; q < G; ++q)
+                    if (q < rem) {
+                        const double hi = add_rn(mul_rn(C1[q].y, A1[q]), mul_rn(C1[q].x, f));
+                        f = sub_rn(mul_rn(C1[q].x, A1[q]), mul_rn(C1[q].y, f));
+                        zt[-(q - 1) * ROWS] = hi;
+                    }
+            }
+            zp[-(len - 1) * ROWS] = f;  // z[bottom] = the last lo
+            u += len;
+        }
+        __syncthreads();  // this stage is refilled by the next iteration's copy
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
     if (k < js)
-        for (int64_t i = 0; i < js; ++i) z[i * js + k] = zs[i * rows + tid];
+        for (int64_t i = 0; i < js; ++i) z[i * js + k] = zs[i * ROWS + tid];
 }
 
 // C (d x js) row-major.  The final Z after imtql2's column sort is
@@ -181,24 +273,51 @@ static int nblk(int64_t work, int threads) {
     return (int)std::max<int64_t>(1, std::min<int64_t>(b, (int64_t)device_props().sms * 16));
 }
 
-void rot_apply(double* z, int64_t js, const int32_t* ri, const double* rc, const double* rs, int64_t nrot,
-               cudaStream_t s) {
-    // rows per block in shared memory: as many as fit next to the staged rotations
-    const size_t avail = 200 * 1024;
-    int rows = 64;
-    while (rows >= 16 && (size_t)js * rows * sizeof(double) > avail) rows >>= 1;
-    if (rows >= 16) {
-        const size_t smem = (size_t)js * rows * sizeof(double);
-        // the kernel also holds 20 KB of static shared memory: always raise the dynamic limit
-        SVDB_CUDA(cudaFuncSetAttribute(k_rot_apply_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_rot_apply_smem<<<(unsigned)((js + rows - 1) / rows), rows, smem, s>>>(z, js, ri, rc, rs, nrot);
-        const cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess)
-            throw Error(SVDB_ERR_CUDA, "k_rot_apply_smem(js=" + std::to_string(js) + ", rows=" + std::to_string(rows) +
-                                           ", smem=" + std::to_string(smem) + "): " + cudaGetErrorString(e));
-    } else {
-        k_rot_apply<<<(unsigned)((js + 127) / 128), 128, 0, s>>>(z, js, ri, rc, rs, nrot);
+void rot_pack(const int32_t* ri, const double* rc, const double* rs, int64_t nrot, int64_t js,
+              std::vector<double>& cs, std::vector<int32_t>& il) {
+    const int64_t npad = rot_padded(nrot);
+    cs.assign((size_t)(2 * npad), 0.0);
+    il.assign((size_t)(2 * npad), 0);
+    int64_t start = 0;
+    for (int64_t t = 0; t <= nrot; ++t) {
+        if (t < nrot) {
+            if (ri[t] < 0 || ri[t] > js - 2)
+                throw Error(SVDB_ERR_LAS2, "rotation " + std::to_string(t) + " has index " + std::to_string(ri[t]) +
+                                               " outside [0, " + std::to_string(js - 2) + "]");
+            cs[(size_t)(2 * t)] = rc[t];
+            cs[(size_t)(2 * t + 1)] = rs[t];
+            il[(size_t)(2 * t)] = ri[t];
+        }
+        const bool cut = t == nrot || (t > start && (t % kRotChunk == 0 || ri[t] != ri[t - 1] - 1));
+        if (cut) {
+            il[(size_t)(2 * start + 1)] = (int32_t)(t - start);
+            start = t;
+        }
     }
+}
+
+template <int ROWS>
+static void launch_rot_smem(double* z, int64_t js, const double2* cs, const int2* il, int64_t nrot, cudaStream_t s) {
+    const size_t smem = 2 * (size_t)kRotChunk * kRotStageBytes + (size_t)js * ROWS * sizeof(double);
+    SVDB_CUDA(cudaFuncSetAttribute(k_rot_apply_smem<ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_rot_apply_smem<ROWS><<<(unsigned)((js + ROWS - 1) / ROWS), ROWS, smem, s>>>(z, js, cs, il, nrot);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+        throw Error(SVDB_ERR_CUDA, "k_rot_apply_smem(js=" + std::to_string(js) + ", rows=" + std::to_string(ROWS) +
+                                       ", smem=" + std::to_string(smem) + "): " + cudaGetErrorString(e));
+}
+
+void rot_apply(double* z, int64_t js, const double* cs, const int32_t* il, int64_t nrot, cudaStream_t s) {
+    // rows per block in shared memory: as many as fit next to the two stages
+    const size_t stage = 2 * (size_t)kRotChunk * kRotStageBytes;
+    const size_t avail = (size_t)device_props().smem_optin - stage;
+    const double2* cs2 = reinterpret_cast<const double2*>(cs);
+    const int2* il2 = reinterpret_cast<const int2*>(il);
+    const size_t row_bytes = (size_t)js * sizeof(double);
+    if (row_bytes * 64 <= avail) launch_rot_smem<64>(z, js, cs2, il2, nrot, s);
+    else if (row_bytes * 32 <= avail) launch_rot_smem<32>(z, js, cs2, il2, nrot, s);
+    else if (row_bytes * 16 <= avail) launch_rot_smem<16>(z, js, cs2, il2, nrot, s);
+    else k_rot_apply<<<(unsigned)((js + 127) / 128), 128, 0, s>>>(z, js, cs2, il2, nrot);
     SVDB_CHECK_LAUNCH();
 }
 

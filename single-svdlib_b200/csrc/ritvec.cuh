@@ -3,15 +3,29 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
+#include <vector>
 
 #include "svdb_internal.h"
 
 namespace svdb {
 
-// Z (js x js, column-major) = I rotated by the recorded plane rotations.
-void rot_apply(double* z, int64_t js, const int32_t* ri, const double* rc, const double* rs, int64_t nrot,
-               cudaStream_t s);
+// Rotations are staged in chunks of kRotChunk; a rotation takes 24 bytes of a
+// stage: (c, s) and (index, segment length).
+constexpr int kRotChunk = 512;
+constexpr int kRotStageBytes = 24;
+inline int64_t rot_padded(int64_t nrot) { return std::max<int64_t>(4, (nrot + 3) / 4 * 4); }
+// Packs the recorded rotations for rot_apply: cs[2t], cs[2t+1] = c, s of
+// rotation t; il[2t] = its index; il[2t+1] = the length of the segment that
+// starts at t (0 inside one).  Segments are runs whose index falls by one
+// from rotation to rotation, cut at multiples of kRotChunk.  Both lists hold
+// 2 * rot_padded(nrot) entries.  Throws SVDB_ERR_LAS2 for an index outside
+// [0, js - 2].
+void rot_pack(const int32_t* ri, const double* rc, const double* rs, int64_t nrot, int64_t js,
+              std::vector<double>& cs, std::vector<int32_t>& il);
+// Z (js x js, column-major) = I rotated by the packed rotations.
+void rot_apply(double* z, int64_t js, const double* cs, const int32_t* il, int64_t nrot, cudaStream_t s);
 // Coefficients of the back-transform for output rows rowk[0..d).
 void build_coef(const double* z, int64_t js, const int32_t* perm, const int32_t* rowk, int64_t d, bool legacy,
                 double eps_a, double* C, cudaStream_t s);
