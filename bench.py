@@ -113,6 +113,18 @@ class ClockSampler:
         self.proc = None
         self.out = None
 
+    def _lines(self):
+        try:
+            with open(self.out.name) as f:
+                return sum(1 for _ in f)
+        except OSError:
+            return 0
+
+    def _wait_lines(self, n, limit_s):
+        t_end = time.time() + limit_s
+        while self._lines() < n and time.time() < t_end and self.proc.poll() is None:
+            time.sleep(0.01)
+
     def __enter__(self):
         try:
             self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
@@ -121,10 +133,13 @@ class ClockSampler:
                                          stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
+        if self.proc:
+            self._wait_lines(1, 5.0)  # sampling runs before the timed region starts
         return self
 
     def __exit__(self, *a):
         if self.proc:
+            self._wait_lines(self._lines() + 1, 1.0)  # and one sample at its end
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)

@@ -20,58 +20,12 @@
 
 #include "lanczos_kernel.cuh"
 #include "ops.cuh"
+#include "ql_host.h"
 #include "ritvec.cuh"
 #include "svdb_internal.h"
 
 namespace svdb {
 
-// SvdFloat::eps of the run's scalar T (src/utils.rs:87-113): f64::EPSILON,
-// or f32::EPSILON while a T = f32 run holds a ScalarEps on this thread.  The
-// tolerances, pythag's and compare's thresholds all follow it; the arithmetic
-// stays FP64.
-static thread_local double EPS = std::numeric_limits<double>::epsilon();
-struct ScalarEps {
-    double saved;
-    explicit ScalarEps(bool f32) : saved(EPS) {
-        EPS = f32 ? (double)std::numeric_limits<float>::epsilon() : std::numeric_limits<double>::epsilon();
-    }
-    ~ScalarEps() { EPS = saved; }
-};
-static double eps34() { return std::pow(EPS, 0.75); }
-static inline bool compare(double a, double b) { return std::fabs(b - a) < EPS; }  // src/utils.rs:110-112
-
-// ------------------------------------------------------ scalar helpers ----
-// svd_pythag as written in the current crate (mod.rs:361-380): r = (s/u)^2.
-static double pythag_current(double a, double b) {
-    double n = std::fmax(std::fabs(a), std::fabs(b));
-    if (!(n > 0.0)) return 0.0;
-    double p = n, q = std::fmin(std::fabs(a), std::fabs(b)) / p;
-    double r = q * q, t = 4.0 + r;
-    while (!compare(t, 4.0)) {
-        double s = r / t, u = 1.0 + 2.0 * s;
-        p = p * u;
-        double su = s / u;
-        r = su * su;
-        t = 4.0 + r;
-    }
-    return p;
-}
-// Moler-Morrison as in SVDLIBC / legacy.rs:878-895: r *= (s/u)^2.
-static double pythag_legacy(double a, double b) {
-    double n = std::fmax(std::fabs(a), std::fabs(b));
-    if (!(n > 0.0)) return 0.0;
-    double p = n, q = std::fmin(std::fabs(a), std::fabs(b)) / p;
-    double r = q * q, t = 4.0 + r;
-    while (!compare(t, 4.0)) {
-        double s = r / t, u = 1.0 + 2.0 * s;
-        p *= u;
-        double su = s / u;
-        r *= su * su;
-        t = 4.0 + r;
-    }
-    return p;
-}
-static double fsign(double a, double b) { return ((a >= 0.0 && b >= 0.0) || (a < 0.0 && b < 0.0)) ? a : -a; }
 static size_t idamax(size_t n, const double* x) {
     if (n == 0) throw Error(SVDB_ERR_SHAPE, "svd_idamax: unexpected inputs!");
     size_t imax = 0;
@@ -200,77 +154,6 @@ static void imtqlb_current(size_t n, double* d, double* e, double* bnd, size_t m
     }
 }
 
-// imtqlb of SVDLIBC (legacy.rs:955-1070)
-static void imtqlb_legacy(size_t n, double* d, double* e, double* bnd) {
-    if (n == 1) return;
-    bnd[0] = 1.0;
-    size_t last = n - 1;
-    for (size_t i = 1; i <= last; ++i) { bnd[i] = 0.0; e[i - 1] = e[i]; }
-    e[last] = 0.0;
-    size_t i = 0;
-    for (size_t l = 0; l <= last; ++l) {
-        size_t iteration = 0;
-        while (iteration <= 30) {
-            size_t m = l;
-            while (m < n) {
-                if (m == last) break;
-                double test = std::fabs(d[m]) + std::fabs(d[m + 1]);
-                if (compare(test, test + std::fabs(e[m]))) break;
-                ++m;
-            }
-            double p = d[l], f = bnd[l];
-            if (m == l) {
-                bool exchange = true;
-                if (l > 0) {
-                    i = l;
-                    while (i >= 1 && exchange) {
-                        if (p < d[i - 1]) { d[i] = d[i - 1]; bnd[i] = bnd[i - 1]; --i; }
-                        else exchange = false;
-                    }
-                }
-                if (exchange) i = 0;
-                d[i] = p;
-                bnd[i] = f;
-                iteration = 31;
-            } else {
-                if (iteration == 30)
-                    throw Error(SVDB_ERR_IMTQLB,
-                                "svdlibrs/imtqlb: imtqlb no convergence to an eigenvalue after 30 iterations");
-                ++iteration;
-                double g = (d[l + 1] - p) / (2.0 * e[l]);
-                double r = pythag_legacy(g, 1.0);
-                g = d[m] - p + e[l] / (g + fsign(r, g));
-                double s = 1.0, c = 1.0;
-                p = 0.0;
-                i = m - 1;
-                bool underflow = false;
-                while (!underflow && i >= l) {
-                    f = s * e[i];
-                    double b = c * e[i];
-                    r = pythag_legacy(f, g);
-                    e[i + 1] = r;
-                    if (compare(r, 0.0)) { underflow = true; break; }
-                    s = f / r;
-                    c = g / r;
-                    g = d[i + 1] - p;
-                    r = (d[i] - g) * s + 2.0 * c * b;
-                    p = s * r;
-                    d[i + 1] = g + p;
-                    g = c * r - b;
-                    f = bnd[i + 1];
-                    bnd[i + 1] = s * bnd[i] + c * f;
-                    bnd[i] = c * bnd[i] - s * f;
-                    if (i == 0) break;
-                    --i;
-                }
-                if (underflow) d[i + 1] -= p;
-                else { d[l] -= p; e[l] = g; }
-                e[m] = 0.0;
-            }
-        }
-    }
-}
-
 // error_bound (mod.rs:840-899, identical in legacy.rs)
 static size_t error_bound(bool& enough, double endl, double endr, double* ritz, double* bnd, size_t step,
                           double tol) {
@@ -306,86 +189,6 @@ static size_t error_bound(bool& enough, double endl, double endr, double* ritz, 
         }
     }
     return neig;
-}
-
-// The scalar chain of imtql2 (mod.rs:901-1028 / legacy.rs:1590-1700) without
-// z: every applied rotation is recorded, and the final selection sort of the
-// eigenvalues becomes a column permutation.
-struct Rotations {
-    std::vector<int32_t> i;
-    std::vector<double> c, s;
-    std::vector<int32_t> perm;
-};
-
-static void imtql2_scalar(size_t n, double* d, double* e, const Mode& md, Rotations& R) {
-    const size_t max_it = md.max_imtql2;
-    R.perm.resize(n);
-    for (size_t k = 0; k < n; ++k) R.perm[k] = (int32_t)k;
-    if (n == 1) return;
-    size_t last = n - 1;
-    for (size_t i = 1; i < n; ++i) e[i - 1] = e[i];
-    e[last] = 0.0;
-    for (size_t l = 0; l < n; ++l) {
-        size_t iteration = 0;
-        while (iteration <= max_it) {
-            size_t m = l;
-            while (m < n) {
-                if (m == last) break;
-                double test = std::fabs(d[m]) + std::fabs(d[m + 1]);
-                if (compare(test, test + std::fabs(e[m]))) break;
-                ++m;
-            }
-            if (m == l) break;
-            if (iteration == max_it) {
-                char buf[160];
-                snprintf(buf, sizeof buf,
-                         "svdlibrs/imtql2: imtql2 no convergence to an eigenvalue after %zu iterations", max_it);
-                throw Error(SVDB_ERR_IMTQL2, buf);
-            }
-            ++iteration;
-            double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
-            double r = md.legacy ? pythag_legacy(g, 1.0) : pythag_current(g, 1.0);
-            g = d[m] - d[l] + e[l] / (g + fsign(r, g));
-            double s = 1.0, c = 1.0, p = 0.0;
-            size_t i = m - 1;
-            bool underflow = false;
-            while (!underflow && i >= l) {
-                double f = s * e[i];
-                double b = c * e[i];
-                r = md.legacy ? pythag_legacy(f, g) : pythag_current(f, g);
-                e[i + 1] = r;
-                if (compare(r, 0.0)) underflow = true;
-                else {
-                    s = f / r;
-                    c = g / r;
-                    g = d[i + 1] - p;
-                    r = (d[i] - g) * s + 2.0 * c * b;
-                    p = s * r;
-                    d[i + 1] = g + p;
-                    g = c * r - b;
-                    R.i.push_back((int32_t)i);
-                    R.c.push_back(c);
-                    R.s.push_back(s);
-                    if (i == 0) break;
-                    --i;
-                }
-            }
-            if (underflow) d[i + 1] -= p;
-            else { d[l] -= p; e[l] = g; }
-            e[m] = 0.0;
-        }
-    }
-    for (size_t l = 1; l < n; ++l) {
-        size_t i = l - 1, k = i;
-        double p = d[i];
-        for (size_t j = l; j < n; ++j)
-            if (d[j] < p) { k = j; p = d[j]; }
-        if (k != i) {
-            d[k] = d[i];
-            d[i] = p;
-            std::swap(R.perm[i], R.perm[k]);
-        }
-    }
 }
 
 // ----------------------------------------------------------- the run ----
@@ -430,6 +233,10 @@ class Las2Run {
     int64_t npurge_ = 0;
     int lz_blocks_ = 0, lz_cluster_ = 0;
     std::vector<double> alf_h_, bet_h_, ritz_, bnd_, w5_;
+    // rotations of lanso's last Ritz analysis when it ran imtqlb (SVDLIBC)
+    // on the whole T: ritvec's imtql2 would make the same ones (ql_host.h)
+    Rotations lz_rot_;
+    int64_t lz_rot_n_ = -1;
 
     double* w(int k) { return W_[perm_[k]].p; }
     void opb(const double* x, double* y) {
@@ -587,6 +394,7 @@ int64_t Las2Run::lanso(int64_t dim, int64_t iterations, double endl, double endr
         }
         // analyse T in unreduced blocks (mod.rs:1345-1377)
         int64_t l = 0;
+        lz_rot_n_ = -1;
         for (int64_t it = 0; it < j; ++it) {
             if (l > j) break;
             int64_t i = l;
@@ -599,7 +407,11 @@ int64_t Las2Run::lanso(int64_t dim, int64_t iterations, double endl, double endr
             size_t sz = (size_t)(i - l);
             dcopy_rev(sz + 1, l, alf_h_.data(), ritz_.data());
             dcopy_rev(sz, l + 1, bet_h_.data(), w5_.data());
-            if (md_.legacy) imtqlb_legacy(sz + 1, ritz_.data() + l, w5_.data() + l, bnd_.data() + l);
+            if (md_.legacy) {
+                const bool whole = l == 0 && i == j;
+                imtqlb_legacy(sz + 1, ritz_.data() + l, w5_.data() + l, bnd_.data() + l, whole ? &lz_rot_ : nullptr);
+                if (whole) lz_rot_n_ = (int64_t)sz + 1;
+            }
             else imtqlb_current(sz + 1, ritz_.data() + l, w5_.data() + l, bnd_.data() + l, md_.max_imtqlb, warned);
             for (int64_t mm = l; mm <= i; ++mm) bnd_[mm] = rnm * std::fabs(bnd_[mm]);
             l = i + 1;
@@ -634,7 +446,19 @@ void Las2Run::ritvec(int64_t dimensions, double kappa, int64_t steps, int64_t ne
     SVDB_CUDA(cudaStreamSynchronize(s_));
     dcopy_rev((size_t)steps, 1, bet_h_.data(), w5_.data());
     Rotations R;
-    imtql2_scalar((size_t)js, d.data(), w5_.data(), md_, R);
+    if (md_.legacy && lz_rot_n_ == js && md_.max_imtql2 == 30) {
+        // T is the one lanso's last imtqlb saw: its record is imtql2's
+        R.i.swap(lz_rot_.i);
+        R.c.swap(lz_rot_.c);
+        R.s.swap(lz_rot_.s);
+        d = lz_rot_.d;
+        R.perm.resize((size_t)js);
+        for (int64_t k = 0; k < js; ++k) R.perm[(size_t)k] = (int32_t)k;
+        ql_sort_perm((size_t)js, d.data(), R.perm);
+        lz_rot_n_ = -1;
+    } else {
+        imtql2_scalar((size_t)js, d.data(), w5_.data(), md_.legacy, md_.max_imtql2, R);
+    }
 
     // selection of the output rows (their ritz index k, in output order)
     std::vector<int32_t> rowk;
