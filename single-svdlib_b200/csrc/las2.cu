@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <limits>
 #include <random>
 
@@ -211,6 +212,17 @@ class Las2Run {
         : A_(A), s_(s), fp32_(fp32 || f32), f32_(f32) {
         legacy_ = legacy;
     }
+    ~Las2Run() {
+        for (int b = 0; b < 2; ++b) {
+            if (rot_ev_[b]) {
+                cudaEventSynchronize(rot_ev_[b]);  // the copy out of rot_pin_[b] has finished
+                cudaEventDestroy(rot_ev_[b]);
+            }
+            host_result_free(rot_pin_[b]);
+        }
+    }
+    Las2Run(const Las2Run&) = delete;
+    Las2Run& operator=(const Las2Run&) = delete;
 
     void run(int64_t dimensions, int64_t iterations, double endl, double endr, double kappa, uint32_t seed,
              Las2Out& out);
@@ -237,6 +249,20 @@ class Las2Run {
     // on the whole T: ritvec's imtql2 would make the same ones (ql_host.h)
     Rotations lz_rot_;
     int64_t lz_rot_n_ = -1;
+    // Z of that T, applied on the stream piece by piece while imtqlb runs
+    // (a recorded rotation is final): kRotPiece rotations a piece, packed
+    // into two page-locked buffers in turn
+    static constexpr size_t kRotPiece = 8192;
+    DevBuf<double> zrot_, rot_dcs_;
+    DevBuf<int32_t> rot_dil_;
+    void* rot_pin_[2] = {nullptr, nullptr};
+    cudaEvent_t rot_ev_[2] = {nullptr, nullptr};
+    int rot_buf_ = 0;
+    int64_t zrot_n_ = -1, zrot_js_ = 0, zrot_js_cur_ = 0;
+    size_t rot_done_ = 0;
+    bool rot_started_ = false;
+    void rot_stream_begin(int64_t js);
+    void rot_stream_flush(size_t upto);
 
     double* w(int k) { return W_[perm_[k]].p; }
     void opb(const double* x, double* y) {
@@ -251,6 +277,46 @@ class Las2Run {
     int64_t lanso(int64_t dim, int64_t iterations, double endl, double endr, int64_t& neig, uint32_t seed);
     void ritvec(int64_t dimensions, double kappa, int64_t steps, int64_t neig, Las2Out& out);
 };
+
+void Las2Run::rot_stream_begin(int64_t js) {
+    if (!rot_pin_[0]) {
+        const size_t bytes = (size_t)rot_padded((int64_t)kRotPiece) * 24;  // (c, s) and (index, length)
+        for (int b = 0; b < 2; ++b) {
+            rot_pin_[b] = host_result_alloc(bytes);
+            SVDB_CUDA(cudaEventCreateWithFlags(&rot_ev_[b], cudaEventDisableTiming));
+        }
+        rot_dcs_.alloc(2 * rot_padded((int64_t)kRotPiece), s_);
+        rot_dil_.alloc(2 * rot_padded((int64_t)kRotPiece), s_);
+    }
+    if (js * js > zrot_js_ * zrot_js_) zrot_.alloc(js * js, s_);
+    zrot_js_ = std::max(zrot_js_, js);
+    zrot_n_ = -1;
+    rot_done_ = 0;
+    rot_started_ = false;
+    zrot_js_cur_ = js;
+}
+
+// Applies rotations rot_done_ .. upto of lz_rot_ to zrot_ (the first piece
+// starts from I; an empty list still makes I).
+void Las2Run::rot_stream_flush(size_t upto) {
+    if (upto == rot_done_ && rot_started_) return;
+    const int64_t cnt = (int64_t)(upto - rot_done_);
+    const int b = rot_buf_;
+    rot_buf_ ^= 1;
+    SVDB_CUDA(cudaEventSynchronize(rot_ev_[b]));  // the copy out of this buffer has finished
+    double* pcs = static_cast<double*>(rot_pin_[b]);
+    int32_t* pil = reinterpret_cast<int32_t*>(pcs + 2 * rot_padded((int64_t)kRotPiece));
+    rot_pack(lz_rot_.i.data() + rot_done_, lz_rot_.c.data() + rot_done_, lz_rot_.s.data() + rot_done_, cnt,
+             zrot_js_cur_, pcs, pil);
+    if (cnt) {
+        SVDB_CUDA(cudaMemcpyAsync(rot_dcs_.p, pcs, (size_t)cnt * 16, cudaMemcpyHostToDevice, s_));
+        SVDB_CUDA(cudaMemcpyAsync(rot_dil_.p, pil, (size_t)cnt * 8, cudaMemcpyHostToDevice, s_));
+    }
+    SVDB_CUDA(cudaEventRecord(rot_ev_[b], s_));
+    rot_apply(zrot_.p, zrot_js_cur_, rot_dcs_.p, rot_dil_.p, cnt, !rot_started_, s_);
+    rot_done_ = upto;
+    rot_started_ = true;
+}
 
 void Las2Run::ensure_q(int64_t rows) {
     if (rows <= qcap_) return;
@@ -394,7 +460,7 @@ int64_t Las2Run::lanso(int64_t dim, int64_t iterations, double endl, double endr
         }
         // analyse T in unreduced blocks (mod.rs:1345-1377)
         int64_t l = 0;
-        lz_rot_n_ = -1;
+        lz_rot_n_ = zrot_n_ = -1;
         for (int64_t it = 0; it < j; ++it) {
             if (l > j) break;
             int64_t i = l;
@@ -408,9 +474,15 @@ int64_t Las2Run::lanso(int64_t dim, int64_t iterations, double endl, double endr
             dcopy_rev(sz + 1, l, alf_h_.data(), ritz_.data());
             dcopy_rev(sz, l + 1, bet_h_.data(), w5_.data());
             if (md_.legacy) {
-                const bool whole = l == 0 && i == j;
-                imtqlb_legacy(sz + 1, ritz_.data() + l, w5_.data() + l, bnd_.data() + l, whole ? &lz_rot_ : nullptr);
-                if (whole) lz_rot_n_ = (int64_t)sz + 1;
+                if (l == 0 && i == j) {  // the whole T: record its rotations and apply them meanwhile
+                    rot_stream_begin((int64_t)sz + 1);
+                    const std::function<void(size_t)> flush = [this](size_t k) { rot_stream_flush(k); };
+                    imtqlb_legacy(sz + 1, ritz_.data(), w5_.data(), bnd_.data(), &lz_rot_, &flush, kRotPiece);
+                    rot_stream_flush(lz_rot_.i.size());
+                    lz_rot_n_ = zrot_n_ = (int64_t)sz + 1;
+                } else {
+                    imtqlb_legacy(sz + 1, ritz_.data() + l, w5_.data() + l, bnd_.data() + l);
+                }
             }
             else imtqlb_current(sz + 1, ritz_.data() + l, w5_.data() + l, bnd_.data() + l, md_.max_imtqlb, warned);
             for (int64_t mm = l; mm <= i; ++mm) bnd_[mm] = rnm * std::fabs(bnd_[mm]);
@@ -446,6 +518,7 @@ void Las2Run::ritvec(int64_t dimensions, double kappa, int64_t steps, int64_t ne
     SVDB_CUDA(cudaStreamSynchronize(s_));
     dcopy_rev((size_t)steps, 1, bet_h_.data(), w5_.data());
     Rotations R;
+    const bool have_z = md_.legacy && lz_rot_n_ == js && zrot_n_ == js && md_.max_imtql2 == 30;
     if (md_.legacy && lz_rot_n_ == js && md_.max_imtql2 == 30) {
         // T is the one lanso's last imtqlb saw: its record is imtql2's
         R.i.swap(lz_rot_.i);
@@ -504,21 +577,28 @@ void Las2Run::ritvec(int64_t dimensions, double kappa, int64_t steps, int64_t ne
     SVDB_CUDA(cudaEventCreate(&e0));
     SVDB_CUDA(cudaEventCreate(&e1));
     SVDB_CUDA(cudaEventRecord(e0, s_));
-    const int64_t nrot = (int64_t)R.i.size();
-    std::vector<double> hcs;
-    std::vector<int32_t> hil;
-    rot_pack(R.i.data(), R.c.data(), R.s.data(), nrot, js, hcs, hil);
-    const int64_t npad = rot_padded(nrot);
-    DevBuf<int32_t> dil(2 * npad, s_), dperm(js, s_), drowk(d_out, s_);
-    DevBuf<double> dcs(2 * npad, s_), Z(js * js, s_), C(d_out * js, s_);
-    if (nrot) {
-        SVDB_CUDA(cudaMemcpyAsync(dcs.p, hcs.data(), nrot * 16, cudaMemcpyHostToDevice, s_));
-        SVDB_CUDA(cudaMemcpyAsync(dil.p, hil.data(), nrot * 8, cudaMemcpyHostToDevice, s_));
+    DevBuf<int32_t> dperm(js, s_), drowk(d_out, s_);
+    DevBuf<double> Z, C(d_out * js, s_);
+    const double* zp = zrot_.p;  // Z made while lanso's imtqlb ran
+    if (!have_z) {
+        const int64_t nrot = (int64_t)R.i.size();
+        std::vector<double> hcs;
+        std::vector<int32_t> hil;
+        rot_pack(R.i.data(), R.c.data(), R.s.data(), nrot, js, hcs, hil);
+        const int64_t npad = rot_padded(nrot);
+        DevBuf<int32_t> dil(2 * npad, s_);
+        DevBuf<double> dcs(2 * npad, s_);
+        Z.alloc(js * js, s_);
+        if (nrot) {
+            SVDB_CUDA(cudaMemcpyAsync(dcs.p, hcs.data(), nrot * 16, cudaMemcpyHostToDevice, s_));
+            SVDB_CUDA(cudaMemcpyAsync(dil.p, hil.data(), nrot * 8, cudaMemcpyHostToDevice, s_));
+        }
+        rot_apply(Z.p, js, dcs.p, dil.p, nrot, true, s_);
+        zp = Z.p;
     }
     SVDB_CUDA(cudaMemcpyAsync(dperm.p, R.perm.data(), js * 4, cudaMemcpyHostToDevice, s_));
     SVDB_CUDA(cudaMemcpyAsync(drowk.p, rowk.data(), d_out * 4, cudaMemcpyHostToDevice, s_));
-    rot_apply(Z.p, js, dcs.p, dil.p, nrot, s_);
-    build_coef(Z.p, js, dperm.p, drowk.p, d_out, md_.legacy, ae, C.p, s_);
+    build_coef(zp, js, dperm.p, drowk.p, d_out, md_.legacy, ae, C.p, s_);
     SVDB_CUDA(cudaEventRecord(e1, s_));
     backtransform(C.p, Q_.p, js, n_, d_out, out.Vt.p, s_);
     sigma_and_u(*op1_, *op2_, fp32_, out.Vt.p, d_out, n_, m_, md_.legacy, ae, out.S.p, out.Ut.p, s_);

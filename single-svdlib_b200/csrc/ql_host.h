@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
+#include <functional>
 #include <limits>
 #include <vector>
 
@@ -80,7 +81,10 @@ struct Rotations {
 // (legacy.rs:1590-1700) on the same (d, e): imtqlb adds only the bnd row and
 // an insertion sort of the converged entries below l, which no later sweep
 // reads.  So for the T that ritvec passes to imtql2 the record is imtql2's.
-static inline void imtqlb_legacy(size_t n, double* d, double* e, double* bnd, Rotations* rec = nullptr) {
+// With flush, flush(k) is called each time the record reaches k rotations, k
+// a multiple of every: rotations before k are final.
+static inline void imtqlb_legacy(size_t n, double* d, double* e, double* bnd, Rotations* rec = nullptr,
+                                 const std::function<void(size_t)>* flush = nullptr, size_t every = 0) {
     if (rec) {
         rec->i.clear();
         rec->c.clear();
@@ -151,6 +155,7 @@ static inline void imtqlb_legacy(size_t n, double* d, double* e, double* bnd, Ro
                         rec->i.push_back((int32_t)i);
                         rec->c.push_back(c);
                         rec->s.push_back(s);
+                        if (flush && rec->i.size() % every == 0) (*flush)(rec->i.size());
                     }
                     if (i == 0) break;
                     --i;

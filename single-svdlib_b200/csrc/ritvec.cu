@@ -19,10 +19,11 @@ namespace svdb {
 // Z is column-major: Z(row k, col i) at z[i * js + k]; thread k walks row k.
 // Rotation t is (c, s) = cs[t] and index il[t].x (rot_pack).
 __global__ void __launch_bounds__(128) k_rot_apply(double* __restrict__ z, int64_t js, const double2* __restrict__ cs,
-                                                   const int2* __restrict__ il, int64_t nrot) {
+                                                   const int2* __restrict__ il, int64_t nrot, int first) {
     const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= js) return;
-    for (int64_t i = 0; i < js; ++i) z[i * js + k] = (i == k) ? 1.0 : 0.0;
+    if (first)
+        for (int64_t i = 0; i < js; ++i) z[i * js + k] = (i == k) ? 1.0 : 0.0;
     for (int64_t t = 0; t < nrot; ++t) {
         const int64_t i = il[t].x;
         const double c = cs[t].x, s = cs[t].y;
@@ -105,12 +106,13 @@ __device__ __forceinline__ void rot_group_apply(double* zg, const double (&A)[kR
 template <int ROWS>
 __global__ void __launch_bounds__(ROWS) k_rot_apply_smem(double* __restrict__ z, int64_t js,
                                                          const double2* __restrict__ cs,
-                                                         const int2* __restrict__ il, int64_t nrot) {
+                                                         const int2* __restrict__ il, int64_t nrot, int first) {
     extern __shared__ __align__(16) unsigned char rot_smem[];
     double* zs = reinterpret_cast<double*>(rot_smem + 2 * kRotChunk * kRotStageBytes);  // js x ROWS
     const int tid = threadIdx.x;
     const int64_t k = blockIdx.x * (int64_t)ROWS + tid;
-    for (int64_t i = 0; i < js; ++i) zs[i * ROWS + tid] = (i == k) ? 1.0 : 0.0;
+    for (int64_t i = 0; i < js; ++i)  // I, or the Z that earlier pieces of the list made
+        zs[i * ROWS + tid] = first ? ((i == k) ? 1.0 : 0.0) : (k < js ? z[i * js + k] : 0.0);
     constexpr int G = kRotGroup;
     const int64_t nchunk = (nrot + kRotChunk - 1) / kRotChunk;
     if (nchunk > 0) rot_stage_load(rot_stage(rot_smem, 0), cs, il, 0, (int)(nrot < kRotChunk ? nrot : kRotChunk));
@@ -273,51 +275,60 @@ static int nblk(int64_t work, int threads) {
     return (int)std::max<int64_t>(1, std::min<int64_t>(b, (int64_t)device_props().sms * 16));
 }
 
-void rot_pack(const int32_t* ri, const double* rc, const double* rs, int64_t nrot, int64_t js,
-              std::vector<double>& cs, std::vector<int32_t>& il) {
+void rot_pack(const int32_t* ri, const double* rc, const double* rs, int64_t nrot, int64_t js, double* cs,
+              int32_t* il) {
     const int64_t npad = rot_padded(nrot);
-    cs.assign((size_t)(2 * npad), 0.0);
-    il.assign((size_t)(2 * npad), 0);
+    std::fill(cs, cs + 2 * npad, 0.0);
+    std::fill(il, il + 2 * npad, 0);
     int64_t start = 0;
     for (int64_t t = 0; t <= nrot; ++t) {
         if (t < nrot) {
             if (ri[t] < 0 || ri[t] > js - 2)
                 throw Error(SVDB_ERR_LAS2, "rotation " + std::to_string(t) + " has index " + std::to_string(ri[t]) +
                                                " outside [0, " + std::to_string(js - 2) + "]");
-            cs[(size_t)(2 * t)] = rc[t];
-            cs[(size_t)(2 * t + 1)] = rs[t];
-            il[(size_t)(2 * t)] = ri[t];
+            cs[2 * t] = rc[t];
+            cs[2 * t + 1] = rs[t];
+            il[2 * t] = ri[t];
         }
         const bool cut = t == nrot || (t > start && (t % kRotChunk == 0 || ri[t] != ri[t - 1] - 1));
         if (cut) {
-            il[(size_t)(2 * start + 1)] = (int32_t)(t - start);
+            il[2 * start + 1] = (int32_t)(t - start);
             start = t;
         }
     }
 }
 
+void rot_pack(const int32_t* ri, const double* rc, const double* rs, int64_t nrot, int64_t js,
+              std::vector<double>& cs, std::vector<int32_t>& il) {
+    cs.resize((size_t)(2 * rot_padded(nrot)));
+    il.resize((size_t)(2 * rot_padded(nrot)));
+    rot_pack(ri, rc, rs, nrot, js, cs.data(), il.data());
+}
+
 template <int ROWS>
-static void launch_rot_smem(double* z, int64_t js, const double2* cs, const int2* il, int64_t nrot, cudaStream_t s) {
+static void launch_rot_smem(double* z, int64_t js, const double2* cs, const int2* il, int64_t nrot, int first,
+                            cudaStream_t s) {
     const size_t smem = 2 * (size_t)kRotChunk * kRotStageBytes + (size_t)js * ROWS * sizeof(double);
     SVDB_CUDA(cudaFuncSetAttribute(k_rot_apply_smem<ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_rot_apply_smem<ROWS><<<(unsigned)((js + ROWS - 1) / ROWS), ROWS, smem, s>>>(z, js, cs, il, nrot);
+    k_rot_apply_smem<ROWS><<<(unsigned)((js + ROWS - 1) / ROWS), ROWS, smem, s>>>(z, js, cs, il, nrot, first);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess)
         throw Error(SVDB_ERR_CUDA, "k_rot_apply_smem(js=" + std::to_string(js) + ", rows=" + std::to_string(ROWS) +
                                        ", smem=" + std::to_string(smem) + "): " + cudaGetErrorString(e));
 }
 
-void rot_apply(double* z, int64_t js, const double* cs, const int32_t* il, int64_t nrot, cudaStream_t s) {
+void rot_apply(double* z, int64_t js, const double* cs, const int32_t* il, int64_t nrot, bool first, cudaStream_t s) {
     // rows per block in shared memory: as many as fit next to the two stages
     const size_t stage = 2 * (size_t)kRotChunk * kRotStageBytes;
     const size_t avail = (size_t)device_props().smem_optin - stage;
     const double2* cs2 = reinterpret_cast<const double2*>(cs);
     const int2* il2 = reinterpret_cast<const int2*>(il);
     const size_t row_bytes = (size_t)js * sizeof(double);
-    if (row_bytes * 64 <= avail) launch_rot_smem<64>(z, js, cs2, il2, nrot, s);
-    else if (row_bytes * 32 <= avail) launch_rot_smem<32>(z, js, cs2, il2, nrot, s);
-    else if (row_bytes * 16 <= avail) launch_rot_smem<16>(z, js, cs2, il2, nrot, s);
-    else k_rot_apply<<<(unsigned)((js + 127) / 128), 128, 0, s>>>(z, js, cs2, il2, nrot);
+    const int f = first ? 1 : 0;
+    if (row_bytes * 64 <= avail) launch_rot_smem<64>(z, js, cs2, il2, nrot, f, s);
+    else if (row_bytes * 32 <= avail) launch_rot_smem<32>(z, js, cs2, il2, nrot, f, s);
+    else if (row_bytes * 16 <= avail) launch_rot_smem<16>(z, js, cs2, il2, nrot, f, s);
+    else k_rot_apply<<<(unsigned)((js + 127) / 128), 128, 0, s>>>(z, js, cs2, il2, nrot, f);
     SVDB_CHECK_LAUNCH();
 }
 

@@ -22,10 +22,14 @@ inline int64_t rot_padded(int64_t nrot) { return std::max<int64_t>(4, (nrot + 3)
 // from rotation to rotation, cut at multiples of kRotChunk.  Both lists hold
 // 2 * rot_padded(nrot) entries.  Throws SVDB_ERR_LAS2 for an index outside
 // [0, js - 2].
+void rot_pack(const int32_t* ri, const double* rc, const double* rs, int64_t nrot, int64_t js, double* cs,
+              int32_t* il);
 void rot_pack(const int32_t* ri, const double* rc, const double* rs, int64_t nrot, int64_t js,
               std::vector<double>& cs, std::vector<int32_t>& il);
-// Z (js x js, column-major) = I rotated by the packed rotations.
-void rot_apply(double* z, int64_t js, const double* cs, const int32_t* il, int64_t nrot, cudaStream_t s);
+// Z (js x js, column-major) = Z0 rotated by the packed rotations, where Z0 is
+// I (first) or Z itself: a list may be applied in consecutive pieces (a cut
+// between two rotations is exact).
+void rot_apply(double* z, int64_t js, const double* cs, const int32_t* il, int64_t nrot, bool first, cudaStream_t s);
 // Coefficients of the back-transform for output rows rowk[0..d).
 void build_coef(const double* z, int64_t js, const int32_t* perm, const int32_t* rowk, int64_t d, bool legacy,
                 double eps_a, double* C, cudaStream_t s);
