@@ -196,6 +196,19 @@ def test_poisson_5000x2000_legacy():
 
 
 @pytest.mark.slow
+def test_poisson_5000x2000_legacy_vectors_with_pieced_rotations():
+    """192 steps give lanso's last imtqlb about 38,000 rotations: Z is built in
+    five pieces of at most 8,192 while the host recurrence runs, after a first
+    analysis pass on T of order 20 (Z reallocated as T grows).  u and vt
+    against the oracle's sequential imtql2."""
+    A = M.poisson_rows(5000, 2000, 20, 42)
+    ref, err, got = run_pair("csr", A, 10, 42, "legacy")
+    assert err is None
+    assert ref["steps"] + 1 > 128  # js^2 / 2 well above one piece
+    check_same(ref, got, s_tol=1e-11, vec_tol=1e-9)
+
+
+@pytest.mark.slow
 def test_poisson_5000x2000_lanczos_as_written_fails_like_the_crate():
     f = FIX["poisson_5000x2000_seed42_dim10"]["lanczos"]
     A = M.poisson_rows(5000, 2000, 20, 42)
