@@ -573,7 +573,7 @@ static void enqueue(svdb_batch& B) {
     const size_t smem = ((size_t)c * (c + 1) + (size_t)(c + 1) * (c + 1) + (c + 1)) * sizeof(double);
     if (smem > 40 * 1024)  // jacobi_svd_body keeps a little static shared memory too
         SVDB_CUDA(cudaFuncSetAttribute(k_b_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_b_jacobi<<<(unsigned)B.count, 512, smem, B.s>>>(B.Rout.p, c, B.Ur.p, B.Vr.p, B.sig.p, B.jstat.p);
+    k_b_jacobi<<<(unsigned)B.count, jacobi_threads(c, 512), smem, B.s>>>(B.Rout.p, c, B.Ur.p, B.Vr.p, B.sig.p, B.jstat.p);
     SVDB_CHECK_LAUNCH();
     // U_b = Q_b V_J[:, :rank] (m x rank);  V_b^T = (Q_Bt U_J[:, :rank])^T (rank x nb)
     right_mul<T, double, false>(B, Y, LY, B.Vr.p, c, (int)B.rank, B.U.p, nullptr);

@@ -154,9 +154,19 @@ __device__ __forceinline__ void chol_inv_body(const double* __restrict__ G, int 
     }
 }
 
+// Lanes per column pair in jacobi_svd_body (about eight elements of a column
+// per lane), and the block size that gives every pair of the padded columns
+// its lanes, capped at `cap` threads.
+__host__ __device__ inline int jacobi_group(int c) { return c <= 64 ? 8 : (c <= 128 ? 16 : 32); }
+__host__ __device__ inline int jacobi_threads(int c, int cap) {
+    const int cp = c + (c & 1);
+    const int t = ((cp / 2) * jacobi_group(c) + 31) / 32 * 32;
+    return t < 32 ? 32 : (t > cap ? cap : t);
+}
+
 // One-sided Jacobi SVD of R (c x c, row-major) in one block: W = R V with
 // orthogonal columns, sigma_j = |W_j|, U_j = W_j / sigma_j.  Round-robin pair
-// ordering, one warp per pair.  Outputs sorted by descending sigma:
+// ordering, jacobi_group(c) lanes per pair.  Outputs sorted by descending sigma:
 // U (c x c), V (c x c), sig (c).  *status = sweeps << 8, | 2 if the sweep limit is reached.
 // sm: (c * cp + cp * cp + cp) doubles, cp = c rounded up to even.  Any
 // block size that is a multiple of 32.
@@ -177,49 +187,62 @@ __device__ __forceinline__ void jacobi_svd_body(const double* __restrict__ R, in
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const int half = cp / 2;
+    // G lanes per column pair, 32 / G pairs per warp: the pair's scalar work
+    // (three sums, the rotation's sqrt, division and rsqrt) is issued once
+    // per warp for 32 / G pairs.  Pairs are walked warp by warp so that the
+    // shuffles see the whole warp.
+    const int G = jacobi_group(c), gpw = 32 / G, sub = lane & (G - 1), gw = lane / G;
     const double tol = 2.220446049250313e-16 * (double)(c > 4 ? c : 4);
     int sweep = 0;
     for (; sweep < 60; ++sweep) {
         if (threadIdx.x == 0) s_rot = 0;
         __syncthreads();
         for (int round = 0; round < cp - 1; ++round) {
-            for (int pr = warp; pr < half; pr += nwarps) {
+            for (int base = warp * gpw; base < half; base += nwarps * gpw) {
+                const int pr = base + gw;
+                const bool valid = pr < half;
                 // round-robin: position 0 fixed, others rotate
-                int a_pos = pr, b_pos = cp - 1 - pr;
                 auto at = [&](int pos) { return pos == 0 ? 0 : 1 + (pos - 1 + round) % (cp - 1); };
-                int p = at(a_pos), q = at(b_pos);
-                if (p > q) { int t = p; p = q; q = t; }
-                double al = 0, be = 0, ga = 0;
-                for (int i = lane; i < c; i += 32) {
-                    const double x = W[p * c + i], y = W[q * c + i];
-                    al = fma(x, x, al);
-                    be = fma(y, y, be);
-                    ga = fma(x, y, ga);
+                int p = 0, q = 0;
+                if (valid) {
+                    p = at(pr);
+                    q = at(cp - 1 - pr);
+                    if (p > q) { int t = p; p = q; q = t; }
                 }
-                al = warp_sum(al);
-                be = warp_sum(be);
-                ga = warp_sum(ga);
+                double al = 0, be = 0, ga = 0;
+                if (valid)
+                    for (int i = sub; i < c; i += G) {
+                        const double x = W[p * c + i], y = W[q * c + i];
+                        al = fma(x, x, al);
+                        be = fma(y, y, be);
+                        ga = fma(x, y, ga);
+                    }
+                for (int o = G >> 1; o > 0; o >>= 1) {
+                    al += __shfl_xor_sync(0xffffffffu, al, o);
+                    be += __shfl_xor_sync(0xffffffffu, be, o);
+                    ga += __shfl_xor_sync(0xffffffffu, ga, o);
+                }
                 // |ga| > tol sqrt(al be), compared in squares.  The rotation of the
                 // usual zeta = (be - al) / (2 ga), t = sign(zeta) / (|zeta| +
                 // sqrt(1 + zeta^2)), cs = 1 / sqrt(1 + t^2), with numerator and
                 // denominator of t scaled by |2 ga|: one sqrt, one division, one
                 // reciprocal square root on the dependent path.
-                if (ga != 0.0 && ga * ga > (tol * tol) * (al * be)) {
+                if (valid && ga != 0.0 && ga * ga > (tol * tol) * (al * be)) {
                     const double d = be - al, g2 = 2.0 * ga;
                     const bool pos = (d >= 0.0) == (ga > 0.0) || d == 0.0;  // sign(zeta) >= 0
                     const double t = (pos ? fabs(g2) : -fabs(g2)) / (fabs(d) + sqrt(fma(d, d, g2 * g2)));
                     const double cs = rsqrt(fma(t, t, 1.0)), sn = cs * t;
-                    for (int i = lane; i < c; i += 32) {
+                    for (int i = sub; i < c; i += G) {
                         const double x = W[p * c + i], y = W[q * c + i];
                         W[p * c + i] = cs * x - sn * y;
                         W[q * c + i] = sn * x + cs * y;
                     }
-                    for (int i = lane; i < cp; i += 32) {
+                    for (int i = sub; i < cp; i += G) {
                         const double x = Vs[p * cp + i], y = Vs[q * cp + i];
                         Vs[p * cp + i] = cs * x - sn * y;
                         Vs[q * cp + i] = sn * x + cs * y;
                     }
-                    if (lane == 0) s_rot = 1;
+                    if (sub == 0) s_rot = 1;
                 }
             }
             __syncthreads();

@@ -632,7 +632,7 @@ void randomized(const svdb_matrix* A, uint64_t target_rank, uint64_t n_oversampl
             cholesky_qr(cx, Bt.p, n, c, R.p);
             DevBuf<double> Rt((size_t)r * r, s);
             transpose_dense<double>(R.p, Rt.p, r, r, s);
-            k_jacobi_svd<<<1, 1024, smem, s>>>(Rt.p, r, Vr.p, Ur.p, sig.p, jac_status.p);
+            k_jacobi_svd<<<1, jacobi_threads(r, 1024), smem, s>>>(Rt.p, r, Vr.p, Ur.p, sig.p, jac_status.p);
             // U_B = V_J (c x r); V_B = Q_b U_J (n x r)
             SVDB_CUDA(cudaMemcpyAsync(UB.p, Vr.p, (size_t)r * r * 8, cudaMemcpyDeviceToDevice, s));
             DevBuf<double> VB((size_t)n * r, s);
@@ -645,7 +645,7 @@ void randomized(const svdb_matrix* A, uint64_t target_rank, uint64_t n_oversampl
             cholesky_qr(cx, B.p, c, (int)n, R.p);
             DevBuf<double> Rt((size_t)r * r, s);
             transpose_dense<double>(R.p, Rt.p, r, r, s);
-            k_jacobi_svd<<<1, 1024, smem, s>>>(Rt.p, r, Vr.p, Ur.p, sig.p, jac_status.p);
+            k_jacobi_svd<<<1, jacobi_threads(r, 1024), smem, s>>>(Rt.p, r, Vr.p, Ur.p, sig.p, jac_status.p);
             right_mul(B.p, c, (int)n, Ur.p, r, r, UB.p, s);
             transpose_dense<double>(Vr.p, VtB.p, r, r, s);
         }
