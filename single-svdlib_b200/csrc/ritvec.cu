@@ -275,36 +275,6 @@ static int nblk(int64_t work, int threads) {
     return (int)std::max<int64_t>(1, std::min<int64_t>(b, (int64_t)device_props().sms * 16));
 }
 
-void rot_pack(const int32_t* ri, const double* rc, const double* rs, int64_t nrot, int64_t js, double* cs,
-              int32_t* il) {
-    const int64_t npad = rot_padded(nrot);
-    std::fill(cs, cs + 2 * npad, 0.0);
-    std::fill(il, il + 2 * npad, 0);
-    int64_t start = 0;
-    for (int64_t t = 0; t <= nrot; ++t) {
-        if (t < nrot) {
-            if (ri[t] < 0 || ri[t] > js - 2)
-                throw Error(SVDB_ERR_LAS2, "rotation " + std::to_string(t) + " has index " + std::to_string(ri[t]) +
-                                               " outside [0, " + std::to_string(js - 2) + "]");
-            cs[2 * t] = rc[t];
-            cs[2 * t + 1] = rs[t];
-            il[2 * t] = ri[t];
-        }
-        const bool cut = t == nrot || (t > start && (t % kRotChunk == 0 || ri[t] != ri[t - 1] - 1));
-        if (cut) {
-            il[2 * start + 1] = (int32_t)(t - start);
-            start = t;
-        }
-    }
-}
-
-void rot_pack(const int32_t* ri, const double* rc, const double* rs, int64_t nrot, int64_t js,
-              std::vector<double>& cs, std::vector<int32_t>& il) {
-    cs.resize((size_t)(2 * rot_padded(nrot)));
-    il.resize((size_t)(2 * rot_padded(nrot)));
-    rot_pack(ri, rc, rs, nrot, js, cs.data(), il.data());
-}
-
 template <int ROWS>
 static void launch_rot_smem(double* z, int64_t js, const double2* cs, const int2* il, int64_t nrot, int first,
                             cudaStream_t s) {
