@@ -112,7 +112,7 @@ __device__ __forceinline__ bool lz_sum(double v, double* part, GridBarrier* bar,
 }
 
 template <bool FP32, bool CL>
-__global__ void __launch_bounds__(kThreads, 2) k_lanczos_block(const __grid_constant__ LzArgs a) {
+__global__ void __launch_bounds__(kThreads, CL ? 1 : 2) k_lanczos_block(const __grid_constant__ LzArgs a) {
     __shared__ double sh[32];
     __shared__ double cl_slot[2], cl_out;
     int par = 0;
