@@ -181,12 +181,12 @@ def peak_hbm():
         return 6650.0, "fallback"
 
 
-def profiled_traffic(name):
-    """Bytes per launch from a committed ncu summary line 'traffic_bytes_per_launch: <n>'."""
+def profiled_traffic(name, key="traffic_bytes_per_launch"):
+    """DRAM bytes from a committed ncu summary line '<key>: <n>' (per launch, or per Lanczos step)."""
     path = os.path.join(ROOT, "profiles", name)
     try:
         for line in open(path):
-            if line.startswith("traffic_bytes_per_launch:"):
+            if line.startswith(key + ":"):
                 return float(line.split(":", 1)[1])
     except OSError:
         pass
@@ -425,7 +425,9 @@ def run_las2(args):
               sigma_rel_err_vs_oracle=sigma_err_oracle, phases=phases,
               lanczos_as_written={"status": asw_status, "seconds": ms_asw / 1e3},
               roofline={"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                        "traffic": None, "kernel": "k_lanczos_block (per step: A x and A^T x)",
+                        "traffic": profiled_traffic("lanczos_block_las2_5000x2000.md", "traffic_bytes_per_step"),
+                        "traffic_unit": "DRAM bytes per Lanczos step (ncu)",
+                        "kernel": "k_lanczos_block (per step: A x and A^T x)",
                         "peak_source": peak_kind, "us_per_lanczos_step": per_step_us, "spmv_standalone": spmv},
               cpu_baseline=cpu,
               e2e={"value": e2e_s, "unit": "s", "h2d_bytes_per_step": 8 * (m + 1) + 16 * nnz,
