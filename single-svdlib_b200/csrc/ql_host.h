@@ -155,7 +155,7 @@ static inline void imtqlb_legacy(size_t n, double* d, double* e, double* bnd, Ro
                         rec->i.push_back((int32_t)i);
                         rec->c.push_back(c);
                         rec->s.push_back(s);
-                        if (flush && rec->i.size() % every == 0) (*flush)(rec->i.size());
+                        if (flush && every && rec->i.size() % every == 0) (*flush)(rec->i.size());
                     }
                     if (i == 0) break;
                     --i;
