@@ -11,8 +11,12 @@ per solve with the matrix resident in HBM (CUDA events, max over ranks);
 `e2e` is the same through the public API from pinned host buffers (matrix
 upload and result download inside the timed region).  Several GPUs run
 independent replicas (weak scaling).  `--impl reference` times the CPU
-restatement of the crate's path (oracle/, all host threads) on a row sample
-of the same workload and scales it to the full matrix.
+restatement of the crate's path (oracle/, all host threads) on the whole
+workload every step.  Both arms draw the same Omega: the library's seeded
+stream, restated on the host for the CPU solve.  The line also carries sigma
+against that CPU solve and, under `las2_1Mx200k`, the SpMV half of the metric
+(standalone A x / A^T x GB/s in FP32 and FP64 values on the 1M x 200k LAS2
+matrix, and one mixed and one f64 LAS2 solve of it).
 
 Other workloads (--workload), one JSON line each with the same keys:
   las2        LAS2 f64 on the 5,000 x 2,000 Poisson(20) CSR, dimensions 10,
@@ -52,6 +56,7 @@ for p in (os.path.join(ROOT, "single-svdlib_b200"), os.path.join(ROOT, "oracle")
 M_ROWS, N_COLS = 100_000, 30_000
 TARGET_RANK, OVERSAMPLES, POWER_ITERS, SEED = 50, 10, 3, 7
 GEN_SEED = 2024
+METRIC = "time-to-k-triplets (s), randomized_svd k=50"
 WORKLOAD = ("randomized_svd 100000x30000 count-like CSR (lambda_j~Gamma(0.5,2), row nnz~LogNormal(ln600,0.5), "
             "values log1p(Poisson(lambda_j)+1)), rank 50 + 10 oversamples, 3 power iterations, QR, seed 7, "
             "MaskedCSRMatrix all columns")
@@ -59,26 +64,9 @@ WORKLOAD = ("randomized_svd 100000x30000 count-like CSR (lambda_j~Gamma(0.5,2), 
 
 # ------------------------------------------------------------------ data --
 def generate(m=M_ROWS, n=N_COLS, seed=GEN_SEED):
-    """Seeded synthetic count-like CSR.  Columns are drawn proportional to
-    lambda_j with replacement and merged per row (realised nnz is reported)."""
-    rng = np.random.default_rng(seed)
-    lam = rng.gamma(0.5, 2.0, n)
-    k = np.clip(np.rint(rng.lognormal(np.log(600.0), 0.5, m)), 1, n).astype(np.int64)
-    cdf = np.cumsum(lam / lam.sum())
-    cdf[-1] = 1.0
-    rows = np.repeat(np.arange(m, dtype=np.int64), k)
-    cols = np.searchsorted(cdf, rng.random(rows.size), side="right").astype(np.int64)
-    np.minimum(cols, n - 1, out=cols)
-    keys = rows * n + cols
-    keys.sort()
-    keep = np.ones(keys.size, dtype=bool)
-    keep[1:] = keys[1:] != keys[:-1]
-    rows, cols = np.divmod(keys[keep], n)
-    del keys, keep
-    indptr = np.zeros(m + 1, np.int64)
-    np.cumsum(np.bincount(rows, minlength=m), out=indptr[1:])
-    vals = np.log1p(rng.poisson(lam[cols]) + 1.0)
-    return indptr, cols, vals
+    """The seeded count-like CSR of the workload (tests/matrices.py)."""
+    import matrices as Mx
+    return Mx.count_like(m, n, seed)
 
 
 def stage(msg):
@@ -205,23 +193,22 @@ def max_over_ranks(x, world):
     return float(t.item())
 
 
-def cpu_reference(indptr, cols, vals, threads, sample_rows, omega):
-    """The CPU restatement of randomized_svd (oracle/) on the first `sample_rows` rows.
-
-    Returns (estimated seconds for the full matrix, measured seconds, sample nnz): the
-    sparse-product time is scaled by the nnz ratio, the m-row dense work (QR of Y,
-    U = Q U_B) by the row ratio, and the n-row / small-SVD work is taken as measured."""
+def cpu_reference(indptr, cols, vals, threads, omega):
+    """One randomized_svd of the whole matrix on the CPU restatement (oracle/,
+    OpenMP over the crate's Rayon loops).  Returns (seconds, sigma)."""
     import oracle as O
     O.set_threads(threads)
-    nnz_s = int(indptr[sample_rows])
-    A = {"nrows": sample_rows, "ncols": N_COLS, "indptr": indptr[: sample_rows + 1], "indices": cols[:nnz_s],
-         "data": vals[:nnz_s]}
+    A = {"nrows": len(indptr) - 1, "ncols": N_COLS, "indptr": indptr, "indices": cols, "data": vals}
     t0 = time.perf_counter()
     r = O.randomized(A, TARGET_RANK, OVERSAMPLES, POWER_ITERS, "QR", omega=omega)
-    measured = time.perf_counter() - t0
-    t = r["times"]
-    full = t["sparse"] * (len(vals) / nnz_s) + t["rows"] * (M_ROWS / sample_rows) + t["fixed"]
-    return full, measured, nnz_s
+    return time.perf_counter() - t0, r["s"]
+
+
+def shared_omega():
+    """The Omega both arms use: the library's seeded stream for SEED, restated
+    on the host (the device draws the same matrix from the seed)."""
+    import oracle as O
+    return O.omega_stream(SEED, N_COLS, TARGET_RANK + OVERSAMPLES)
 
 
 # ------------------------------------------------------- other workloads --
@@ -444,36 +431,54 @@ LARGE_WORKLOAD = ("LAS2 1000000x200000 CSR, row lengths Zipf(1.85) on [20,20000]
 
 
 def gen_large(torch, m, n, seed=3):
-    """Seeded 1M x 200k CSR on the device (torch CUDA generator): int64 indptr, int32 columns, f64 values."""
-    rng = np.random.default_rng(seed)
-    ks = np.arange(20, 20001)
-    p = ks.astype(np.float64) ** -1.85
-    p /= p.sum()
-    rowlen = torch.from_numpy(rng.choice(ks, size=m, p=p)).cuda()
-    g = torch.Generator(device="cuda")
-    g.manual_seed(seed)
-    nnz0 = int(rowlen.sum())
-    keys = torch.repeat_interleave(torch.arange(m, device="cuda", dtype=torch.int64), rowlen) * n
-    keys += torch.randint(0, n, (nnz0,), device="cuda", generator=g, dtype=torch.int64)
-    keys = torch.unique_consecutive(torch.sort(keys).values)
-    rows = keys // n
-    cols = (keys - rows * n).to(torch.int32)
-    del keys
-    nnz = rows.numel()
-    indptr = torch.zeros(m + 1, dtype=torch.int64, device="cuda")
-    indptr[1:] = torch.cumsum(torch.bincount(rows, minlength=m), 0)
-    vals = torch.randn(nnz, dtype=torch.float64, device="cuda", generator=g)
-    r = 20
-    u = torch.randn(m, r, dtype=torch.float64, device="cuda", generator=g)
-    v = torch.randn(n, r, dtype=torch.float64, device="cuda", generator=g)
-    u /= u.norm(dim=0)
-    v /= v.norm(dim=0)
-    sig = torch.logspace(2, 0, r, dtype=torch.float64, device="cuda") * (m * n / nnz)
-    for c0 in range(0, nnz, 1 << 23):
-        c1 = min(nnz, c0 + (1 << 23))
-        vals[c0:c1] += (u[rows[c0:c1]] * v[cols[c0:c1].long()] * sig).sum(1)
-    del rows, u, v
-    return indptr, cols, vals
+    """The seeded 1M x 200k LAS2 matrix, generated on the device (tests/matrices.py)."""
+    import matrices as Mx
+    return Mx.zipf_planted_device(torch, m, n, seed)
+
+
+def las2_large_leg(torch, L, args, stream):
+    """The SpMV half of the metric on the 1M x 200k LAS2 matrix: standalone
+    A x and A^T x in FP32 and FP64 values (algorithmic GB/s), and one LAS2
+    solve (dimensions 100, SVDLIBC semantics) of each precision, timed with
+    CUDA events including the host copy of the results."""
+    from single_svdlib import _abi
+    from single_svdlib._core import check, options, rec_from_c
+    m, n = int(LARGE_M * args.scale), int(LARGE_N * args.scale)
+    indptr, cols, vals = gen_large(torch, m, n)
+    nnz = vals.numel()
+    h = C.c_void_p()
+    check(L.svdb_matrix_create_csr_device(m, n, nnz, indptr.data_ptr(), cols.data_ptr(), vals.data_ptr(),
+                                          C.byref(h)))
+    del indptr, cols, vals
+    try:
+        spmv = {"fp32_values": _spmv_gbs(torch, L, check, h, m, n, nnz, 1, stream),
+                "fp64_values": _spmv_gbs(torch, L, check, h, m, n, nnz, 0, stream)}
+        peak, peak_kind = peak_hbm()
+        for d in spmv.values():
+            for v in d.values():
+                v["frac_of_peak"] = v["gbs"] / peak
+        st, r = _las2_call(L, C, check, _abi, options, h, LARGE_DIMS, 0, 42, True, "mixed", 1, stream)
+        check(st)
+        L.svdb_rec_free(C.byref(r))
+        res = {}
+        for prec in ("mixed", "f64"):
+            ms, recs = _timed(torch, stream, 1, lambda: _las2_call(L, C, check, _abi, options, h, LARGE_DIMS, 0, 42,
+                                                                   True, prec, 0, stream), 1)
+            st, r = recs[0]
+            check(st)
+            rec = rec_from_c(r)
+            L.svdb_rec_free(C.byref(r))
+            res[prec] = (ms / 1e3, rec.s, rec.diagnostics.lanczos_steps)
+        k = min(len(res["f64"][1]), len(res["mixed"][1]))
+        err = float(np.max(np.abs(res["mixed"][1][:k] - res["f64"][1][:k]) / np.abs(res["f64"][1][:k]))) if k else None
+        return {"workload": LARGE_WORKLOAD, "nrows": m, "ncols": n, "nnz": nnz, "peak_gbs": peak,
+                "peak_source": peak_kind, "spmv": spmv,
+                "las2_mixed_s": res["mixed"][0], "las2_f64_s": res["f64"][0],
+                "mixed_speedup_vs_f64": res["f64"][0] / res["mixed"][0], "sigma_rel_err_mixed_vs_f64": err,
+                "lanczos_steps": {"mixed": res["mixed"][2], "f64": res["f64"][2]},
+                "timing": "CUDA events around one solve each (host results included), after one warm-up solve"}
+    finally:
+        L.svdb_matrix_destroy(h)
 
 
 def run_las2_large(args):
@@ -853,6 +858,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-sample-rows", type=int, default=20000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-large", action="store_true", help="randomized: skip the 1M x 200k SpMV / LAS2 leg")
     ap.add_argument("--scale", type=float, default=1.0, help="shrink both dimensions (smoke runs only)")
     ap.add_argument("--workload", default="randomized",
                     choices=["randomized", "las2", "las2-large", "adjoint", "batch"])
@@ -876,19 +882,18 @@ def main():
             return 0
         indptr, cols, vals = load_or_generate(0, 1)
         nnz = len(vals)
-        om = np.random.default_rng(SEED).standard_normal((N_COLS, TARGET_RANK + OVERSAMPLES))
+        om = shared_omega()
         for _ in range(args.warmup):
-            cpu_reference(indptr, cols, vals, threads, min(1000, args.cpu_sample_rows), om)
+            cpu_reference(indptr, cols, vals, threads, om)
         times = []
         for _ in range(args.steps):
-            t, measured, nnz_s = cpu_reference(indptr, cols, vals, threads, args.cpu_sample_rows, om)
+            t, _s = cpu_reference(indptr, cols, vals, threads, om)
             times.append(t)
         v = statistics.mean(times)
-        sample = (f"first {args.cpu_sample_rows} of {M_ROWS} rows ({nnz_s} of {nnz} nnz), full randomized_svd on "
-                  f"the CPU restatement ({measured:.1f} s measured); sparse-product time scaled by nnz, m-row "
-                  f"dense work by rows")
+        sample = (f"the whole workload every step ({M_ROWS}x{N_COLS}, {nnz} nnz): randomized_svd restated in C++ "
+                  f"(OpenMP over the crate's Rayon loops), Omega = the library's seeded stream for seed {SEED}")
         print(json.dumps({
-            "impl": "reference", "metric": "time-to-k-triplets (s), randomized_svd k=50", "value": v, "unit": "s",
+            "impl": "reference", "metric": METRIC, "value": v, "unit": "s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3,
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": {"workload": WORKLOAD, "nnz": nnz},
@@ -1036,19 +1041,25 @@ def main():
     ms_f64 = max_over_ranks(ms_f64, world)
     e2e_s = max_over_ranks(e2e_s, world)
 
-    cpu = None
+    cpu, sig_oracle = None, None
     if rank == 0 and not args.no_cpu_baseline:
-        stage("cpu baseline")
-        om = np.random.default_rng(SEED).standard_normal((n, l))
-        t, measured, nnz_s = cpu_reference(indptr, cols, vals, threads, args.cpu_sample_rows, om)
+        stage("cpu baseline + oracle parity")
+        t, s_ref = cpu_reference(indptr, cols, vals, threads, shared_omega())
         cpu = {"value": t, "unit": "s", "cores": threads, "kind": "port",
-               "sample": f"first {args.cpu_sample_rows} of {m} rows ({nnz_s} of {nnz} nnz), full randomized_svd "
-                         f"on the CPU restatement ({measured:.1f} s measured); sparse-product time scaled by nnz, "
-                         f"m-row dense work by rows"}
+               "sample": f"the whole workload, one solve ({m}x{n}, {nnz} nnz): randomized_svd restated in C++ "
+                         f"(OpenMP over the crate's Rayon loops), Omega = the library's seeded stream for seed {SEED}"}
+        sig_oracle = {p_: float(np.max(np.abs(sig[p_] - s_ref) / np.abs(s_ref))) for p_ in ("f64", "mixed")}
+    del indptr, cols, vals, h_indptr, h_cols, h_vals
+    L.svdb_matrix_destroy(masked)
+    L.svdb_matrix_destroy(parent)
+    large = None
+    if not args.no_large:
+        stage("1M x 200k SpMV / LAS2 leg")
+        large = las2_large_leg(torch, L, args, stream)
 
     if rank == 0:
         line = {
-            "metric": "time-to-k-triplets (s), randomized_svd k=50, FP32 GPU (sigma rel err vs f64 stated)",
+            "metric": METRIC,
             "value": ms_mixed / 1e3, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_mixed, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
@@ -1058,6 +1069,7 @@ def main():
                        "l2": "inputs larger than L2 (FP32 CSR + CSC ~ %.0f MB)" % (nnz * 16 / 1e6)},
             "f64_value": ms_f64 / 1e3, "mixed_speedup_vs_f64": ms_f64 / ms_mixed,
             "sigma_rel_err_vs_f64": sigma_err,
+            "sigma_rel_err_vs_oracle": sig_oracle,
             "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                          "traffic": profiled_traffic("spmm_randomized_100kx30k.md"), "kernel": dominant,
                          "peak_source": peak_kind,
@@ -1067,11 +1079,10 @@ def main():
             "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": int(launches),
             "clocks": clocks,
+            "las2_1Mx200k": large,
         }
         print(json.dumps(line), flush=True)
     stage("teardown")
-    L.svdb_matrix_destroy(masked)
-    L.svdb_matrix_destroy(parent)
     if world > 1:
         torch.distributed.destroy_process_group()
     stage("done")

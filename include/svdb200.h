@@ -252,11 +252,13 @@ int svdb_multiply_with_dense_device(const svdb_matrix* a, const void* d_dense, u
  * allocate device memory where they apply the operator (their own allocator
  * holds the GPU's memory, or an allocation's synchronisation is not
  * acceptable there).  The intermediate vector lives in a fixed 2^20-double
- * (8 MiB) device array that every GPU loading the library keeps until exit;
- * a larger intermediate (rows of A, or columns when transposed) returns
- * SVDB_ERR_UNSUPPORTED.  The array's address is looked up on the first call on
- * each device, so make that call before any stream capture.  All calls share
- * the array: calls that overlap on the GPU race and must be serialised. */
+ * (8 MiB) device array.  It is placed in a GPU's memory, and its address looked
+ * up, when the first matrix handle is created on that GPU (an allocating call),
+ * and it stays there until exit; this call itself loads and allocates nothing.
+ * The handle's device must be the current device (SVDB_ERR_ARG otherwise).
+ * A larger intermediate (rows of A, or columns when transposed) returns
+ * SVDB_ERR_UNSUPPORTED.  All calls share the array: calls that overlap on the
+ * GPU race and must be serialised. */
 int svdb_opb_device_noalloc(const svdb_matrix* a, const double* d_x, double* d_y, int transposed, void* stream);
 
 /* svd_opa on device buffers: d_y = A d_x, or A^T d_x when transposed (double
@@ -280,6 +282,16 @@ int svdb_gram_device(const double* d_x, uint64_t rows, uint64_t c, double* d_g, 
  * both caches (of the current device) to the driver, after a device
  * synchronisation. */
 int svdb_release_cached_memory(void);
+
+/* Self-test of the bounded device waits, with no counterpart in the
+ * reference: makes one wait run out on purpose -- which = 0 the grid barrier
+ * of the cooperative Lanczos block (a one-block grid that expects a second
+ * arrival), which = 1 the mbarrier wait of the tensor-core Gram (a barrier
+ * nothing arrives on) -- with a limit of limit_ns (1 .. 2e9).  Returns
+ * SVDB_ERR_TIMEOUT when the wait gave up as designed; the context stays
+ * usable.  The limit of the real waits (2 s) can be lowered for a process with
+ * the environment variable SVDB_WAIT_LIMIT_NS, read at each launch. */
+int svdb_wait_selftest(int which, uint64_t limit_ns);
 
 /* Number of kernels this library has launched in the process so far. */
 uint64_t svdb_kernel_launches(void);

@@ -273,6 +273,34 @@ def randomized(A, target_rank, n_oversamples, n_power_iters, normalizer="QR", om
 
 
 # --------------------------------------------------------- numpy checkers ----
+def _splitmix64(x):
+    """splitmix64 finaliser (Steele, Lea and Flood 2014) on uint64 arrays, wrapping."""
+    with np.errstate(over="ignore"):
+        x = x + np.uint64(0x9E3779B97F4A7C15)
+        x = (x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        x = (x ^ (x >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        return x ^ (x >> np.uint64(31))
+
+
+def omega_stream(seed, n, l):
+    """The library's seeded Omega (n x l, row-major), restated in numpy so that
+    the checker and the CUDA solve draw the same matrix from the same seed.
+
+    Entry i: two uniforms from splitmix64 of (key + 2i, key + 2i + 1) with
+    key = splitmix64(seed ^ 0x5DEECE66D), then Box-Muller.  The crate itself
+    draws Omega with rand_distr's Normal (src/randomized/mod.rs:299-313), whose
+    stream is not restated here.  Values agree with the device's to a few ulps
+    (the device evaluates cos(pi * 2u) with cospi)."""
+    key = _splitmix64(np.array([np.uint64(seed) ^ np.uint64(0x5DEECE66D)], dtype=np.uint64))[0]
+    i = np.arange(n * l, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        a = _splitmix64(key + np.uint64(2) * i)
+        b = _splitmix64(key + np.uint64(2) * i + np.uint64(1))
+    u1 = ((a >> np.uint64(11)).astype(np.float64) + 0.5) * (1.0 / 9007199254740992.0)
+    u2 = (b >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+    return (np.sqrt(-2.0 * np.log(u1)) * np.cos(np.pi * (2.0 * u2))).reshape(n, l)
+
+
 def svd_flip(u=None, v=None, u_based_decision=True):
     """svd_flip (src/randomized/mod.rs:332-438), restated in numpy on copies.
 

@@ -15,17 +15,18 @@ __device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(
 
 // ------------------------------------------------------------------------
 // Grid barrier for cooperative launches.  Every spin is bounded: after
-// ~kBarrierTimeoutNs of waiting the block records SVDB_ERR_TIMEOUT in *err
-// and leaves the barrier; all blocks then return at their next check.
+// limit_ns of waiting (the host writes it with the zeroed counters before
+// each launch: 2 s unless SVDB_WAIT_LIMIT_NS says otherwise) the block
+// records SVDB_ERR_TIMEOUT in err and leaves the barrier; all blocks then
+// return at their next check.
 // ------------------------------------------------------------------------
 struct GridBarrier {
     unsigned int count;
     unsigned int gen;
     int err;
     int pad;
+    unsigned long long limit_ns;
 };
-
-constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;  // 2 s
 
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
@@ -33,8 +34,24 @@ __device__ __forceinline__ unsigned long long global_ns() {
     return t;
 }
 
+// Waits for phase `parity` of the shared-memory mbarrier at shared address
+// `bar` to complete; gives up after limit_ns of %globaltimer (false).
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity, unsigned long long limit_ns) {
+    uint32_t ok = 0;
+    const unsigned long long t0 = global_ns();
+    while (true) {
+        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+                     : "=r"(ok)
+                     : "r"(bar), "r"(parity)
+                     : "memory");
+        if (ok) return true;
+        if (global_ns() - t0 > limit_ns) return false;
+    }
+}
+
 // Returns false (uniformly within the block) when the barrier failed.
-__device__ __forceinline__ bool grid_sync(GridBarrier* bar) {
+// `expected` is the number of blocks that must arrive (0: the whole grid).
+__device__ __forceinline__ bool grid_sync(GridBarrier* bar, unsigned int expected = 0) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -44,8 +61,9 @@ __device__ __forceinline__ bool grid_sync(GridBarrier* bar) {
         unsigned int g = gen.load(cuda::memory_order_relaxed);
         __threadfence();
         unsigned int arrived = cnt.fetch_add(1u, cuda::memory_order_acq_rel);
+        const unsigned long long limit = bar->limit_ns;
         int ok = 1;
-        if (arrived == gridDim.x - 1) {
+        if (arrived == (expected ? expected : gridDim.x) - 1) {
             cnt.store(0u, cuda::memory_order_relaxed);
             gen.fetch_add(1u, cuda::memory_order_release);
         } else {
@@ -53,7 +71,7 @@ __device__ __forceinline__ bool grid_sync(GridBarrier* bar) {
             unsigned int spins = 0;
             while (gen.load(cuda::memory_order_acquire) == g) {
                 if (err.load(cuda::memory_order_relaxed) != 0) { ok = 0; break; }
-                if ((++spins & 255u) == 0 && global_ns() - t0 > kBarrierTimeoutNs) {
+                if ((++spins & 255u) == 0 && global_ns() - t0 > limit) {
                     err.store(8 /* SVDB_ERR_TIMEOUT */, cuda::memory_order_relaxed);
                     ok = 0;
                     break;

@@ -40,11 +40,6 @@ constexpr uint32_t kGtIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((64u >> 3) <
 __device__ int g_gram_tc_err;
 
 __device__ __forceinline__ uint32_t gt_smem(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ uint64_t gt_timer() {
-    uint64_t t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
 // shared-memory matrix descriptor: K-major, no swizzle, LBO 128 B, SBO 1024 B
 __device__ __forceinline__ uint64_t gt_desc(uint32_t saddr) {
     return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(1024 >> 4) << 32) |
@@ -55,16 +50,7 @@ __device__ __forceinline__ int gt_off(int row, int k) {
     return (row >> 3) * 1024 + (k >> 2) * 128 + (row & 7) * 16 + (k & 3) * 4;
 }
 __device__ __forceinline__ bool gt_wait(uint32_t bar, uint32_t parity, uint64_t limit_ns) {
-    uint32_t ok = 0;
-    const uint64_t t0 = gt_timer();
-    while (true) {
-        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-                     : "=r"(ok)
-                     : "r"(bar), "r"(parity)
-                     : "memory");
-        if (ok) return true;
-        if (gt_timer() - t0 > limit_ns) return false;
-    }
+    return mbar_wait_bounded(bar, parity, limit_ns);
 }
 
 #define SVDB_LD32(v, taddr)                                                                                        \
@@ -80,7 +66,7 @@ __device__ __forceinline__ bool gt_wait(uint32_t bar, uint32_t parity, uint64_t 
 
 __global__ void __launch_bounds__(kGtThreads) k_gram_tc(const double* __restrict__ X, int64_t rows, int c,
                                                         int64_t chunk, double* __restrict__ part,
-                                                        const int* __restrict__ cond) {
+                                                        const int* __restrict__ cond, uint64_t limit_ns) {
     if (cond && *cond == 0) return;
     extern __shared__ __align__(1024) unsigned char sm[];
     float* xch = reinterpret_cast<float*>(sm + 2 * kGtTileBytes);  // 64 x 64: rows 64..127 of D
@@ -124,7 +110,7 @@ __global__ void __launch_bounds__(kGtThreads) k_gram_tc(const double* __restrict
             xv[u] = (k < nk && col < c) ? X[(kb + k) * c + col] : 0.0;
         }
         if (st >= 2) {
-            if (tid == 0 && !gt_wait(gt_smem(&s_bar[buf]), (uses[buf] - 1) & 1, 2000000000ull)) s_failed = 1;
+            if (tid == 0 && !gt_wait(gt_smem(&s_bar[buf]), (uses[buf] - 1) & 1, limit_ns)) s_failed = 1;
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncthreads();
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -168,7 +154,7 @@ __global__ void __launch_bounds__(kGtThreads) k_gram_tc(const double* __restrict
     // the last commit covers every MMA issued before it
     if (tid == 0 && !s_failed && nstage > 0) {
         const int lb = (nstage - 1) & 1;
-        if (!gt_wait(gt_smem(&s_bar[lb]), (uses[lb] - 1) & 1, 2000000000ull)) s_failed = 1;
+        if (!gt_wait(gt_smem(&s_bar[lb]), (uses[lb] - 1) & 1, limit_ns)) s_failed = 1;
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -205,8 +191,8 @@ __global__ void __launch_bounds__(kGtThreads) k_gram_tc(const double* __restrict
     }
     if (s_failed && tid == 0) {
         atomicOr(&g_gram_tc_err, 1);
-        for (int bq = 0; bq < 2; ++bq)  // give the MMAs in flight a last chance to land
-            if (uses[bq]) gt_wait(gt_smem(&s_bar[bq]), (uses[bq] - 1) & 1, 100000000ull);
+        for (int bq = 0; bq < 2; ++bq)  // the MMAs in flight must land before TMEM is freed (2 s at most)
+            if (uses[bq]) gt_wait(gt_smem(&s_bar[bq]), (uses[bq] - 1) & 1, 2000000000ull);
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -230,7 +216,7 @@ int gram_tc_launch(const double* X, int64_t rows, int c, double* part, int64_t p
         SVDB_CUDA(cudaFuncSetAttribute(k_gram_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kGtSmem));
         attr = true;
     }
-    k_gram_tc<<<nblk, kGtThreads, kGtSmem, s>>>(X, rows, c, chunk, part, cond);
+    k_gram_tc<<<nblk, kGtThreads, kGtSmem, s>>>(X, rows, c, chunk, part, cond, wait_limit_ns());
     SVDB_CHECK_LAUNCH();
     return nblk;
 }
@@ -244,7 +230,7 @@ void gram_tc_check() {
         const int z = 0;
         SVDB_CUDA(cudaMemcpyToSymbol(g_gram_tc_err, &z, sizeof(int)));
         if (e & 2) throw Error(SVDB_ERR_CUDA, "tensor-core Gram: shared memory not 1 KB aligned; no MMA was issued");
-        throw Error(SVDB_ERR_TIMEOUT, "tensor-core Gram: an MMA commit did not arrive within 2 s");
+        throw Error(SVDB_ERR_TIMEOUT, "tensor-core Gram: an MMA commit did not arrive within the wait limit");
     }
 }
 

@@ -392,7 +392,10 @@ int64_t Las2Run::lanczos_step(int64_t first, int64_t last, int64_t& ll, bool& en
         hs.npurge = npurge_;
         hs.j = j;
         SVDB_CUDA(cudaMemcpyAsync(st_.p, &hs, sizeof hs, cudaMemcpyHostToDevice, s_));
-        SVDB_CUDA(cudaMemsetAsync(bar_.p, 0, sizeof(GridBarrier), s_));
+        GridBarrier b0;
+        std::memset(&b0, 0, sizeof b0);
+        b0.limit_ns = wait_limit_ns();
+        SVDB_CUDA(cudaMemcpyAsync(bar_.p, &b0, sizeof b0, cudaMemcpyHostToDevice, s_));
         LzArgs a;
         std::memset(&a, 0, sizeof a);
         a.op1 = {op1_->ptr.p, op1_->idx.p, op1_->val.p, fp32_ ? op1_->val32.p : nullptr, op1_->nmajor,

@@ -14,6 +14,13 @@
 
 namespace svdb {
 
+uint64_t wait_limit_ns() {
+    const char* e = getenv("SVDB_WAIT_LIMIT_NS");
+    if (!e || !*e) return 2000000000ull;
+    const unsigned long long v = strtoull(e, nullptr, 10);
+    return v ? v : 1;
+}
+
 const DeviceProps& device_props() {
     static thread_local int cached_dev = -1;
     static thread_local DeviceProps props;
@@ -322,6 +329,7 @@ void release_cached_memory() {
 }
 
 static svdb_matrix* new_handle() {
+    noalloc_reserve();  // svdb_opb_device_noalloc's scratch on the current device
     svdb_matrix* a = new svdb_matrix();
     SVDB_CUDA(cudaGetDevice(&a->device));
     keep_pool_cached(a->device);

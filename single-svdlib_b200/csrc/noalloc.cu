@@ -8,12 +8,17 @@
 // acceptable.  They pass x and y in their own device memory; the intermediate
 // vector A x lives in a fixed array compiled into this library.
 //
-// The array is a file-scope __device__ variable, so every GPU that loads the
-// library holds it (kScratchDoubles doubles = 8 MiB) until the process exits.
-// Host code may not use the variable's name as a device address; the address
-// is taken with cudaGetSymbolAddress once per device, on the first call made
-// on that device, with that device current.  That first call should therefore
-// come before any stream capture.
+// The array is a file-scope __device__ variable (kScratchDoubles doubles =
+// 8 MiB).  This file is its own CUDA module, and CUDA loads modules lazily by
+// default, so the array is placed in device memory when its address is first
+// taken.  Host code may not use the variable's name as a device address; the
+// address is taken with cudaGetSymbolAddress once per device, with that
+// device current, by noalloc_reserve(), which every matrix handle's creation
+// calls.  So the 8 MiB are reserved on a GPU when the first matrix handle is
+// created there (an allocating call anyway), and held until the process
+// exits; a call of svdb_opb_device_noalloc itself never loads or allocates
+// anything.  The handle's device must be current when it is called: the
+// scratch address is looked up for the current device.
 //
 // All calls share the one array: calls whose work overlaps on the GPU (on
 // different streams, or from different host threads) race on it and must be
@@ -48,6 +53,8 @@ static double* scratch_for_current_device() {
     }
     return static_cast<double*>(g_scratch_addr[dev]);
 }
+
+void noalloc_reserve() { (void)scratch_for_current_device(); }
 
 }  // namespace svdb
 

@@ -46,15 +46,20 @@ __global__ void __launch_bounds__(256) k_spmv(const int64_t* __restrict__ rp, co
     spmv_binned(rp, ci, v, bins, gwarp, nwarps, xl, [&](int64_t r, double acc) { y[r] = acc; });
 }
 
+// One resident wave of k_spmv<VT> on the current device.  The occupancy is
+// cached per thread and device, like device_props().
 template <typename VT>
 static int spmv_grid() {
-    static int per_sm[2] = {0, 0};
-    int& ps = per_sm[sizeof(VT) == 4];
-    if (!ps) {
-        SVDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ps, k_spmv<VT>, 256, 0));
-        if (ps < 1) ps = 1;
+    static thread_local int cached_dev = -1;
+    static thread_local int per_sm = 0;
+    int dev = 0;
+    SVDB_CUDA(cudaGetDevice(&dev));
+    if (dev != cached_dev) {
+        SVDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spmv<VT>, 256, 0));
+        if (per_sm < 1) per_sm = 1;
+        cached_dev = dev;
     }
-    return ps * device_props().sms;
+    return per_sm * device_props().sms;
 }
 
 void spmv(const DevCompressed& m, bool fp32, const double* x, double* y, cudaStream_t s) {

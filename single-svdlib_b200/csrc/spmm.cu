@@ -503,11 +503,6 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 // TMA path (opt-in, SVDB_SPMM=tma): FP32 operand with contiguous rows of l
 // (a multiple of 4, at most 64) on a 16-byte aligned base.  On B200 it moved
 // about 4.9 TB/s of 256-byte rows against 7.4 TB/s for the register gathers
-// of k_spmm_seg (100,000 x 30,000, 65 M nonzeros, l = 60), so it is not the
-// default; the variable is read on every call.
-// TMA path (opt-in, SVDB_SPMM=tma): FP32 operand with contiguous rows of l
-// (a multiple of 4, at most 64) on a 16-byte aligned base.  On B200 it moved
-// about 4.9 TB/s of 256-byte rows against 7.4 TB/s for the register gathers
 // of k_spmm_seg (100,000 x 30,000, 65 M nonzeros, l = 60), and splitting the
 // segments between the two kernels on two streams was no faster than
 // k_spmm_seg alone: both are held by the same L2 gather traffic.  So it is

@@ -174,6 +174,14 @@ struct DeviceProps {
     size_t smem_optin = 0;  // dynamic shared memory a block may opt into (less 1 KB for static use)
 };
 const DeviceProps& device_props();
+// Looks up (once per device) the address of svdb_opb_device_noalloc's
+// scratch array on the current device, which places the array in device
+// memory; called by every matrix handle's creation (csrc/noalloc.cu).
+void noalloc_reserve();
+// Limit of the bounded device waits on the default path (the Lanczos grid
+// barrier, the tensor-core Gram's commit waits): SVDB_WAIT_LIMIT_NS from the
+// environment (read at each launch, at least 1), else 2 s.
+uint64_t wait_limit_ns();
 
 // ------------------------------------------------------- kernel entries ----
 // y[r] = sum_k val[k] * x[idx[k]] over the rows of `m` (group-per-row).

@@ -76,3 +76,66 @@ def lowrank_plus_noise(m, n, rank, noise, seed, density=1.0) -> dict:
 
 def omega(n, l, seed) -> np.ndarray:
     return np.random.default_rng(seed).standard_normal((n, l))
+
+
+def count_like(m=100_000, n=30_000, seed=2024):
+    """The randomized-SVD workload: a seeded count-like CSR.  Column rates
+    lambda_j ~ Gamma(0.5, 2); row lengths ~ LogNormal(ln 600, 0.5), capped at n;
+    columns drawn proportional to lambda_j with replacement and merged per row
+    (the realised nnz is what the caller reports); values log1p(Poisson(lambda_j) + 1).
+    Returns (indptr int64, cols int64, vals f64)."""
+    rng = np.random.default_rng(seed)
+    lam = rng.gamma(0.5, 2.0, n)
+    k = np.clip(np.rint(rng.lognormal(np.log(600.0), 0.5, m)), 1, n).astype(np.int64)
+    cdf = np.cumsum(lam / lam.sum())
+    cdf[-1] = 1.0
+    rows = np.repeat(np.arange(m, dtype=np.int64), k)
+    cols = np.searchsorted(cdf, rng.random(rows.size), side="right").astype(np.int64)
+    np.minimum(cols, n - 1, out=cols)
+    keys = rows * n + cols
+    keys.sort()
+    keep = np.ones(keys.size, dtype=bool)
+    keep[1:] = keys[1:] != keys[:-1]
+    rows, cols = np.divmod(keys[keep], n)
+    del keys, keep
+    indptr = np.zeros(m + 1, np.int64)
+    np.cumsum(np.bincount(rows, minlength=m), out=indptr[1:])
+    vals = np.log1p(rng.poisson(lam[cols]) + 1.0)
+    return indptr, cols, vals
+
+
+def zipf_planted_device(torch, m=1_000_000, n=200_000, seed=3):
+    """The large LAS2 workload, generated on the device (torch CUDA generator):
+    row lengths Zipf(1.85) on [20, 20000] (numpy seed), columns uniform with
+    duplicates merged, values N(0,1) plus a planted rank-20 signal
+    sum_r s_r u_i v_j (unit u, v; s geometric 100..1, scaled by 1/density).
+    Returns (indptr int64, cols int32, vals f64) as CUDA tensors."""
+    rng = np.random.default_rng(seed)
+    ks = np.arange(20, 20001)
+    p = ks.astype(np.float64) ** -1.85
+    p /= p.sum()
+    rowlen = torch.from_numpy(rng.choice(ks, size=m, p=p)).cuda()
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    nnz0 = int(rowlen.sum())
+    keys = torch.repeat_interleave(torch.arange(m, device="cuda", dtype=torch.int64), rowlen) * n
+    keys += torch.randint(0, n, (nnz0,), device="cuda", generator=g, dtype=torch.int64)
+    keys = torch.unique_consecutive(torch.sort(keys).values)
+    rows = keys // n
+    cols = (keys - rows * n).to(torch.int32)
+    del keys
+    nnz = rows.numel()
+    indptr = torch.zeros(m + 1, dtype=torch.int64, device="cuda")
+    indptr[1:] = torch.cumsum(torch.bincount(rows, minlength=m), 0)
+    vals = torch.randn(nnz, dtype=torch.float64, device="cuda", generator=g)
+    r = 20
+    u = torch.randn(m, r, dtype=torch.float64, device="cuda", generator=g)
+    v = torch.randn(n, r, dtype=torch.float64, device="cuda", generator=g)
+    u /= u.norm(dim=0)
+    v /= v.norm(dim=0)
+    sig = torch.logspace(2, 0, r, dtype=torch.float64, device="cuda") * (m * n / nnz)
+    for c0 in range(0, nnz, 1 << 23):
+        c1 = min(nnz, c0 + (1 << 23))
+        vals[c0:c1] += (u[rows[c0:c1]] * v[cols[c0:c1].long()] * sig).sum(1)
+    del rows, u, v
+    return indptr, cols, vals

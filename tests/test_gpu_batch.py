@@ -1,7 +1,7 @@
 """Batches of masked column subsets (svdb_batch_*): each subset's result
 against randomized_svd on MaskedCSRMatrix::with_columns with the same seed
 (f64: singular values 1e-10 relative, leading singular subspaces to 1e-8;
-FP32 products: 1e-5 against the f64 batch), the with_columns semantics
+FP32 products: 1e-6 against the f64 batch), the with_columns semantics
 (order and duplicates ignored, bounds), the captured graph against direct
 launches, and the autotuner's reported choice."""
 import numpy as np
@@ -57,7 +57,7 @@ def test_batch_mixed_against_f64_and_graph_against_direct():
     for a, b, c in zip(g1, g2, f64):
         np.testing.assert_array_equal(a.s, b.s)          # same kernels, same order
         np.testing.assert_array_equal(a.u, b.u)
-        np.testing.assert_allclose(a.s, c.s, rtol=1e-5)  # FP32 products vs f64
+        np.testing.assert_allclose(a.s, c.s, rtol=1e-6)  # FP32 products vs f64
     info = b1.info()
     assert info["count"] == len(subs)
     assert info["subsets_per_row_item"] in (1, 2, 4, 8)

@@ -48,6 +48,26 @@ def test_matches_svdb_opb_on_two_calls(transposed):
             _close(_noalloc(h, x, transposed), h.svd_opb(x, transposed=transposed))
 
 
+def test_first_call_allocates_nothing():
+    """The device's free memory is the same before and after the first call on
+    a fresh handle: the scratch array was placed when the handle was created."""
+    import torch
+    A = M.uniform(2000, 900, 0.01, 5)
+    h = CsrMatrix(A["nrows"], A["ncols"], A["indptr"], A["indices"], A["data"])
+    x = np.random.default_rng(3).standard_normal(A["ncols"])
+    want = h.svd_opb(x)  # the allocating path loads the same SpMV kernel
+    dx = torch.from_numpy(x).cuda()
+    dy = torch.zeros(A["ncols"], dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    rc = _abi.lib().svdb_opb_device_noalloc(h.handle, dx.data_ptr(), dy.data_ptr(), 0, None)
+    assert rc == 0, _abi.last_error()
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+    _close(dy.cpu().numpy(), want)
+
+
 def test_rejects_intermediates_above_the_limit():
     import scipy.sparse as sp
     m = (1 << 20) + 1
