@@ -283,6 +283,24 @@ int svdb_gram_device(const double* d_x, uint64_t rows, uint64_t c, double* d_g, 
  * synchronisation. */
 int svdb_release_cached_memory(void);
 
+/* The tridiagonal QL recurrences on the device, one GPU thread in FP64 with
+ * the crate's unfused operation order: routine 0 = imtqlb of SVDLIBC
+ * (src/legacy.rs:955-1070), 1 = imtqlb as written (src/lanczos/mod.rs:428-584,
+ * max_it its iteration cap, *warned its soft failure), 2/3 = imtql2's scalar
+ * chain with SVDLIBC's / the current pythag (src/legacy.rs:1590-1700,
+ * src/lanczos/mod.rs:901-1028), max_it its cap.  d and e (order n, e[0]
+ * unused) are host arrays, overwritten with the results as the host routines
+ * leave them; bnd (routines 0-1) gets the bounds row, perm (2-3) imtql2's
+ * column order; the first rot_cap plane rotations (i, c, s) are returned and
+ * *n_rot counts them all (routine 1 records none).  *device_ms is the kernel's
+ * time.  Errors: SVDB_ERR_IMTQLB / SVDB_ERR_IMTQL2 as the crate raises them.
+ * The solver runs these recurrences on the host, where the chain of
+ * divisions is faster; this entry point exists to measure and test the device
+ * form. */
+int svdb_tridiag_device(int routine, uint64_t n, double* d, double* e, double* bnd, int32_t* rot_i, double* rot_c,
+                        double* rot_s, uint64_t rot_cap, uint64_t* n_rot, int32_t* perm, uint64_t max_it,
+                        int* warned, double* device_ms);
+
 /* Self-test of the bounded device waits, with no counterpart in the
  * reference: makes one wait run out on purpose -- which = 0 the grid barrier
  * of the cooperative Lanczos block (a one-block grid that expects a second
@@ -292,6 +310,15 @@ int svdb_release_cached_memory(void);
  * usable.  The limit of the real waits (2 s) can be lowered for a process with
  * the environment variable SVDB_WAIT_LIMIT_NS, read at each launch. */
 int svdb_wait_selftest(int which, uint64_t limit_ns);
+
+/* The dense-column split the FP32 products (SVDB_MIXED) of this matrix use,
+ * with no counterpart in the reference: the number of columns whose density
+ * is at least SVDB_DENSE_MIN_DENSITY (0.03 by default) that are multiplied as
+ * a dense block on the tensor cores (3xTF32, FP64 drains), and the nonzeros
+ * they hold; both 0 before the first FP32 product or when no split is used
+ * (too few dense columns, more than 64 dense operand columns, or
+ * SVDB_DENSE_SPLIT=0). */
+int svdb_dense_split_info(const svdb_matrix* a, uint64_t* dense_cols, uint64_t* dense_nnz);
 
 /* Number of kernels this library has launched in the process so far. */
 uint64_t svdb_kernel_launches(void);

@@ -282,12 +282,26 @@ int svdb_multiply_with_dense_device(const svdb_matrix* a, const void* d_dense, u
                 ensure_fp32(a);
                 SVDB_CUDA(cudaStreamSynchronize(a->stream));
             }
-            spmm_dev<float, float>(op, true, (const float*)d_dense, (int)l, (float*)d_result, s);
+            if (dense_split_usable(a, (int)l)) {
+                dense_split_spmm<float, float>(a, transpose_self != 0, (const float*)d_dense, (const float*)d_dense,
+                                               (int)l, (float*)d_result, s);
+                dense_split_check();
+            } else {
+                spmm_dev<float, float>(op, true, (const float*)d_dense, (int)l, (float*)d_result, s);
+            }
         }
     });
 }
 
 uint64_t svdb_kernel_launches(void) { return g_launches.load(); }
+
+int svdb_dense_split_info(const svdb_matrix* a, uint64_t* dense_cols, uint64_t* dense_nnz) {
+    return guarded([&] {
+        check_handle(a);
+        if (!dense_cols || !dense_nnz) throw Error(SVDB_ERR_ARG, "null argument");
+        dense_split_info(a, dense_cols, dense_nnz);
+    });
+}
 
 int svdb_multiply_transposed_by_dense(const svdb_matrix* a, const double* q, uint64_t l, double* result) {
     return guarded([&] {

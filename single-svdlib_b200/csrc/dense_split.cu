@@ -1,0 +1,749 @@
+// Dense-column split of the FP32 SpMM (SVDB_MIXED), for A X and A^T Y with
+// at most 64 dense columns, the products of randomized_svd
+// (src/lanczos/masked.rs:265-471,616-733).
+//
+// The columns of A whose density is at least a threshold (3 % by default)
+// are copied, once per matrix, into a dense block D = A[:, J] (m x nd, FP32,
+// row-major) and its transpose Dt (nd x m).  Their share of every product
+// then runs on the tensor cores as a streamed GEMM instead of a row gather
+// per nonzero:
+//
+//   A X   = A_rest X          + D  X[J, :]      (every row gets both parts)
+//   A^T Y = A_rest^T Y        ; rows J: Dt Y     (disjoint rows)
+//
+// A_rest is A without the columns J; it keeps the segment-gather kernel.
+// On the count-like randomized workload (Gamma(0.5)-weighted columns) the
+// columns of density >= 3 % hold about 60 % of the nonzeros, and their
+// gathers of 240-byte dense rows through L2 were most of the SpMM's time.
+//
+// k_dense_tc computes C (128 x 64 tile) = A_tile (128 x K) . B (64 x K)^T in
+// 3xTF32 (A = Ah + Al, B = Bh + Bl, C = Ah Bh + Ah Bl + Al Bh, each term
+// with FP32 accumulation in tensor memory), draining the accumulator into
+// FP64 every `chunk` stages of 32 columns of K.  Warp roles, one CTA per SM:
+//   warp 0      TMA producer: A stage (128 x 32 FP32, 128-byte swizzle) and
+//               the Bh, Bl stages (64 x 32) into a 4-deep shared-memory ring;
+//   warp 1      tensor-memory owner and MMA issuer (one thread): A from tensor
+//               memory (tcgen05.mma ... [a_tmem]), B from shared memory;
+//   warps 2..5  read the A stage (one row per thread), split it into its TF32
+//               head and remainder, store both into tensor memory
+//               (tcgen05.st), and drain the accumulators into FP64.
+// Keeping A out of shared memory after the TMA copy (its split goes to tensor
+// memory) leaves shared memory 2 bytes of traffic per byte of A instead of 7.
+// Every mbarrier wait is bounded (SVDB_WAIT_LIMIT_NS, 2 s by default); on a
+// timeout the kernel raises g_dense_err, every role leaves its loop, the
+// copies and MMAs in flight are waited for (bounded) and tensor memory is
+// freed.  No TMA load uses multicast; every tensor map covers this GPU's own
+// memory.
+#include <cub/cub.cuh>
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cstdlib>
+#include <memory>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "device_common.cuh"
+#include "ops.cuh"
+#include "svdb_internal.h"
+
+namespace svdb {
+
+constexpr int kDtM = 128;                                  // rows per tile (tensor-memory lanes)
+constexpr int kDtN = 64;                                   // output columns per tile (l <= 64)
+constexpr int kDtK = 32;                                   // K per stage: one 128-byte swizzle row
+constexpr int kDtStages = 4;
+constexpr int kDtAbytes = kDtM * kDtK * 4;                 // 16 KB
+constexpr int kDtBbytes = kDtN * kDtK * 4;                 // 8 KB
+constexpr int kDtStageBytes = kDtAbytes + 2 * kDtBbytes;   // 32 KB
+constexpr int kDtAccBytes = kDtN * kDtM * 8;               // FP64 accumulators, [column][row]
+constexpr int kDtSmem = kDtStages * kDtStageBytes + kDtAccBytes + 1024;
+constexpr int kDtThreads = 192;
+constexpr int kDtChunk = 32;                               // stages per FP64 drain (K = 1024)
+// F32 accumulator, TF32 A and B, both K-major, N = 64, M = 128
+constexpr uint32_t kDtIdesc =
+    (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kDtN >> 3) << 17) | ((uint32_t)(kDtM >> 4) << 24);
+// tensor memory: accumulators in columns [0, 128) (two buffers of 64), the A
+// operand in [128, 256) (two slots of 32 head + 32 remainder columns)
+constexpr uint32_t kDtTmemCols = 256;
+constexpr uint32_t kDtAcol = 128;
+
+__device__ int g_dense_err;
+
+struct DtArgs {
+    int64_t rows;     // valid rows of A (output rows in mode 0)
+    int64_t k_total;  // K extent of A and B
+    int64_t k_per;    // K per work item (a multiple of kDtK)
+    int32_t m_tiles, k_splits;
+    int32_t l;        // output columns written (mode 0)
+    int32_t mode;     // 0: out[row * ldo + j] += C; 1: out[((ks * m_tiles * 128) + row) * 64 + j] = C
+    int32_t out_f32;  // mode 0: out holds floats (else doubles)
+    void* out;
+    int64_t ldo;
+    unsigned long long limit_ns;
+};
+
+__device__ __forceinline__ uint32_t dt_smem(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups 1024 B apart
+__device__ __forceinline__ uint64_t dt_desc(uint32_t saddr) {
+    return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+           (1ull << 46) | (2ull << 61);
+}
+
+// bounded wait that also gives up when another role has aborted
+__device__ __forceinline__ bool dt_wait(uint32_t bar, uint32_t parity, unsigned long long limit,
+                                        volatile int* abort) {
+    const unsigned long long t0 = global_ns();
+    uint32_t ok = 0, spins = 0;
+    while (true) {
+        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+                     : "=r"(ok)
+                     : "r"(bar), "r"(parity)
+                     : "memory");
+        if (ok) return true;
+        if ((++spins & 63u) == 0) {
+            if (*abort) return false;
+            if (global_ns() - t0 > limit) {
+                *abort = 1;
+                atomicOr(&g_dense_err, 1);
+                return false;
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void dt_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void dt_tma(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            dst),
+        "l"(map), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+__device__ __forceinline__ void dt_mma(uint32_t d, uint32_t a_tmem, uint64_t b, uint32_t acc) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n}" ::"r"(d),
+        "r"(a_tmem), "l"(b), "r"(kDtIdesc), "r"(acc)
+        : "memory");
+}
+
+__device__ __forceinline__ void dt_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+#define DT_ST32(taddr, v)                                                                                           \
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, " \
+                 "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32};" \
+                 ::"r"(taddr), "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]),          \
+                 "r"(v[7]), "r"(v[8]), "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]),        \
+                 "r"(v[15]), "r"(v[16]), "r"(v[17]), "r"(v[18]), "r"(v[19]), "r"(v[20]), "r"(v[21]), "r"(v[22]),     \
+                 "r"(v[23]), "r"(v[24]), "r"(v[25]), "r"(v[26]), "r"(v[27]), "r"(v[28]), "r"(v[29]), "r"(v[30]),     \
+                 "r"(v[31])                                                                                          \
+                 : "memory")
+
+#define DT_LD32(v, taddr)                                                                                          \
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, " \
+                 "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, " \
+                 "[%32];"                                                                                          \
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),  \
+                   "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),         \
+                   "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),       \
+                   "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),       \
+                   "=r"(v[29]), "=r"(v[30]), "=r"(v[31])                                                            \
+                 : "r"(taddr)                                                                                      \
+                 : "memory")
+
+// TF32 head of x, rounded to nearest (the remainder x - head is exact in FP32)
+__device__ __forceinline__ float tf32_head(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+
+__global__ void __launch_bounds__(kDtThreads, 1)
+    k_dense_tc(const __grid_constant__ CUtensorMap amap, const __grid_constant__ CUtensorMap bhmap,
+               const __grid_constant__ CUtensorMap blmap, const DtArgs a) {
+    extern __shared__ unsigned char dyn[];
+    __shared__ __align__(8) uint64_t bar_full[kDtStages], bar_empty[kDtStages], bar_tmf[2], bar_tme[2],
+        bar_accf[2], bar_acce[2], bar_fin;
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_abort;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(dyn) + 1023) & ~uintptr_t(1023));
+    double* sacc = reinterpret_cast<double*>(sm + kDtStages * kDtStageBytes);
+    volatile int* abort = &s_abort;
+
+    if (tid == 0) {
+        for (int s = 0; s < kDtStages; ++s) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(dt_smem(&bar_full[s])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 5;" ::"r"(dt_smem(&bar_empty[s])) : "memory");
+        }
+        for (int t = 0; t < 2; ++t) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;" ::"r"(dt_smem(&bar_tmf[t])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(dt_smem(&bar_tme[t])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(dt_smem(&bar_accf[t])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;" ::"r"(dt_smem(&bar_acce[t])) : "memory");
+        }
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(dt_smem(&bar_fin)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_abort = 0;
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dt_smem(&s_tmem)),
+                     "r"(kDtTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = s_tmem;
+    const int64_t items = (int64_t)a.m_tiles * a.k_splits;
+    auto item_geom = [&](int64_t it, int64_t& m0, int64_t& kb, int& nst, int& ks) {
+        ks = (int)(it / a.m_tiles);
+        m0 = (it % a.m_tiles) * kDtM;
+        kb = (int64_t)ks * a.k_per;
+        const int64_t ke = min(a.k_total, kb + a.k_per);
+        nst = (int)((ke - kb + kDtK - 1) / kDtK);
+    };
+
+    uint32_t issued = 0;  // producer: stages issued; MMA: stages consumed
+    if (warp == 0 && lane == 0) {
+        // ------------------------------------------------------- producer --
+        for (int64_t it = blockIdx.x; it < items && !*abort; it += gridDim.x) {
+            int64_t m0, kb;
+            int nst, ks;
+            item_geom(it, m0, kb, nst, ks);
+            for (int st = 0; st < nst; ++st, ++issued) {
+                const int s = issued % kDtStages;
+                if (!dt_wait(dt_smem(&bar_empty[s]), ((issued / kDtStages) & 1) ^ 1, a.limit_ns, abort)) break;
+                unsigned char* base = sm + s * kDtStageBytes;
+                const uint32_t fb = dt_smem(&bar_full[s]);
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fb), "r"(kDtStageBytes)
+                             : "memory");
+                const int kx = (int)(kb + (int64_t)st * kDtK);
+                dt_tma(dt_smem(base), &amap, kx, (int)m0, fb);
+                dt_tma(dt_smem(base + kDtAbytes), &bhmap, kx, 0, fb);
+                dt_tma(dt_smem(base + kDtAbytes + kDtBbytes), &blmap, kx, 0, fb);
+            }
+        }
+        // every copy issued must land before the CTA may exit
+        for (uint32_t q = 0; q < kDtStages && q < issued; ++q) {
+            const uint32_t last = issued - 1 - q;  // the last issue into slot last % kDtStages
+            volatile int never = 0;
+            dt_wait(dt_smem(&bar_full[last % kDtStages]), (last / kDtStages) & 1, 2000000000ull, &never);
+        }
+    } else if (warp == 1 && lane == 0) {
+        // ------------------------------------------------------------ MMA --
+        uint32_t ch = 0;
+        bool any = false;
+        for (int64_t it = blockIdx.x; it < items && !*abort; it += gridDim.x) {
+            int64_t m0, kb;
+            int nst, ks;
+            item_geom(it, m0, kb, nst, ks);
+            bool ok = true;
+            for (int st = 0; st < nst && ok; ++st, ++issued) {
+                const int s = issued % kDtStages, t = issued & 1, b = ch & 1;
+                const bool first = (st % kDtChunk) == 0, last = (st % kDtChunk) == kDtChunk - 1 || st == nst - 1;
+                if (first && !dt_wait(dt_smem(&bar_acce[b]), ((ch >> 1) & 1) ^ 1, a.limit_ns, abort)) { ok = false; break; }
+                if (!dt_wait(dt_smem(&bar_full[s]), (issued / kDtStages) & 1, a.limit_ns, abort)) { ok = false; break; }
+                if (!dt_wait(dt_smem(&bar_tmf[t]), (issued >> 1) & 1, a.limit_ns, abort)) { ok = false; break; }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const unsigned char* base = sm + s * kDtStageBytes;
+                const uint64_t bh = dt_desc(dt_smem(base + kDtAbytes));
+                const uint64_t bl = dt_desc(dt_smem(base + kDtAbytes + kDtBbytes));
+                const uint32_t d = tmem + (uint32_t)b * kDtN;
+                const uint32_t ah = tmem + kDtAcol + (uint32_t)t * 64, al = ah + 32;
+#pragma unroll
+                for (int kk = 0; kk < kDtK / 8; ++kk) {
+                    const uint64_t koff = (uint64_t)((kk * 32) >> 4);  // 8 TF32 = 32 bytes along the swizzled row
+                    dt_mma(d, ah + kk * 8, bh + koff, (first && kk == 0) ? 0u : 1u);
+                    dt_mma(d, ah + kk * 8, bl + koff, 1u);
+                    dt_mma(d, al + kk * 8, bh + koff, 1u);
+                }
+                any = true;
+                dt_commit(dt_smem(&bar_empty[s]));
+                dt_commit(dt_smem(&bar_tme[t]));
+                if (last) {
+                    dt_commit(dt_smem(&bar_accf[b]));
+                    ++ch;
+                }
+            }
+            if (!ok) break;
+        }
+        if (any) {  // the last MMAs must complete before tensor memory is freed
+            dt_commit(dt_smem(&bar_fin));
+            volatile int never = 0;
+            dt_wait(dt_smem(&bar_fin), 0, 2000000000ull, &never);
+        }
+    } else if (warp >= 2) {
+        // ------------------------------------- split, tensor-memory store, drain --
+        const int g = warp & 3;          // tensor-memory lane group of this warp
+        const int r = g * 32 + lane;     // row of the tile
+        const uint32_t lane_base = tmem + ((uint32_t)(g * 32) << 16);
+        for (int j = 0; j < kDtN; ++j) sacc[j * kDtM + r] = 0.0;
+        uint32_t ch = 0;
+        bool pending = false, pending_last = false;
+        int64_t pend_m0 = 0;
+        int pend_ks = 0;
+        auto drain = [&]() -> bool {
+            const int b = ch & 1;
+            if (!dt_wait(dt_smem(&bar_accf[b]), (ch >> 1) & 1, a.limit_ns, abort)) return false;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                uint32_t v[32];
+                DT_LD32(v, lane_base + (uint32_t)b * kDtN + h * 32);
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                for (int j = 0; j < 32; ++j) sacc[(h * 32 + j) * kDtM + r] += (double)__uint_as_float(v[j]);
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) dt_arrive(dt_smem(&bar_acce[b]));
+            ++ch;
+            if (pending_last) {
+                const int64_t row = pend_m0 + r;
+                if (a.mode == 0) {
+                    if (row < a.rows) {
+                        if (a.out_f32) {
+                            float* o = static_cast<float*>(a.out) + row * a.ldo;
+                            for (int j = 0; j < a.l; ++j) o[j] = (float)((double)o[j] + sacc[j * kDtM + r]);
+                        } else {
+                            double* o = static_cast<double*>(a.out) + row * a.ldo;
+                            for (int j = 0; j < a.l; ++j) o[j] += sacc[j * kDtM + r];
+                        }
+                    }
+                } else {
+                    double* o = static_cast<double*>(a.out) + (((int64_t)pend_ks * a.m_tiles * kDtM) + row) * kDtN;
+                    for (int j = 0; j < kDtN; ++j) o[j] = sacc[j * kDtM + r];
+                }
+                for (int j = 0; j < kDtN; ++j) sacc[j * kDtM + r] = 0.0;
+            }
+            pending = false;
+            return true;
+        };
+        bool ok = true;
+        for (int64_t it = blockIdx.x; it < items && ok && !*abort; it += gridDim.x) {
+            int64_t m0, kb;
+            int nst, ks;
+            item_geom(it, m0, kb, nst, ks);
+            for (int st = 0; st < nst; ++st, ++issued) {
+                const int s = issued % kDtStages, t = issued & 1;
+                if (!dt_wait(dt_smem(&bar_full[s]), (issued / kDtStages) & 1, a.limit_ns, abort)) { ok = false; break; }
+                const unsigned char* row_p = sm + s * kDtStageBytes + r * 128;
+                uint32_t hi[32], lo[32];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const float4 x = *reinterpret_cast<const float4*>(row_p + ((q ^ (r & 7)) << 4));
+                    const float xs[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        const float h = tf32_head(xs[e]);
+                        hi[q * 4 + e] = __float_as_uint(h);
+                        lo[q * 4 + e] = __float_as_uint(xs[e] - h);
+                    }
+                }
+                __syncwarp();
+                if (lane == 0) dt_arrive(dt_smem(&bar_empty[s]));
+                if (!dt_wait(dt_smem(&bar_tme[t]), ((issued >> 1) & 1) ^ 1, a.limit_ns, abort)) { ok = false; break; }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t slot = lane_base + kDtAcol + (uint32_t)t * 64;
+                DT_ST32(slot, hi);
+                DT_ST32(slot + 32, lo);
+                asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                __syncwarp();
+                if (lane == 0) dt_arrive(dt_smem(&bar_tmf[t]));
+                if ((st % kDtChunk) == 0 && pending && !drain()) { ok = false; break; }
+                if ((st % kDtChunk) == kDtChunk - 1 || st == nst - 1) {
+                    pending = true;
+                    pending_last = (st == nst - 1);
+                    pend_m0 = m0;
+                    pend_ks = ks;
+                }
+            }
+        }
+        if (ok && pending) drain();
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 1) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kDtTmemCols) : "memory");
+    }
+}
+
+// ------------------------------------------------------- operand prep --
+// B of A X: Bh/Bl (64 x kp, K-major) = TF32 head / remainder of X[cols[k], j]
+// (zero past l and for padding columns cols[k] < 0), from the FP64 operand.
+template <typename XT>
+__global__ void k_dense_b_gather(const XT* __restrict__ X, int l, const int32_t* __restrict__ cols, int64_t kp,
+                                 float* __restrict__ bh, float* __restrict__ bl) {
+    const int64_t total = (int64_t)kDtN * kp;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        const int j = (int)(i / kp);
+        const int64_t k = i - (int64_t)j * kp;
+        const int32_t c = cols[k];
+        const double x = (j < l && c >= 0) ? (double)X[(int64_t)c * l + j] : 0.0;
+        const float h = tf32_head((float)x);
+        bh[i] = h;
+        bl[i] = (float)(x - (double)h);
+    }
+}
+
+// B of A^T Y: Bh/Bl (64 x kp) = head / remainder of Y^T (Y: rows x l), zero
+// past rows and l.  32 x 32 tiles through shared memory.
+template <typename XT>
+__global__ void k_dense_b_transpose(const XT* __restrict__ Y, int64_t rows, int l, int64_t kp,
+                                    float* __restrict__ bh, float* __restrict__ bl) {
+    __shared__ double tile[32][33];
+    const int64_t k0 = (int64_t)blockIdx.x * 32;
+    const int j0 = blockIdx.y * 32;
+    for (int rr = threadIdx.y; rr < 32; rr += blockDim.y) {
+        const int64_t k = k0 + rr;
+        const int j = j0 + threadIdx.x;
+        tile[rr][threadIdx.x] = (k < rows && j < l) ? (double)Y[k * l + j] : 0.0;
+    }
+    __syncthreads();
+    for (int jj = threadIdx.y; jj < 32; jj += blockDim.y) {
+        const int j = j0 + jj;
+        const int64_t k = k0 + threadIdx.x;
+        if (k < kp) {
+            const double x = tile[threadIdx.x][jj];
+            const float h = tf32_head((float)x);
+            bh[(int64_t)j * kp + k] = h;
+            bl[(int64_t)j * kp + k] = (float)(x - (double)h);
+        }
+    }
+}
+
+// Z[cols[r], j] = sum over the K splits of the partial tiles (fixed order)
+template <typename OT>
+__global__ void k_dense_reduce(const double* __restrict__ part, int ksplits, int64_t mrows, int64_t nd,
+                               const int32_t* __restrict__ cols, int l, OT* __restrict__ Z) {
+    const int64_t total = nd * l;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = i / l;
+        const int j = (int)(i - r * l);
+        double acc = 0.0;
+        for (int k = 0; k < ksplits; ++k) acc += part[((int64_t)k * mrows + r) * kDtN + j];
+        Z[(int64_t)cols[r] * l + j] = (OT)acc;
+    }
+}
+
+// --------------------------------------------------------------- build --
+// D[r, k] and Dt[k, r] from column cols[k] of the CSC (one warp per column).
+__global__ void k_dense_scatter(const int64_t* __restrict__ cp, const int32_t* __restrict__ ri,
+                                const float* __restrict__ v, const int32_t* __restrict__ cols, int64_t nd,
+                                int64_t ndp, int64_t mp, float* __restrict__ D, float* __restrict__ Dt) {
+    const int lane = threadIdx.x & 31;
+    const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t k = gw; k < nd; k += nw) {
+        const int32_t c = cols[k];
+        for (int64_t e = cp[c] + lane; e < cp[c + 1]; e += 32) {
+            const int64_t r = ri[e];
+            D[r * ndp + k] = v[e];
+            Dt[k * mp + r] = v[e];
+        }
+    }
+}
+
+// entries of each major slice kept when keep(minor) (drop_major: the whole
+// slice is dropped when the major index is flagged instead); counts first
+__global__ void k_rest_count(const int64_t* __restrict__ p, const int32_t* __restrict__ idx, int64_t nmajor,
+                             const uint8_t* __restrict__ dense, bool by_major, int64_t* __restrict__ cnt) {
+    const int lane = threadIdx.x & 31;
+    const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t r = gw; r <= nmajor; r += nw) {
+        if (r == nmajor) {
+            if (lane == 0) cnt[r] = 0;
+            continue;
+        }
+        int64_t c = 0;
+        if (by_major) {
+            c = dense[r] ? 0 : p[r + 1] - p[r];
+        } else {
+            for (int64_t e = p[r] + lane; e < p[r + 1]; e += 32) c += dense[idx[e]] ? 0 : 1;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+        }
+        if (lane == 0) cnt[r] = c;
+    }
+}
+
+__global__ void k_rest_fill(const int64_t* __restrict__ p, const int32_t* __restrict__ idx,
+                            const float* __restrict__ v, int64_t nmajor, const uint8_t* __restrict__ dense,
+                            bool by_major, const int64_t* __restrict__ np, int32_t* __restrict__ nidx,
+                            float* __restrict__ nv) {
+    const int lane = threadIdx.x & 31;
+    const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t r = gw; r < nmajor; r += nw) {
+        if (by_major && dense[r]) continue;
+        int64_t out = np[r];
+        for (int64_t e0 = p[r]; e0 < p[r + 1]; e0 += 32) {
+            const int64_t e = e0 + lane;
+            const bool in = e < p[r + 1];
+            const int32_t c = in ? idx[e] : 0;
+            const bool keep = in && (by_major || !dense[c]);
+            const unsigned m = __ballot_sync(0xffffffffu, keep);
+            if (keep) {
+                const int64_t o = out + __popc(m & ((1u << lane) - 1u));
+                nidx[o] = c;
+                nv[o] = v[e];
+            }
+            out += __popc(m);
+        }
+    }
+}
+
+static PFN_cuTensorMapEncodeTiled_v12000 dt_encode() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        cudaDriverEntryPointQueryResult q;
+        void* p = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// FP32 row-major [rows x cols] (cols a multiple of 32, rows of cols * 4 bytes,
+// 16-byte aligned base), boxes of box_rows x 32 with the 128-byte swizzle
+static CUtensorMap dt_map(const float* base, int64_t cols, int64_t rows, int box_rows) {
+    CUtensorMap m;
+    const cuuint64_t gdim[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+    const cuuint64_t gstr[1] = {(cuuint64_t)cols * 4};
+    const cuuint32_t box[2] = {(cuuint32_t)kDtK, (cuuint32_t)box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    if ((reinterpret_cast<uintptr_t>(base) & 15) || (cols % kDtK))
+        throw Error(SVDB_ERR_CUDA, "dense split: operand not aligned for the tensor memory accelerator");
+    CUresult r = dt_encode()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), gdim, gstr, box, estr,
+                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw Error(SVDB_ERR_CUDA, "dense split: cuTensorMapEncodeTiled failed");
+    return m;
+}
+
+static int dt_grid(int64_t items) {
+    return (int)std::max<int64_t>(1, std::min<int64_t>(items, device_props().sms));
+}
+
+static void dt_launch(const float* A, int64_t a_rows, int64_t a_cols, const float* bh, const float* bl,
+                      int64_t k_per, int ksplits, int l, int mode, bool out_f32, void* out, int64_t ldo,
+                      cudaStream_t s) {
+    static std::once_flag attr;
+    std::call_once(attr, [] {
+        SVDB_CUDA(cudaFuncSetAttribute(k_dense_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kDtSmem));
+    });
+    const CUtensorMap am = dt_map(A, a_cols, a_rows, kDtM);
+    const CUtensorMap hm = dt_map(bh, a_cols, kDtN, kDtN);
+    const CUtensorMap lm = dt_map(bl, a_cols, kDtN, kDtN);
+    DtArgs g;
+    g.rows = a_rows;
+    g.k_total = a_cols;
+    g.k_per = k_per;
+    g.m_tiles = (int)((a_rows + kDtM - 1) / kDtM);
+    g.k_splits = ksplits;
+    g.l = l;
+    g.mode = mode;
+    g.out_f32 = out_f32 ? 1 : 0;
+    g.out = out;
+    g.ldo = ldo;
+    g.limit_ns = wait_limit_ns();
+    const int64_t items = (int64_t)g.m_tiles * ksplits;
+    k_dense_tc<<<dt_grid(items), kDtThreads, kDtSmem, s>>>(am, hm, lm, g);
+    SVDB_CHECK_LAUNCH();
+}
+
+void dense_split_check() {
+    int e = 0;
+    SVDB_CUDA(cudaMemcpyFromSymbol(&e, g_dense_err, sizeof(int)));
+    if (e) {
+        const int z = 0;
+        SVDB_CUDA(cudaMemcpyToSymbol(g_dense_err, &z, sizeof(int)));
+        throw Error(SVDB_ERR_TIMEOUT, "dense split: a tensor-core pipeline wait exceeded its limit");
+    }
+}
+
+static int64_t nblocks(int64_t work, int threads) {
+    return std::max<int64_t>(1, std::min<int64_t>((work + threads - 1) / threads, (int64_t)device_props().sms * 16));
+}
+
+// Compacted copy of `src` keeping the entries whose minor index is not dense
+// (by_major = false) or the major slices that are not dense (by_major = true).
+static void build_rest(const DevCompressed& src, const uint8_t* dense, bool by_major, DevCompressed& out,
+                       cudaStream_t s) {
+    out.nmajor = src.nmajor;
+    out.nminor = src.nminor;
+    out.owner_stream = s;
+    out.ptr.alloc(src.nmajor + 1, s);
+    DevBuf<int64_t> cnt(src.nmajor + 1, s);
+    k_rest_count<<<(int)nblocks((src.nmajor + 1) * 32, 256), 256, 0, s>>>(src.ptr.p, src.idx.p, src.nmajor, dense,
+                                                                           by_major, cnt.p);
+    SVDB_CHECK_LAUNCH();
+    size_t tb = 0;
+    SVDB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt.p, out.ptr.p, src.nmajor + 1, s));
+    DevBuf<uint8_t> tmp(std::max<size_t>(tb, 1), s);
+    SVDB_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, tb, cnt.p, out.ptr.p, src.nmajor + 1, s));
+    int64_t nnz = 0;
+    SVDB_CUDA(cudaMemcpyAsync(&nnz, out.ptr.p + src.nmajor, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    SVDB_CUDA(cudaStreamSynchronize(s));
+    out.nnz = nnz;
+    out.idx.alloc(std::max<int64_t>(nnz, 1), s);
+    out.val32.alloc(std::max<int64_t>(nnz, 1), s);
+    k_rest_fill<<<(int)nblocks(src.nmajor * 32, 256), 256, 0, s>>>(src.ptr.p, src.idx.p, src.val32.p, src.nmajor,
+                                                                   dense, by_major, out.ptr.p, out.idx.p, out.val32.p);
+    SVDB_CHECK_LAUNCH();
+    build_seg_plan(out, s);
+}
+
+static double dense_min_density() {
+    const char* e = getenv("SVDB_DENSE_MIN_DENSITY");
+    if (e && *e) return atof(e);
+    return 0.03;
+}
+
+static bool dense_enabled() {
+    const char* e = getenv("SVDB_DENSE_SPLIT");
+    return !(e && std::string(e) == "0");
+}
+
+static std::mutex g_dense_mu;
+
+// The split of the structures `a` computes with, built on first use (under
+// SVDB_MIXED, with FP32 values present).  Null when no column is dense
+// enough, the matrix is small, or the split is switched off.
+static DenseSplit* dense_split_for(const svdb_matrix* a) {
+    const svdb_matrix* owner = (a->kind == KIND_MASKED && a->all_columns) ? a->parent : a;
+    svdb_matrix* w = const_cast<svdb_matrix*>(owner);
+    std::lock_guard<std::mutex> lk(g_dense_mu);
+    if (w->dense_tried) return w->dense.get();
+    w->dense_tried = true;
+    const DevCompressed& csr = w->csr;
+    const DevCompressed& csc = w->csc;
+    const int64_t m = csr.nmajor, n = csr.nminor;
+    if (m < 4 * kDtM || n < kDtM || !csr.val32.p || !csc.val32.p) return nullptr;
+    cudaStream_t s = w->stream;
+    // column counts from the CSC offsets; the densest columns first
+    std::vector<int64_t> cp(n + 1);
+    SVDB_CUDA(cudaMemcpyAsync(cp.data(), csc.ptr.p, (n + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    SVDB_CUDA(cudaStreamSynchronize(s));
+    const double thr = dense_min_density() * (double)m;
+    std::vector<int32_t> order;
+    for (int64_t j = 0; j < n; ++j)
+        if ((double)(cp[j + 1] - cp[j]) >= thr) order.push_back((int32_t)j);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int32_t x, int32_t y) { return cp[x + 1] - cp[x] > cp[y + 1] - cp[y]; });
+    // memory: D and Dt take 8 m nd bytes; keep them under a quarter of the free memory and 16 GB
+    size_t free_b = 0, total_b = 0;
+    SVDB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const double cap = std::min<double>(16e9, 0.25 * (double)free_b);
+    const int64_t mp = (m + kDtK - 1) / kDtK * kDtK;
+    int64_t nd_max = (int64_t)(cap / (8.0 * (double)mp)) / kDtM * kDtM;
+    int64_t nd = std::min<int64_t>((int64_t)order.size(), nd_max);
+    if (nd < kDtM) return nullptr;
+    order.resize(nd);
+    std::sort(order.begin(), order.end());  // ascending columns: the operand gather reads X in order
+    const int64_t ndp = (nd + kDtM - 1) / kDtM * kDtM;
+    auto ds = std::make_unique<DenseSplit>();
+    ds->nd = nd;
+    ds->ndp = ndp;
+    ds->mp = mp;
+    std::vector<int32_t> cols(ndp, -1);
+    std::copy(order.begin(), order.end(), cols.begin());
+    std::vector<uint8_t> flag(n, 0);
+    for (int32_t c : order) flag[c] = 1;
+    ds->cols.alloc(ndp, s);
+    DevBuf<uint8_t> dflag(n, s);
+    SVDB_CUDA(cudaMemcpyAsync(ds->cols.p, cols.data(), ndp * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    SVDB_CUDA(cudaMemcpyAsync(dflag.p, flag.data(), n, cudaMemcpyHostToDevice, s));
+    ds->D.alloc((size_t)m * ndp, s);
+    ds->Dt.alloc((size_t)ndp * mp, s);
+    SVDB_CUDA(cudaMemsetAsync(ds->D.p, 0, (size_t)m * ndp * sizeof(float), s));
+    SVDB_CUDA(cudaMemsetAsync(ds->Dt.p, 0, (size_t)ndp * mp * sizeof(float), s));
+    k_dense_scatter<<<(int)nblocks(nd * 32, 256), 256, 0, s>>>(csc.ptr.p, csc.idx.p, csc.val32.p, ds->cols.p, nd, ndp,
+                                                              mp, ds->D.p, ds->Dt.p);
+    SVDB_CHECK_LAUNCH();
+    build_rest(csr, dflag.p, false, ds->rest_csr, s);
+    build_rest(csc, dflag.p, true, ds->rest_csc, s);
+    ds->dense_nnz = csr.nnz - ds->rest_csr.nnz;
+    SVDB_CUDA(cudaStreamSynchronize(s));
+    w->dense = std::move(ds);
+    return w->dense.get();
+}
+
+// nd and the nonzeros in the dense block (0, 0 when the matrix has no split)
+void dense_split_info(const svdb_matrix* a, uint64_t* nd, uint64_t* dense_nnz) {
+    const svdb_matrix* owner = (a->kind == KIND_MASKED && a->all_columns) ? a->parent : a;
+    std::lock_guard<std::mutex> lk(g_dense_mu);
+    *nd = owner->dense ? (uint64_t)owner->dense->nd : 0;
+    *dense_nnz = owner->dense ? (uint64_t)owner->dense->dense_nnz : 0;
+}
+
+bool dense_split_usable(const svdb_matrix* a, int l) {
+    if (l < 1 || l > kDtN || !dense_enabled()) return false;
+    return dense_split_for(a) != nullptr;
+}
+
+// Y (m x l) = A X (transpose = false; X: n x l) or Z (n x l) = A^T Y
+// (transpose = true; Y: m x l), FP32 products; x32 is the FP32 copy of the
+// dense operand (minor x l) that the sparse remainder gathers (X itself when
+// XT is float).  Everything runs on stream s in order: the remainder writes
+// every output row, then the dense part adds its share (A X) or writes the
+// dense rows (A^T Y).
+template <typename XT, typename OT>
+void dense_split_spmm(const svdb_matrix* a, bool transpose, const XT* X, const float* x32, int l, OT* Y,
+                      cudaStream_t s) {
+    DenseSplit* ds = dense_split_for(a);
+    if (!ds) throw Error(SVDB_ERR_ARG, "dense split: not available for this matrix");
+    if (l < 1 || l > kDtN) throw Error(SVDB_ERR_ARG, "dense split: 1 to 64 dense columns");
+    const int64_t m = ds->rest_csr.nmajor;
+    constexpr bool of32 = std::is_same<OT, float>::value;
+    if (!transpose) {
+        spmm_dev<float, OT>(ds->rest_csr, true, x32, l, Y, s);  // every row written
+        DevBuf<float> bh((size_t)kDtN * ds->ndp, s), bl((size_t)kDtN * ds->ndp, s);
+        k_dense_b_gather<XT><<<(int)nblocks(kDtN * ds->ndp, 256), 256, 0, s>>>(X, l, ds->cols.p, ds->ndp, bh.p,
+                                                                               bl.p);
+        SVDB_CHECK_LAUNCH();
+        dt_launch(ds->D.p, m, ds->ndp, bh.p, bl.p, ds->ndp, 1, l, 0, of32, Y, l, s);
+    } else {
+        spmm_dev<float, OT>(ds->rest_csc, true, x32, l, Y, s);  // dense rows written as 0
+        DevBuf<float> bh((size_t)kDtN * ds->mp, s), bl((size_t)kDtN * ds->mp, s);
+        dim3 tb(32, 8), tg((unsigned)(ds->mp / 32), (unsigned)(kDtN / 32));
+        k_dense_b_transpose<XT><<<tg, tb, 0, s>>>(X, m, l, ds->mp, bh.p, bl.p);
+        SVDB_CHECK_LAUNCH();
+        const int64_t m_tiles = ds->ndp / kDtM;
+        int ks = (int)std::max<int64_t>(1, (4 * (int64_t)device_props().sms + m_tiles - 1) / m_tiles);
+        const int64_t k_per = ((ds->mp + ks - 1) / ks + kDtK - 1) / kDtK * kDtK;
+        ks = (int)((ds->mp + k_per - 1) / k_per);
+        DevBuf<double> part((size_t)ks * ds->ndp * kDtN, s);
+        dt_launch(ds->Dt.p, ds->ndp, ds->mp, bh.p, bl.p, k_per, ks, l, 1, false, part.p, kDtN, s);
+        k_dense_reduce<OT><<<(int)nblocks(ds->nd * l, 256), 256, 0, s>>>(part.p, ks, ds->ndp, ds->nd, ds->cols.p, l,
+                                                                          Y);
+        SVDB_CHECK_LAUNCH();
+    }
+}
+
+template void dense_split_spmm<double, double>(const svdb_matrix*, bool, const double*, const float*, int, double*,
+                                               cudaStream_t);
+template void dense_split_spmm<float, float>(const svdb_matrix*, bool, const float*, const float*, int, float*,
+                                             cudaStream_t);
+
+}  // namespace svdb

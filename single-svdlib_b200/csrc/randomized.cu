@@ -551,6 +551,8 @@ void randomized(const svdb_matrix* A, uint64_t target_rank, uint64_t n_oversampl
     // FP32 copy of the dense operand (half the gathered bytes), FP64 sums and output.
     DevBuf<float> f_in;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> spmm_events;  // read once, at the end
+    // SVDB_MIXED with dense columns: their share of each product on the tensor cores
+    const bool split = mixed && !f32 && dense_split_usable(A, l);
     auto spmm = [&](const DevCompressed& M, const double* X, int c, double* Y) {
         cudaEvent_t a, b;
         SVDB_CUDA(cudaEventCreate(&a));
@@ -562,7 +564,8 @@ void randomized(const svdb_matrix* A, uint64_t target_rank, uint64_t n_oversampl
             if ((int64_t)f_in.n < M.nminor * c) f_in.alloc(M.nminor * c, s);
             k_to_float<<<nb(M.nminor * c, 256), 256, 0, s>>>(X, f_in.p, M.nminor * c);
             SVDB_CHECK_LAUNCH();
-            spmm_dev<float, double>(M, true, f_in.p, c, Y, s);
+            if (split) dense_split_spmm<double, double>(A, &M == &Acsc, X, f_in.p, c, Y, s);
+            else spmm_dev<float, double>(M, true, f_in.p, c, Y, s);
         }
         SVDB_CUDA(cudaEventRecord(b, s));
         spmm_events.emplace_back(a, b);
@@ -680,6 +683,7 @@ void randomized(const svdb_matrix* A, uint64_t target_rank, uint64_t n_oversampl
     spmm_tma_check();
     spmm_panel_check();
     gram_tc_check();
+    if (split) dense_split_check();
     if (verbose) printf("SVD | Randomized | Jacobi sweeps on R: %d%s\n", hjac >> 8, (hjac & 2) ? " (limit)" : "");
     if (hflags & 2) throw Error(SVDB_ERR_LAS2, "randomized_svd: CholeskyQR broke down even with a shift");
 

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <memory>
 #include <mutex>
 #include <stdexcept>
 #include <string>
@@ -142,6 +143,19 @@ struct DevCompressed {
 // Builds m.plan on stream s (called once per structure, at creation).
 void build_seg_plan(DevCompressed& m, cudaStream_t s);
 
+// Dense-column split of a matrix for the FP32 SpMM (dense_split.cu): the
+// columns J of density above a threshold as a dense block D = A[:, J]
+// (m x ndp FP32, row-major) and its transpose Dt (ndp x mp), and the rest
+// of A without them as a CSR (rest_csr) and a CSR of its transpose with the
+// rows J emptied (rest_csc), each with FP32 values and a segment plan.
+struct DenseSplit {
+    int64_t nd = 0, ndp = 0, mp = 0;  // dense columns; padded to 128; rows padded to 32
+    int64_t dense_nnz = 0;
+    DevBuf<int32_t> cols;             // ndp original column ids, -1 for padding
+    DevBuf<float> D, Dt;
+    DevCompressed rest_csr, rest_csc;
+};
+
 enum MatKind { KIND_CSR = 0, KIND_CSC = 1, KIND_COO = 2, KIND_MASKED = 3 };
 
 }  // namespace svdb
@@ -159,6 +173,9 @@ struct svdb_matrix {
     bool all_columns = false;
     svdb::DevBuf<int64_t> m2o, o2m;
     std::mutex mu;  // serialises calls on one handle
+    // dense-column split of csr/csc for the FP32 SpMM, built on first use
+    std::unique_ptr<svdb::DenseSplit> dense;
+    bool dense_tried = false;
 };
 
 namespace svdb {
@@ -166,6 +183,14 @@ namespace svdb {
 const DevCompressed& csr_of(const svdb_matrix* a);
 const DevCompressed& csc_of(const svdb_matrix* a);
 void ensure_fp32(const svdb_matrix* a);
+// FP32 SpMM through the dense-column split (dense_split.cu): usable when the
+// matrix has enough dense columns and l <= 64 (builds the split on first use).
+bool dense_split_usable(const svdb_matrix* a, int l);
+template <typename XT, typename OT>
+void dense_split_spmm(const svdb_matrix* a, bool transpose, const XT* X, const float* x32, int l, OT* Y,
+                      cudaStream_t s);
+void dense_split_check();  // raises a wait timeout an earlier split SpMM recorded (synchronises)
+void dense_split_info(const svdb_matrix* a, uint64_t* nd, uint64_t* dense_nnz);
 
 struct DeviceProps {
     int sms = 148;

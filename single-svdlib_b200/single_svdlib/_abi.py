@@ -117,6 +117,9 @@ SIGNATURES = {
     "svdb_gram_device": (C.c_int, [vp, u64, u64, vp, C.c_int, vp]),
     "svdb_kernel_launches": (u64, []),
     "svdb_wait_selftest": (C.c_int, [C.c_int, u64]),
+    "svdb_dense_split_info": (C.c_int, [vp, P(u64), P(u64)]),
+    "svdb_tridiag_device": (C.c_int, [C.c_int, u64, vp, vp, vp, vp, vp, vp, u64, P(u64), vp, u64, P(C.c_int),
+                                      P(dbl)]),
     "svdb_opb_device_noalloc": (C.c_int, [vp, vp, vp, C.c_int, vp]),
     "svdb_las2": (C.c_int, [vp, u64, u64, P(dbl), dbl, u32, P(svdb_options), P(svdb_rec)]),
     "svdb_svd": (C.c_int, [vp, P(svdb_rec)]),
