@@ -213,13 +213,13 @@ class Las2Run {
         legacy_ = legacy;
     }
     ~Las2Run() {
+        if (rot_cs_) cudaStreamSynchronize(rot_cs_);  // every copy out of rot_pin_ has finished
         for (int b = 0; b < 2; ++b) {
-            if (rot_ev_[b]) {
-                cudaEventSynchronize(rot_ev_[b]);  // the copy out of rot_pin_[b] has finished
-                cudaEventDestroy(rot_ev_[b]);
-            }
+            if (rot_ev_[b]) cudaEventDestroy(rot_ev_[b]);
+            if (rot_free_[b]) cudaEventDestroy(rot_free_[b]);
             host_result_free(rot_pin_[b]);
         }
+        if (rot_cs_) cudaStreamDestroy(rot_cs_);
     }
     Las2Run(const Las2Run&) = delete;
     Las2Run& operator=(const Las2Run&) = delete;
@@ -251,12 +251,17 @@ class Las2Run {
     int64_t lz_rot_n_ = -1;
     // Z of that T, applied on the stream piece by piece while imtqlb runs
     // (a recorded rotation is final): kRotPiece rotations a piece, packed
-    // into two page-locked buffers in turn
+    // into two page-locked buffers and copied into two device slots in turn,
+    // on a copy stream, so the upload of piece k + 1 overlaps the kernel of
+    // piece k.  rot_ev_[b]: the copy into slot b finished (host buffer b free
+    // again); rot_free_[b]: the kernel that read slot b finished.
     static constexpr size_t kRotPiece = 8192;
     DevBuf<double> zrot_, rot_dcs_;
     DevBuf<int32_t> rot_dil_;
     void* rot_pin_[2] = {nullptr, nullptr};
     cudaEvent_t rot_ev_[2] = {nullptr, nullptr};
+    cudaEvent_t rot_free_[2] = {nullptr, nullptr};
+    cudaStream_t rot_cs_ = nullptr;
     int rot_buf_ = 0;
     int64_t zrot_n_ = -1, zrot_js_ = 0, zrot_js_cur_ = 0;
     size_t rot_done_ = 0;
@@ -281,12 +286,14 @@ class Las2Run {
 void Las2Run::rot_stream_begin(int64_t js) {
     if (!rot_pin_[0]) {
         const size_t bytes = (size_t)rot_padded((int64_t)kRotPiece) * 24;  // (c, s) and (index, length)
+        SVDB_CUDA(cudaStreamCreateWithFlags(&rot_cs_, cudaStreamNonBlocking));
         for (int b = 0; b < 2; ++b) {
             rot_pin_[b] = host_result_alloc(bytes);
             SVDB_CUDA(cudaEventCreateWithFlags(&rot_ev_[b], cudaEventDisableTiming));
+            SVDB_CUDA(cudaEventCreateWithFlags(&rot_free_[b], cudaEventDisableTiming));
         }
-        rot_dcs_.alloc(2 * rot_padded((int64_t)kRotPiece), s_);
-        rot_dil_.alloc(2 * rot_padded((int64_t)kRotPiece), s_);
+        rot_dcs_.alloc(4 * rot_padded((int64_t)kRotPiece), s_);  // two slots of (c, s) pairs
+        rot_dil_.alloc(4 * rot_padded((int64_t)kRotPiece), s_);  // and of (index, length) pairs
     }
     if (js * js > zrot_js_ * zrot_js_) zrot_.alloc(js * js, s_);
     zrot_js_ = std::max(zrot_js_, js);
@@ -308,12 +315,16 @@ void Las2Run::rot_stream_flush(size_t upto) {
     int32_t* pil = reinterpret_cast<int32_t*>(pcs + 2 * rot_padded((int64_t)kRotPiece));
     rot_pack(lz_rot_.i.data() + rot_done_, lz_rot_.c.data() + rot_done_, lz_rot_.s.data() + rot_done_, cnt,
              zrot_js_cur_, pcs, pil);
+    const int64_t slot = (int64_t)b * 2 * rot_padded((int64_t)kRotPiece);
+    SVDB_CUDA(cudaStreamWaitEvent(rot_cs_, rot_free_[b], 0));  // the kernel of two pieces ago read slot b
     if (cnt) {
-        SVDB_CUDA(cudaMemcpyAsync(rot_dcs_.p, pcs, (size_t)cnt * 16, cudaMemcpyHostToDevice, s_));
-        SVDB_CUDA(cudaMemcpyAsync(rot_dil_.p, pil, (size_t)cnt * 8, cudaMemcpyHostToDevice, s_));
+        SVDB_CUDA(cudaMemcpyAsync(rot_dcs_.p + slot, pcs, (size_t)cnt * 16, cudaMemcpyHostToDevice, rot_cs_));
+        SVDB_CUDA(cudaMemcpyAsync(rot_dil_.p + slot, pil, (size_t)cnt * 8, cudaMemcpyHostToDevice, rot_cs_));
     }
-    SVDB_CUDA(cudaEventRecord(rot_ev_[b], s_));
-    rot_apply(zrot_.p, zrot_js_cur_, rot_dcs_.p, rot_dil_.p, cnt, !rot_started_, s_);
+    SVDB_CUDA(cudaEventRecord(rot_ev_[b], rot_cs_));
+    SVDB_CUDA(cudaStreamWaitEvent(s_, rot_ev_[b], 0));
+    rot_apply(zrot_.p, zrot_js_cur_, rot_dcs_.p + slot, rot_dil_.p + slot, cnt, !rot_started_, s_);
+    SVDB_CUDA(cudaEventRecord(rot_free_[b], s_));
     rot_done_ = upto;
     rot_started_ = true;
 }
