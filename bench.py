@@ -602,6 +602,62 @@ ADJ_WORKLOAD = ("truncated-SVD adjoint, 50000x20000 CSR, density 0.5 % uniform p
                 "(tol 1e-10) + SDDMM of rank-2k factors")
 
 
+def adjoint_fd_check(L, C, check, _abi, options, rec_from_c, A, ip64, ix64, k, gU, gs, gV, rng, samples):
+    """Central finite differences of L = <gU, U> + <gs, s> + <gV, V> (U, V sign-fixed
+    by svd_flip, forward LAS2 f64 as above) on `samples` random nonzeros, at steps
+    1e-4 and 1e-6, against the adjoint's gradient at the same point."""
+    from single_svdlib.randomized import svd_flip
+    m, n, nnz = A["nrows"], A["ncols"], len(A["data"])
+
+    def forward(vals):
+        hh = C.c_void_p()
+        check(L.svdb_matrix_create_csr(m, n, nnz, ip64.ctypes.data, ix64.ctypes.data, vals.ctypes.data, C.byref(hh)))
+        try:
+            st, r = _las2_call(L, C, check, _abi, options, hh, k + 8, 0, 42, True, "f64", 0, kappa=1e-10)
+            check(st)
+            rec = rec_from_c(r)
+            L.svdb_rec_free(C.byref(r))
+        finally:
+            L.svdb_matrix_destroy(hh)
+        U, V = svd_flip(np.ascontiguousarray(rec.u[:k].T), np.ascontiguousarray(rec.vt[:k]))
+        return U, rec.s[:k].copy(), V.T
+
+    def loss(vals):
+        U, S, V = forward(vals)
+        return float((gU * U).sum() + (gs * S).sum() + (gV * V).sum())
+
+    U, S, V = forward(A["data"].copy())
+    h = C.c_void_p()
+    check(L.svdb_matrix_create_csr(m, n, nnz, ip64.ctypes.data, ix64.ctypes.data, A["data"].ctypes.data,
+                                   C.byref(h)))
+    o = _abi.svdb_adjoint_options()
+    L.svdb_adjoint_options_default(C.byref(o))
+    o.cg_tol = 1e-12
+    o.cg_max_iters = 50000
+    grad = np.empty(nnz)
+    Uc, Sc, Vc = (np.ascontiguousarray(x) for x in (U, S, V))
+    check(L.svdb_svd_adjoint(h, k, Uc.ctypes.data, Sc.ctypes.data, Vc.ctypes.data, gU.ctypes.data, gs.ctypes.data,
+                             gV.ctypes.data, C.byref(o), grad.ctypes.data))
+    L.svdb_matrix_destroy(h)
+    picks = rng.choice(nnz, samples, replace=False)
+    out = {"samples": int(samples), "cg_iterations": int(o.cg_iterations), "cg_residual": float(o.cg_residual)}
+    t0 = time.perf_counter()
+    for step in (1e-4, 1e-6):
+        fd = []
+        for e in picks:
+            vp = A["data"].copy()
+            vp[e] += step
+            vm = A["data"].copy()
+            vm[e] -= step
+            fd.append((loss(vp) - loss(vm)) / (2 * step))
+        fd = np.array(fd)
+        err = np.abs(fd - grad[picks])
+        out[f"step_{step:g}"] = {"max_rel_err_vs_max_grad": float(err.max() / np.abs(grad[picks]).max()),
+                                 "median_rel_err": float(np.median(err / np.maximum(np.abs(grad[picks]), 1e-300)))}
+    out["seconds"] = time.perf_counter() - t0
+    return out
+
+
 def run_adjoint(args):
     rank, world, local, threads = _env()
     if args.impl == "reference":
@@ -688,12 +744,17 @@ def run_adjoint(args):
         L.svdb_rec_free(C.byref(r))
         L.svdb_matrix_destroy(hh)
     fd_s = time.perf_counter() - t0
+    fd_check = None
+    if args.fd_samples > 0:
+        stage(f"adjoint finite differences on {args.fd_samples} nonzeros")
+        fd_check = adjoint_fd_check(L, C, check, _abi, options, rec_from_c, A, ip64, ix64, k, gU, gs, gV, rng,
+                                    args.fd_samples)
     ms_adj = max_over_ranks(ms_adj, world)
     if rank == 0:
         _line(args, world, "adjoint wall time (s): block-CG complement solves + SDDMM, k=32", ms_adj / 1e3, "f64",
               {"workload": ADJ_WORKLOAD, "nrows": m, "ncols": n, "nnz": nnz, "k": k,
                "parallelism": f"replicas x{world}", "l2": "factors (19 MB FP32) in L2; pattern streamed"},
-              adjoint=info, forward_las2_s=fwd_s, fd_seconds_per_entry=fd_s,
+              adjoint=info, forward_las2_s=fwd_s, fd_seconds_per_entry=fd_s, fd_check=fd_check,
               sddmm_fp32={"ms": ms_sddmm, "nnz_per_s": nnz / (ms_sddmm * 1e-3), "bytes": sddmm_bytes},
               roofline={"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
                         "traffic": None, "kernel": "k_sddmm<float> (rank 64)", "peak_source": peak_kind},
@@ -863,6 +924,8 @@ def main():
     ap.add_argument("--workload", default="randomized",
                     choices=["randomized", "las2", "las2-large", "adjoint", "batch"])
     ap.add_argument("--las2-iterations", type=int, default=0, help="las2-large: Lanczos step cap (0 = the crate's)")
+    ap.add_argument("--fd-samples", type=int, default=0,
+                    help="adjoint: central finite differences on this many random nonzeros (steps 1e-4 and 1e-6)")
     args = ap.parse_args()
     faulthandler.enable()
     if args.workload != "randomized":

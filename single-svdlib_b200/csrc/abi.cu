@@ -295,6 +295,14 @@ int svdb_multiply_with_dense_device(const svdb_matrix* a, const void* d_dense, u
 
 uint64_t svdb_kernel_launches(void) { return g_launches.load(); }
 
+int svdb_sliced_spmv_info(const svdb_matrix* a, int transposed, int32_t* nslices, int32_t* nranges) {
+    return guarded([&] {
+        check_handle(a);
+        if (!nslices || !nranges) throw Error(SVDB_ERR_ARG, "null argument");
+        sliced_info(transposed ? csc_of(a) : csr_of(a), nslices, nranges);
+    });
+}
+
 int svdb_dense_split_info(const svdb_matrix* a, uint64_t* dense_cols, uint64_t* dense_nnz) {
     return guarded([&] {
         check_handle(a);

@@ -10,6 +10,8 @@
 // multiply-then-add, which is what the crate's `y += a * x` computes.
 #include <cooperative_groups.h>
 
+#include <mutex>
+
 #include "lanczos_kernel.cuh"
 #include "spmv.cuh"
 #include "svdb_internal.h"
@@ -27,9 +29,10 @@ __device__ __forceinline__ bool cmp_eq(double a, double b) { return fabs(b - a) 
 // of w3 folded in).  EPI: y = acc + (-rnm) * w2, and returns this thread's
 // share of dot(y, w3).  Only the matrix arrays are read through the
 // non-coherent path: the vectors change between phases of the same launch.
-template <bool FP32, bool SCALE, bool EPI>
+template <bool FP32, bool SCALE, bool EPI, bool SL>
 __device__ __forceinline__ double spmv_rows(const LzOperand& op, const double* x, double rinv, double* y,
-                                            double neg_rnm, const double* w2, const double* w3, double* sh) {
+                                            double neg_rnm, const double* w2, const double* w3, double* sh,
+                                            double* dyn) {
     auto xl = [&](int32_t c) {
         double xv = x[c];
         if (SCALE) xv = mul_rn(xv, rinv);
@@ -45,6 +48,11 @@ __device__ __forceinline__ double spmv_rows(const LzOperand& op, const double* x
             y[r] = acc;
         }
     };
+    if constexpr (SL) {  // x slices in shared memory (spmv.cuh)
+        if (FP32) sliced_rows<float, SCALE>(op.sl, op.svf, x, rinv, dyn, finish);
+        else sliced_rows<double, SCALE>(op.sl, op.sv, x, rinv, dyn, finish);
+        return dotacc;
+    }
     for (int64_t i = blockIdx.x; i < op.nlong; i += gridDim.x) {
         const int64_t r = __ldg(op.long_rows + i);
         const int64_t s = __ldg(op.rp + r), e = __ldg(op.rp + r + 1);
@@ -111,8 +119,9 @@ __device__ __forceinline__ bool lz_sum(double v, double* part, GridBarrier* bar,
     }
 }
 
-template <bool FP32, bool CL>
-__global__ void __launch_bounds__(kThreads, CL ? 1 : 2) k_lanczos_block(const __grid_constant__ LzArgs a) {
+template <bool FP32, bool CL, bool SL = false>
+__global__ void __launch_bounds__(kThreads, (CL || SL) ? 1 : 2) k_lanczos_block(const __grid_constant__ LzArgs a) {
+    extern __shared__ double lz_dyn[];  // SL: the x slice and the row accumulators
     __shared__ double sh[32];
     __shared__ double cl_slot[2], cl_out;
     int par = 0;
@@ -175,7 +184,7 @@ __global__ void __launch_bounds__(kThreads, CL ? 1 : 2) k_lanczos_block(const __
             const double* w4 = WV(4);
             double* w1 = WV(1);
             double* w3s = WV(6);
-            spmv_rows<FP32, true, false>(a.op1, w3, rinv, a.temp, 0.0, nullptr, nullptr, sh);
+            spmv_rows<FP32, true, false, SL>(a.op1, w3, rinv, a.temp, 0.0, nullptr, nullptr, sh, lz_dyn);
             for (int64_t e = tid; e < n; e += nth) {
                 w1[e] = mul_rn(rinv, w0[e]);
                 w3s[e] = mul_rn(w3[e], rinv);
@@ -192,7 +201,7 @@ __global__ void __launch_bounds__(kThreads, CL ? 1 : 2) k_lanczos_block(const __
         // ---- phase 2: w0 = op2 temp - rnm w2; alf[j] = w0 . w3
         double alf_j;
         {
-            double part = spmv_rows<FP32, false, true>(a.op2, a.temp, 1.0, WV(0), -rnm, WV(2), WV(3), sh);
+            double part = spmv_rows<FP32, false, true, SL>(a.op2, a.temp, 1.0, WV(0), -rnm, WV(2), WV(3), sh, lz_dyn);
             if (!lz_sum<CL>(part, a.part, a.bar, sh, cl_slot, &cl_out, par, alf_j)) return;
         }
 
@@ -438,8 +447,35 @@ int lanczos_max_blocks(int threads) {
     return per_sm * device_props().sms;
 }
 
-void launch_lanczos_block(const LzArgs& a, int blocks, int threads, int cluster, cudaStream_t s) {
+// Blocks of the sliced cooperative grid: one per SM (the x slice takes most
+// of the SM's shared memory).
+int lanczos_sliced_blocks(int threads) {
+    static std::once_flag attr;
+    std::call_once(attr, [] {
+        SVDB_CUDA(cudaFuncSetAttribute(k_lanczos_block<false, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       kSlSmem));
+        SVDB_CUDA(cudaFuncSetAttribute(k_lanczos_block<true, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       kSlSmem));
+    });
+    int per_sm = 0, per_sm32 = 0;
+    SVDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lanczos_block<false, false, true>, threads,
+                                                            kSlSmem));
+    SVDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm32, k_lanczos_block<true, false, true>, threads,
+                                                            kSlSmem));
+    per_sm = per_sm < per_sm32 ? per_sm : per_sm32;
+    return per_sm >= 1 ? per_sm * device_props().sms : 0;
+}
+
+void launch_lanczos_block(const LzArgs& a, int blocks, int threads, int cluster, cudaStream_t s, bool sliced) {
     const bool fp32 = a.op1.vf != nullptr;
+    if (sliced) {
+        void* args[] = {(void*)&a};
+        const void* fn = fp32 ? (const void*)k_lanczos_block<true, false, true>
+                              : (const void*)k_lanczos_block<false, false, true>;
+        SVDB_CUDA(cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(threads), args, kSlSmem, s));
+        count_launches(1);
+        return;
+    }
     if (cluster > 0) {  // the whole grid is one cluster of `cluster` blocks
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(cluster);

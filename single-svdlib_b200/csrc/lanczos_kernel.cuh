@@ -4,6 +4,7 @@
 #include <cstdint>
 
 #include "device_common.cuh"
+#include "spmv.cuh"
 #include "svdb_internal.h"
 
 namespace svdb {
@@ -30,6 +31,10 @@ struct LzOperand {
     const int32_t* long_rows;  // rows of more than kSegNnz entries, one block each
     int64_t nlong;
     SpmvBins bins;             // the other rows, by length
+    // the column-sliced copy (sliced launches only, spmv.cuh): its values
+    SlicedOp sl;
+    const double* sv;
+    const float* svf;
 };
 
 struct LzArgs {
@@ -57,7 +62,14 @@ struct LzArgs {
 };
 
 // blocks: a cooperative grid; cluster > 0: one thread-block cluster of that many blocks instead.
-void launch_lanczos_block(const LzArgs& a, int blocks, int threads, int cluster, cudaStream_t s);
+// sliced: both operands carry their column-sliced copy (op.sl), and the grid
+// (one block per SM) stages x slices in kSlSmem bytes of dynamic shared memory.
+void launch_lanczos_block(const LzArgs& a, int blocks, int threads, int cluster, cudaStream_t s, bool sliced = false);
+int lanczos_sliced_blocks(int threads);
+// The column-sliced copy of m (spmv_sliced.cu): built on first use, and its
+// FP32 values when fp32; false when m gets none.  sliced_view: its arrays.
+bool sliced_prepare(const DevCompressed& m, bool fp32, cudaStream_t s);
+SlicedOp sliced_view(const DevCompressed& m);
 int lanczos_max_blocks(int threads);
 bool lanczos_cluster_ok(int cluster, int threads);
 

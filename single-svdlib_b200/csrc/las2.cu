@@ -244,6 +244,7 @@ class Las2Run {
     int eta_sel_ = 0;
     int64_t npurge_ = 0;
     int lz_blocks_ = 0, lz_cluster_ = 0;
+    bool lz_sliced_ = false;  // grid launches use both operands' column-sliced copies
     std::vector<double> alf_h_, bet_h_, ritz_, bnd_, w5_;
     // rotations of lanso's last Ritz analysis when it ran imtqlb (SVDLIBC)
     // on the whole T: ritvec's imtql2 would make the same ones (ql_host.h)
@@ -410,9 +411,17 @@ int64_t Las2Run::lanczos_step(int64_t first, int64_t last, int64_t& ll, bool& en
         LzArgs a;
         std::memset(&a, 0, sizeof a);
         a.op1 = {op1_->ptr.p, op1_->idx.p, op1_->val.p, fp32_ ? op1_->val32.p : nullptr, op1_->nmajor,
-                 op1_->plan.multi_rows.p, op1_->plan.nmulti, op1_->plan.bins};
+                 op1_->plan.multi_rows.p, op1_->plan.nmulti, op1_->plan.bins, SlicedOp{}, nullptr, nullptr};
         a.op2 = {op2_->ptr.p, op2_->idx.p, op2_->val.p, fp32_ ? op2_->val32.p : nullptr, op2_->nmajor,
-                 op2_->plan.multi_rows.p, op2_->plan.nmulti, op2_->plan.bins};
+                 op2_->plan.multi_rows.p, op2_->plan.nmulti, op2_->plan.bins, SlicedOp{}, nullptr, nullptr};
+        if (lz_sliced_) {
+            a.op1.sl = sliced_view(*op1_);
+            a.op1.sv = op1_->sliced.sval.p;
+            a.op1.svf = op1_->sliced.sval32.p;
+            a.op2.sl = sliced_view(*op2_);
+            a.op2.sv = op2_->sliced.sval.p;
+            a.op2.svf = op2_->sliced.sval32.p;
+        }
         a.n = n_;
         for (int k = 0; k < 7; ++k) a.W[k] = W_[k].p;
         a.temp = temp_.p;
@@ -425,7 +434,7 @@ int64_t Las2Run::lanczos_step(int64_t first, int64_t last, int64_t& ll, bool& en
         a.first = j; a.last = last; a.resume = resume ? 1 : 0;
         a.eps1 = EPS * std::sqrt((double)n_);
         a.sqrt_eps = std::sqrt(EPS);
-        launch_lanczos_block(a, lz_blocks_, 512, lz_cluster_, s_);
+        launch_lanczos_block(a, lz_blocks_, 512, lz_cluster_, s_, lz_sliced_);
         GridBarrier hb;
         SVDB_CUDA(cudaMemcpyAsync(&hs, st_.p, sizeof hs, cudaMemcpyDeviceToHost, s_));
         SVDB_CUDA(cudaMemcpyAsync(&hb, bar_.p, sizeof hb, cudaMemcpyDeviceToHost, s_));
@@ -693,6 +702,20 @@ void Las2Run::run(int64_t dimensions, int64_t iterations, double endl, double en
                 if (lanczos_cluster_ok(c, 512)) { lz_cluster_ = c; break; }
         }
         if (lz_cluster_) lz_blocks_ = lz_cluster_;
+    }
+    // Large operators in grid mode: x slices in shared memory for both
+    // products (spmv_sliced.cu), one block per SM (SVDB_SPMV=gather keeps the
+    // gather products).
+    if (!lz_cluster_) {
+        const char* env = getenv("SVDB_SPMV");
+        const bool gather = env && std::string(env) == "gather";
+        if (!gather && sliced_prepare(*op1_, fp32_, s_) && sliced_prepare(*op2_, fp32_, s_)) {
+            const int sb = lanczos_sliced_blocks(512);
+            if (sb > 0) {
+                lz_sliced_ = true;
+                lz_blocks_ = sb;
+            }
+        }
     }
     const int64_t nsplit_max = (n_ + 2047) / 2048;
     part_cap_ = std::max<int64_t>({2 * (int64_t)lz_blocks_, 2 * cap * nsplit_max, 2 * cap});

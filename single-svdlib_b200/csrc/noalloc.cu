@@ -75,8 +75,8 @@ extern "C" int svdb_opb_device_noalloc(const svdb_matrix* a, const double* d_x, 
         if (cur != a->device) throw Error(SVDB_ERR_ARG, "the matrix lives on another device than the current one");
         double* temp = scratch_for_current_device();
         cudaStream_t s = stream ? (cudaStream_t)stream : a->stream;
-        spmv(o1, false, d_x, temp, s);  // temp = A x  (every entry written)
-        spmv(o2, false, temp, d_y, s);  // y = A^T temp
+        spmv(o1, false, d_x, temp, s, false);  // temp = A x  (every entry written); gather kernel, no plan
+        spmv(o2, false, temp, d_y, s, false);  // y = A^T temp
         return SVDB_OK;
     } catch (Error& e) {
         set_last_error(e.what());

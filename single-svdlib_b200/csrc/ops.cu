@@ -3,6 +3,8 @@
 // Gram-Schmidt GEMV pairs for startv (mod.rs:624-628), the ChaCha12 start
 // vector (mod.rs:598-605) and dense transposes.
 #include <algorithm>
+#include <cstdlib>
+#include <string>
 
 #include "device_common.cuh"
 #include "ops.cuh"
@@ -46,6 +48,12 @@ __global__ void __launch_bounds__(256) k_spmv(const int64_t* __restrict__ rp, co
     spmv_binned(rp, ci, v, bins, gwarp, nwarps, xl, [&](int64_t r, double acc) { y[r] = acc; });
 }
 
+// SVDB_SPMV=gather keeps the gather kernel for every operator.
+static bool sliced_off() {
+    const char* e = getenv("SVDB_SPMV");
+    return e && std::string(e) == "gather";
+}
+
 // One resident wave of k_spmv<VT> on the current device.  The occupancy is
 // cached per thread and device, like device_props().
 template <typename VT>
@@ -62,9 +70,10 @@ static int spmv_grid() {
     return per_sm * device_props().sms;
 }
 
-void spmv(const DevCompressed& m, bool fp32, const double* x, double* y, cudaStream_t s) {
+void spmv(const DevCompressed& m, bool fp32, const double* x, double* y, cudaStream_t s, bool allow_sliced) {
     if (m.nmajor == 0) return;
     const bool f = fp32 && m.val32.p;
+    if (allow_sliced && !sliced_off() && spmv_sliced(m, f, x, y, s)) return;
     const int64_t work = std::max<int64_t>(m.plan.bins.items[kSpmvBins] / 8, m.plan.nmulti);
     if (f) {
         const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(work, spmv_grid<float>()));

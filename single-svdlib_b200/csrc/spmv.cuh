@@ -70,4 +70,76 @@ __device__ __forceinline__ void spmv_binned(const int64_t* __restrict__ rp, cons
     }
 }
 
+// ------------------------------------------------- column-sliced SpMV ----
+// Shared by the standalone kernel (spmv_sliced.cu) and the cooperative
+// Lanczos block.  A CTA takes row ranges rg = blockIdx.x, += gridDim.x; for
+// each, every slice of x (scaled by rinv when SCALE) is copied into shared
+// memory and the range's entries of that slice are summed by 8-lane groups
+// into FP64 accumulators in shared memory; FIN(r, sum) is then called once
+// per row (by some thread of the CTA).  `dyn` holds kSlW + kSlRowCap doubles.
+constexpr int kSlW = 20480;       // columns per slice: 160 KB of FP64 x
+constexpr int kSlRowCap = 8192;   // rows per CTA range: 64 KB of FP64 accumulators
+constexpr int kSlG = 8;           // lanes per row
+constexpr int kSlUnroll = 4;
+constexpr int kSlSmem = (kSlW + kSlRowCap) * 8;
+
+struct SlicedOp {
+    int64_t nmajor, nminor;
+    int32_t nslices, nranges;
+    const int64_t* sbase;   // nslices + 1
+    const int32_t* sptr;    // nslices x (nmajor + 1), relative to sbase[s]
+    const uint16_t* sidx;   // column - s * kSlW
+    const int64_t* rstart;  // nranges + 1
+};
+
+template <typename VT, bool SCALE, typename FIN>
+__device__ __forceinline__ void sliced_rows(const SlicedOp& a, const VT* __restrict__ val, const double* x,
+                                            double rinv, double* dyn, FIN fin) {
+    double* xs = dyn;
+    double* yacc = dyn + kSlW;
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int grp = tid / kSlG, sub = tid % kSlG;
+    const int ngrp = nthr / kSlG;
+    for (int64_t rg = blockIdx.x; rg < a.nranges; rg += gridDim.x) {
+        const int64_t r0 = a.rstart[rg], r1 = a.rstart[rg + 1];
+        const int nr = (int)(r1 - r0);
+        for (int i = tid; i < nr; i += nthr) yacc[i] = 0.0;
+        for (int s = 0; s < a.nslices; ++s) {
+            const int64_t c0 = (int64_t)s * kSlW;
+            const int cw = (int)(a.nminor - c0 < kSlW ? a.nminor - c0 : kSlW);
+            __syncthreads();  // every group is done with the previous slice
+            for (int i = tid; i < cw; i += nthr) xs[i] = SCALE ? mul_rn(x[c0 + i], rinv) : x[c0 + i];
+            __syncthreads();
+            const int32_t* pp = a.sptr + (int64_t)s * (a.nmajor + 1);
+            const int64_t base = __ldg(a.sbase + s);
+            for (int64_t r = r0 + grp; r < r1; r += ngrp) {
+                const int64_t b = base + __ldg(pp + r), e = base + __ldg(pp + r + 1);
+                double acc = 0.0;
+                for (int64_t k = b + sub; k < e; k += (int64_t)kSlG * kSlUnroll) {
+                    double vv[kSlUnroll], xv[kSlUnroll];
+#pragma unroll
+                    for (int u = 0; u < kSlUnroll; ++u) {
+                        const int64_t kk = k + (int64_t)u * kSlG;
+                        if (kk < e) {
+                            vv[u] = (double)__ldg(val + kk);
+                            xv[u] = xs[__ldg(a.sidx + kk)];
+                        } else {
+                            vv[u] = 0.0;
+                            xv[u] = 0.0;
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < kSlUnroll; ++u) acc = fma(vv[u], xv[u], acc);
+                }
+#pragma unroll
+                for (int o = kSlG / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+                if (sub == 0) yacc[r - r0] += acc;
+            }
+        }
+        __syncthreads();
+        for (int i = tid; i < nr; i += nthr) fin(r0 + i, yacc[i]);
+        __syncthreads();
+    }
+}
+
 }  // namespace svdb

@@ -126,6 +126,21 @@ struct PanelPlan {
     DevBuf<int64_t> hmulti_first, hmulti_count;
 };
 
+// Column-sliced copy of a structure for the SpMV (spmv_sliced.cu), built on
+// the first product of a large operator: per slice of columns, a CSR over
+// all rows with 16-bit column offsets, and the rows cut into ranges for the
+// CTAs.
+struct SlicedPlan {
+    bool tried = false, usable = false;
+    int32_t nslices = 0, nranges = 0;
+    DevBuf<int64_t> sbase;   // nslices + 1: first entry of each slice
+    DevBuf<int32_t> sptr;    // nslices x (nmajor + 1): row offsets from sbase[s]
+    DevBuf<uint16_t> sidx;   // column minus the slice's first column
+    DevBuf<double> sval;
+    DevBuf<float> sval32;    // made on the first FP32 product
+    DevBuf<int64_t> rstart;  // nranges + 1 row boundaries
+};
+
 struct DevCompressed {
     int64_t nmajor = 0, nminor = 0, nnz = 0;
     DevBuf<int64_t> ptr;
@@ -134,6 +149,7 @@ struct DevCompressed {
     DevBuf<float> val32;  // FP32 copy of val, made on first mixed-precision use
     SegPlan plan;         // built when the handle is created
     PanelPlan panel;      // built on the first panel SpMM
+    SlicedPlan sliced;    // built on the first SpMV of a large operator
     // stream of the handle that owns this structure: buffers made after
     // creation (the panel plan) are allocated, and so freed, on it
     cudaStream_t owner_stream = nullptr;
@@ -210,7 +226,12 @@ uint64_t wait_limit_ns();
 
 // ------------------------------------------------------- kernel entries ----
 // y[r] = sum_k val[k] * x[idx[k]] over the rows of `m` (group-per-row).
-void spmv(const DevCompressed& m, bool fp32, const double* x, double* y, cudaStream_t s);
+// allow_sliced = false keeps the gather kernel (no plan is built: nothing allocated).
+void spmv(const DevCompressed& m, bool fp32, const double* x, double* y, cudaStream_t s, bool allow_sliced = true);
+// The column-sliced SpMV (spmv_sliced.cu); false when m has no sliced plan
+// (small, unsorted within rows, or not enough memory), nothing launched.
+bool spmv_sliced(const DevCompressed& m, bool fp32, const double* x, double* y, cudaStream_t s);
+void sliced_info(const DevCompressed& m, int* nslices, int* nranges);  // 0, 0 without a plan
 
 // Reductions and BLAS-1 (deterministic two-level reductions).
 void dot(const double* x, const double* y, int64_t n, double* d_out, double* scratch, cudaStream_t s);

@@ -118,6 +118,7 @@ SIGNATURES = {
     "svdb_kernel_launches": (u64, []),
     "svdb_wait_selftest": (C.c_int, [C.c_int, u64]),
     "svdb_dense_split_info": (C.c_int, [vp, P(u64), P(u64)]),
+    "svdb_sliced_spmv_info": (C.c_int, [vp, C.c_int, P(i32), P(i32)]),
     "svdb_tridiag_device": (C.c_int, [C.c_int, u64, vp, vp, vp, vp, vp, vp, u64, P(u64), vp, u64, P(C.c_int),
                                       P(dbl)]),
     "svdb_opb_device_noalloc": (C.c_int, [vp, vp, vp, C.c_int, vp]),
