@@ -404,6 +404,12 @@ struct svdb_batch {
     svdb::DevBuf<double> Om64, Y64, Z64, Bt;
     svdb::DevBuf<double> part, G, R1, R2, R3, Ri, Rout, Rtmp, Ur, Vr, sig, U, Vt;
     svdb::DevBuf<int> flags, shifted, jstat;
+    // SVDB_MIXED with a dense-column split of A: the dense columns' share of
+    // every product as one GEMM over all subsets (dense_split.cu); the B
+    // operands of the row and column GEMMs and the column GEMM's tiles
+    const svdb::DenseSplit* dsplit = nullptr;
+    svdb::DevBuf<float> dbh_r, dbl_r, dbh_c, dbl_c;
+    svdb::DevBuf<double> dpart;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     size_t graph_nodes = 0;
@@ -430,7 +436,8 @@ static T* dense_ptr(svdb_batch& B, DevBuf<float>& f, DevBuf<double>& d) {
 // Y_b = A_b X_b with `gs` subsets per row item
 template <typename T>
 static void rows_product(svdb_batch& B, const T* X, T* Y, int gs) {
-    const DevCompressed& A = csr_of(B.A);
+    // with the split: the rest of A here, the dense columns below
+    const DevCompressed& A = B.dsplit ? B.dsplit->rest_csr : csr_of(B.A);
     const int blocks = grid_cap(6);
 #define SVDB_ROWS(GS)                                                                                             \
     case GS:                                                                                                      \
@@ -450,12 +457,17 @@ static void rows_product(svdb_batch& B, const T* X, T* Y, int gs) {
     }
 #undef SVDB_ROWS
     SVDB_CHECK_LAUNCH();
+    if constexpr (std::is_same<T, float>::value) {
+        if (B.dsplit) dense_batch_rows(B.A, X, B.coff.p, B.o2m.p, B.count, (int)B.l, Y, B.dbh_r.p, B.dbl_r.p, B.s);
+    }
 }
 
 // Z_b = A_b^T Y_b
 template <typename T, typename OT>
 static void cols_product(svdb_batch& B, const T* Y, OT* Z) {
-    const DevCompressed& At = csc_of(B.A);
+    // with the split: the rest of A^T here (rows of the dense columns empty,
+    // so their Z rows are written as 0), the dense columns below
+    const DevCompressed& At = B.dsplit ? B.dsplit->rest_csc : csc_of(B.A);
     const int blocks = grid_cap(8);
     if (B.mixed)
         k_b_spmm_cols<float, T, OT, 2><<<blocks, 256, 0, B.s>>>(At.ptr.p, At.idx.p, At.val32.p, B.m, B.m2o.p,
@@ -464,6 +476,11 @@ static void cols_product(svdb_batch& B, const T* Y, OT* Z) {
         k_b_spmm_cols<double, T, OT, 2><<<blocks, 256, 0, B.s>>>(At.ptr.p, At.idx.p, At.val.p, B.m, B.m2o.p,
                                                                  B.coff.p, B.count, (int)B.l, Y, Z);
     SVDB_CHECK_LAUNCH();
+    if constexpr (std::is_same<T, float>::value) {
+        if (B.dsplit)
+            dense_batch_cols<OT>(B.A, Y, B.coff.p, B.o2m.p, B.count, (int)B.l, Z, B.dbh_c.p, B.dbl_c.p, B.dpart.p,
+                                 B.s);
+    }
 }
 
 template <typename T>
@@ -635,6 +652,24 @@ void batch_create(const svdb_matrix* A, const uint64_t* col_off, const uint64_t*
     k_b_o2m<<<dim3(16, (unsigned)count), 256, 0, s>>>(B->m2o.p, B->coff.p, n, B->o2m.p);
     SVDB_CHECK_LAUNCH();
     if (B->mixed) ensure_fp32(A);
+    if (B->mixed && dense_split_usable(A, (int)l)) {
+        const DenseSplit* ds = dense_split_get(A);
+        const size_t ws = dense_batch_workspace(*ds, (int64_t)count, (int)l);
+        size_t free_b = 0, total_b = 0;
+        SVDB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        if (ws < free_b / 2) {
+            const int64_t npad = ((int64_t)count * l + 63) / 64 * 64;
+            B->dbh_r.alloc(npad * ds->ndp, s);
+            B->dbl_r.alloc(npad * ds->ndp, s);
+            B->dbh_c.alloc(npad * ds->mp, s);
+            B->dbl_c.alloc(npad * ds->mp, s);
+            B->dpart.alloc(npad * ds->ndp, s);
+            // the column GEMM's B rows past count * l are never written: zero once
+            SVDB_CUDA(cudaMemsetAsync(B->dbh_c.p, 0, (size_t)npad * ds->mp * sizeof(float), s));
+            SVDB_CUDA(cudaMemsetAsync(B->dbl_c.p, 0, (size_t)npad * ds->mp * sizeof(float), s));
+            B->dsplit = ds;
+        }
+    }
     const int64_t tc = B->total_cols;
     if (B->mixed) {
         B->Om32.alloc(tc * l, s); B->Y32.alloc(count * m * l, s); B->Z32.alloc(tc * l, s);
@@ -755,6 +790,7 @@ void batch_run(svdb_batch* B, svdb_rec* outs) {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     B->last_ms = ms;
+    if (B->dsplit) dense_split_check();
     for (int64_t b = 0; b < B->count; ++b)
         if (flags[b] & 2)
             throw Error(SVDB_ERR_LAS2, "randomized_svd batch: CholeskyQR broke down even with a shift in subset " +

@@ -74,16 +74,24 @@ constexpr uint32_t kDtAcol = 128;
 
 __device__ int g_dense_err;
 
+// Work items: (K split ks, N tile nt, M tile mt).  In a K split the M tiles
+// go in groups of kDtGroup, and a group runs through every N tile before the
+// next group starts, so the group's A tiles and the N tiles in flight stay
+// in L2.  Column g of the product is column g - 64 nt of N tile nt.
+constexpr int kDtGroup = 16;
 struct DtArgs {
-    int64_t rows;     // valid rows of A (output rows in mode 0)
+    int64_t rows;     // valid rows of A (output rows in modes 0 and 2)
     int64_t k_total;  // K extent of A and B
     int64_t k_per;    // K per work item (a multiple of kDtK)
-    int32_t m_tiles, k_splits;
-    int32_t l;        // output columns written (mode 0)
-    int32_t mode;     // 0: out[row * ldo + j] += C; 1: out[((ks * m_tiles * 128) + row) * 64 + j] = C
-    int32_t out_f32;  // mode 0: out holds floats (else doubles)
+    int32_t m_tiles, k_splits, n_tiles;
+    int32_t l;        // mode 0: output columns; mode 2: columns per subset
+    int32_t mode;     // 0: out[row * ldo + g] += C (g < l)
+                      // 1: out[(((ks * n_tiles + nt) * m_tiles * 128) + row) * 64 + j] = C
+                      // 2: out[(b * bm + row) * l + c] += C, g = b l + c (b < bcount): a batch of products
+    int32_t out_f32;  // modes 0 and 2: out holds floats (else doubles)
     void* out;
     int64_t ldo;
+    int64_t bm, bcount;  // mode 2: rows per product block, products
     unsigned long long limit_ns;
 };
 
@@ -209,10 +217,16 @@ __global__ void __launch_bounds__(kDtThreads, 1)
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = s_tmem;
-    const int64_t items = (int64_t)a.m_tiles * a.k_splits;
-    auto item_geom = [&](int64_t it, int64_t& m0, int64_t& kb, int& nst, int& ks) {
-        ks = (int)(it / a.m_tiles);
-        m0 = (it % a.m_tiles) * kDtM;
+    const int64_t per_k = (int64_t)a.m_tiles * a.n_tiles;
+    const int64_t items = per_k * a.k_splits;
+    auto item_geom = [&](int64_t it, int64_t& m0, int64_t& kb, int& nst, int& ks, int& nt) {
+        ks = (int)(it / per_k);
+        const int64_t rem = it - (int64_t)ks * per_k;
+        const int64_t grp = rem / ((int64_t)kDtGroup * a.n_tiles);
+        const int64_t within = rem - grp * kDtGroup * a.n_tiles;
+        const int64_t gsize = min((int64_t)kDtGroup, (int64_t)a.m_tiles - grp * kDtGroup);
+        nt = (int)(within / gsize);
+        m0 = (grp * kDtGroup + (within - (int64_t)nt * gsize)) * kDtM;
         kb = (int64_t)ks * a.k_per;
         const int64_t ke = min(a.k_total, kb + a.k_per);
         nst = (int)((ke - kb + kDtK - 1) / kDtK);
@@ -223,8 +237,8 @@ __global__ void __launch_bounds__(kDtThreads, 1)
         // ------------------------------------------------------- producer --
         for (int64_t it = blockIdx.x; it < items && !*abort; it += gridDim.x) {
             int64_t m0, kb;
-            int nst, ks;
-            item_geom(it, m0, kb, nst, ks);
+            int nst, ks, nt;
+            item_geom(it, m0, kb, nst, ks, nt);
             for (int st = 0; st < nst; ++st, ++issued) {
                 const int s = issued % kDtStages;
                 if (!dt_wait(dt_smem(&bar_empty[s]), ((issued / kDtStages) & 1) ^ 1, a.limit_ns, abort)) break;
@@ -234,8 +248,8 @@ __global__ void __launch_bounds__(kDtThreads, 1)
                              : "memory");
                 const int kx = (int)(kb + (int64_t)st * kDtK);
                 dt_tma(dt_smem(base), &amap, kx, (int)m0, fb);
-                dt_tma(dt_smem(base + kDtAbytes), &bhmap, kx, 0, fb);
-                dt_tma(dt_smem(base + kDtAbytes + kDtBbytes), &blmap, kx, 0, fb);
+                dt_tma(dt_smem(base + kDtAbytes), &bhmap, kx, nt * kDtN, fb);
+                dt_tma(dt_smem(base + kDtAbytes + kDtBbytes), &blmap, kx, nt * kDtN, fb);
             }
         }
         // every copy issued must land before the CTA may exit
@@ -250,8 +264,8 @@ __global__ void __launch_bounds__(kDtThreads, 1)
         bool any = false;
         for (int64_t it = blockIdx.x; it < items && !*abort; it += gridDim.x) {
             int64_t m0, kb;
-            int nst, ks;
-            item_geom(it, m0, kb, nst, ks);
+            int nst, ks, nt;
+            item_geom(it, m0, kb, nst, ks, nt);
             bool ok = true;
             for (int st = 0; st < nst && ok; ++st, ++issued) {
                 const int s = issued % kDtStages, t = issued & 1, b = ch & 1;
@@ -296,7 +310,7 @@ __global__ void __launch_bounds__(kDtThreads, 1)
         uint32_t ch = 0;
         bool pending = false, pending_last = false;
         int64_t pend_m0 = 0;
-        int pend_ks = 0;
+        int pend_ks = 0, pend_nt = 0;
         auto drain = [&]() -> bool {
             const int b = ch & 1;
             if (!dt_wait(dt_smem(&bar_accf[b]), (ch >> 1) & 1, a.limit_ns, abort)) return false;
@@ -315,18 +329,35 @@ __global__ void __launch_bounds__(kDtThreads, 1)
             ++ch;
             if (pending_last) {
                 const int64_t row = pend_m0 + r;
+                const int64_t g0 = (int64_t)pend_nt * kDtN;
                 if (a.mode == 0) {
                     if (row < a.rows) {
+                        const int jn = (int)min((int64_t)kDtN, (int64_t)a.l - g0);
                         if (a.out_f32) {
-                            float* o = static_cast<float*>(a.out) + row * a.ldo;
-                            for (int j = 0; j < a.l; ++j) o[j] = (float)((double)o[j] + sacc[j * kDtM + r]);
+                            float* o = static_cast<float*>(a.out) + row * a.ldo + g0;
+                            for (int j = 0; j < jn; ++j) o[j] = (float)((double)o[j] + sacc[j * kDtM + r]);
                         } else {
-                            double* o = static_cast<double*>(a.out) + row * a.ldo;
-                            for (int j = 0; j < a.l; ++j) o[j] += sacc[j * kDtM + r];
+                            double* o = static_cast<double*>(a.out) + row * a.ldo + g0;
+                            for (int j = 0; j < jn; ++j) o[j] += sacc[j * kDtM + r];
+                        }
+                    }
+                } else if (a.mode == 2) {
+                    if (row < a.rows) {
+                        for (int j = 0; j < kDtN; ++j) {
+                            const int64_t g = g0 + j, b = g / a.l, c = g - b * a.l;
+                            if (b >= a.bcount) break;
+                            const int64_t at = (b * a.bm + row) * a.l + c;
+                            if (a.out_f32) {
+                                float* o = static_cast<float*>(a.out);
+                                o[at] = (float)((double)o[at] + sacc[j * kDtM + r]);
+                            } else {
+                                static_cast<double*>(a.out)[at] += sacc[j * kDtM + r];
+                            }
                         }
                     }
                 } else {
-                    double* o = static_cast<double*>(a.out) + (((int64_t)pend_ks * a.m_tiles * kDtM) + row) * kDtN;
+                    double* o = static_cast<double*>(a.out) +
+                                ((((int64_t)pend_ks * a.n_tiles + pend_nt) * a.m_tiles * kDtM) + row) * kDtN;
                     for (int j = 0; j < kDtN; ++j) o[j] = sacc[j * kDtM + r];
                 }
                 for (int j = 0; j < kDtN; ++j) sacc[j * kDtM + r] = 0.0;
@@ -337,8 +368,8 @@ __global__ void __launch_bounds__(kDtThreads, 1)
         bool ok = true;
         for (int64_t it = blockIdx.x; it < items && ok && !*abort; it += gridDim.x) {
             int64_t m0, kb;
-            int nst, ks;
-            item_geom(it, m0, kb, nst, ks);
+            int nst, ks, nt;
+            item_geom(it, m0, kb, nst, ks, nt);
             for (int st = 0; st < nst; ++st, ++issued) {
                 const int s = issued % kDtStages, t = issued & 1;
                 if (!dt_wait(dt_smem(&bar_full[s]), (issued / kDtStages) & 1, a.limit_ns, abort)) { ok = false; break; }
@@ -372,6 +403,7 @@ __global__ void __launch_bounds__(kDtThreads, 1)
                     pending_last = (st == nst - 1);
                     pend_m0 = m0;
                     pend_ks = ks;
+                    pend_nt = nt;
                 }
             }
         }
@@ -545,29 +577,45 @@ static int dt_grid(int64_t items) {
     return (int)std::max<int64_t>(1, std::min<int64_t>(items, device_props().sms));
 }
 
-static void dt_launch(const float* A, int64_t a_rows, int64_t a_cols, const float* bh, const float* bl,
-                      int64_t k_per, int ksplits, int l, int mode, bool out_f32, void* out, int64_t ldo,
-                      cudaStream_t s) {
+// C = A (a_rows x a_cols) . B^T with B (n_tiles * 64 rows x a_cols) given as
+// its TF32 head bh and remainder bl; see DtArgs for the modes.
+struct DtLaunch {
+    const float* A;
+    int64_t a_rows, a_cols;
+    const float *bh, *bl;
+    int n_tiles = 1;
+    int64_t k_per = 0;
+    int ksplits = 1;
+    int l = 0, mode = 0;
+    bool out_f32 = false;
+    void* out = nullptr;
+    int64_t ldo = 0, bm = 0, bcount = 0;
+};
+
+static void dt_launch(const DtLaunch& p, cudaStream_t s) {
     static std::once_flag attr;
     std::call_once(attr, [] {
         SVDB_CUDA(cudaFuncSetAttribute(k_dense_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kDtSmem));
     });
-    const CUtensorMap am = dt_map(A, a_cols, a_rows, kDtM);
-    const CUtensorMap hm = dt_map(bh, a_cols, kDtN, kDtN);
-    const CUtensorMap lm = dt_map(bl, a_cols, kDtN, kDtN);
+    const CUtensorMap am = dt_map(p.A, p.a_cols, p.a_rows, kDtM);
+    const CUtensorMap hm = dt_map(p.bh, p.a_cols, (int64_t)p.n_tiles * kDtN, kDtN);
+    const CUtensorMap lm = dt_map(p.bl, p.a_cols, (int64_t)p.n_tiles * kDtN, kDtN);
     DtArgs g;
-    g.rows = a_rows;
-    g.k_total = a_cols;
-    g.k_per = k_per;
-    g.m_tiles = (int)((a_rows + kDtM - 1) / kDtM);
-    g.k_splits = ksplits;
-    g.l = l;
-    g.mode = mode;
-    g.out_f32 = out_f32 ? 1 : 0;
-    g.out = out;
-    g.ldo = ldo;
+    g.rows = p.a_rows;
+    g.k_total = p.a_cols;
+    g.k_per = p.k_per ? p.k_per : p.a_cols;
+    g.m_tiles = (int)((p.a_rows + kDtM - 1) / kDtM);
+    g.k_splits = p.ksplits;
+    g.n_tiles = p.n_tiles;
+    g.l = p.l;
+    g.mode = p.mode;
+    g.out_f32 = p.out_f32 ? 1 : 0;
+    g.out = p.out;
+    g.ldo = p.ldo;
+    g.bm = p.bm;
+    g.bcount = p.bcount;
     g.limit_ns = wait_limit_ns();
-    const int64_t items = (int64_t)g.m_tiles * ksplits;
+    const int64_t items = (int64_t)g.m_tiles * p.ksplits * p.n_tiles;
     k_dense_tc<<<dt_grid(items), kDtThreads, kDtSmem, s>>>(am, hm, lm, g);
     SVDB_CHECK_LAUNCH();
 }
@@ -722,7 +770,13 @@ void dense_split_spmm(const svdb_matrix* a, bool transpose, const XT* X, const f
         k_dense_b_gather<XT><<<(int)nblocks(kDtN * ds->ndp, 256), 256, 0, s>>>(X, l, ds->cols.p, ds->ndp, bh.p,
                                                                                bl.p);
         SVDB_CHECK_LAUNCH();
-        dt_launch(ds->D.p, m, ds->ndp, bh.p, bl.p, ds->ndp, 1, l, 0, of32, Y, l, s);
+        DtLaunch p{ds->D.p, m, ds->ndp, bh.p, bl.p};
+        p.l = l;
+        p.mode = 0;
+        p.out_f32 = of32;
+        p.out = Y;
+        p.ldo = l;
+        dt_launch(p, s);
     } else {
         spmm_dev<float, OT>(ds->rest_csc, true, x32, l, Y, s);  // dense rows written as 0
         DevBuf<float> bh((size_t)kDtN * ds->mp, s), bl((size_t)kDtN * ds->mp, s);
@@ -734,7 +788,13 @@ void dense_split_spmm(const svdb_matrix* a, bool transpose, const XT* X, const f
         const int64_t k_per = ((ds->mp + ks - 1) / ks + kDtK - 1) / kDtK * kDtK;
         ks = (int)((ds->mp + k_per - 1) / k_per);
         DevBuf<double> part((size_t)ks * ds->ndp * kDtN, s);
-        dt_launch(ds->Dt.p, ds->ndp, ds->mp, bh.p, bl.p, k_per, ks, l, 1, false, part.p, kDtN, s);
+        DtLaunch p{ds->Dt.p, ds->ndp, ds->mp, bh.p, bl.p};
+        p.k_per = k_per;
+        p.ksplits = ks;
+        p.l = l;
+        p.mode = 1;
+        p.out = part.p;
+        dt_launch(p, s);
         k_dense_reduce<OT><<<(int)nblocks(ds->nd * l, 256), 256, 0, s>>>(part.p, ks, ds->ndp, ds->nd, ds->cols.p, l,
                                                                           Y);
         SVDB_CHECK_LAUNCH();
@@ -745,5 +805,131 @@ template void dense_split_spmm<double, double>(const svdb_matrix*, bool, const d
                                                cudaStream_t);
 template void dense_split_spmm<float, float>(const svdb_matrix*, bool, const float*, const float*, int, float*,
                                              cudaStream_t);
+
+// ------------------------------------------------ batches of subsets --
+// The products of a batch of column subsets (batch.cu) through the split:
+// every subset's share of the dense columns in one GEMM whose N dimension is
+// all subsets' sample columns side by side (g = b l + c).  The sparse rest
+// runs through the batch's own gather kernels on split->rest_csr/rest_csc.
+
+// B of the row products: head / remainder of X_b[o2m_b(J[k]), c] for row
+// g = b l + c (zero when column J[k] is not in subset b, for padding columns,
+// and for g >= count l); X_b sits at X + coff[b] l.
+__global__ void k_bd_rows_b(const float* __restrict__ X, const int64_t* __restrict__ coff,
+                            const int32_t* __restrict__ o2m, const int32_t* __restrict__ cols, int64_t n,
+                            int64_t count, int l, int64_t ndp, int64_t npad, float* __restrict__ bh,
+                            float* __restrict__ bl) {
+    const int64_t total = npad * ndp;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t g = i / ndp, k = i - g * ndp;
+        const int64_t b = g / l, c = g - b * l;
+        double x = 0.0;
+        if (b < count && cols[k] >= 0) {
+            const int32_t o = o2m[b * n + cols[k]];
+            if (o >= 0) x = (double)X[(coff[b] + o) * l + c];
+        }
+        const float h = tf32_head((float)x);
+        bh[i] = h;
+        bl[i] = (float)(x - (double)h);
+    }
+}
+
+// B of the column products: head / remainder of Y_b[k, c] (Y_b at Y + b m l)
+// for row g = b l + c, zero past m; 32 x 32 tiles per subset.
+__global__ void k_bd_cols_b(const float* __restrict__ Y, int64_t m, int l, int64_t mp, float* __restrict__ bh,
+                            float* __restrict__ bl) {
+    __shared__ float tile[32][33];
+    const int64_t b = blockIdx.z;
+    const int64_t k0 = (int64_t)blockIdx.x * 32;
+    const int c0 = blockIdx.y * 32;
+    const float* Yb = Y + b * m * l;
+    for (int rr = threadIdx.y; rr < 32; rr += blockDim.y) {
+        const int64_t k = k0 + rr;
+        const int c = c0 + threadIdx.x;
+        tile[rr][threadIdx.x] = (k < m && c < l) ? Yb[k * l + c] : 0.f;
+    }
+    __syncthreads();
+    for (int cc = threadIdx.y; cc < 32; cc += blockDim.y) {
+        const int c = c0 + cc;
+        const int64_t k = k0 + threadIdx.x;
+        if (c < l && k < mp) {
+            const double x = (double)tile[threadIdx.x][cc];
+            const float h = tf32_head((float)x);
+            const int64_t at = (b * l + c) * mp + k;
+            bh[at] = h;
+            bl[at] = (float)(x - (double)h);
+        }
+    }
+}
+
+// Z_b[o2m_b(J[k]), c] = the GEMM's tile value for (row k, column b l + c)
+template <typename OT>
+__global__ void k_bd_reduce(const double* __restrict__ part, int64_t ndp, const int32_t* __restrict__ cols,
+                            int64_t nd, const int32_t* __restrict__ o2m, const int64_t* __restrict__ coff, int64_t n,
+                            int64_t count, int l, OT* __restrict__ Z) {
+    const int64_t total = count * nd * l;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t b = i / (nd * l);
+        const int64_t rem = i - b * nd * l;
+        const int64_t k = rem / l, c = rem - k * l;
+        const int32_t o = o2m[b * n + cols[k]];
+        if (o < 0) continue;
+        const int64_t g = b * l + c, nt = g / kDtN, j = g - nt * kDtN;
+        Z[(coff[b] + o) * l + c] = (OT)part[(nt * ndp + k) * kDtN + j];
+    }
+}
+
+const DenseSplit* dense_split_get(const svdb_matrix* a) { return dense_split_for(a); }
+
+size_t dense_batch_workspace(const DenseSplit& ds, int64_t count, int l) {
+    const int64_t npad = (count * l + kDtN - 1) / kDtN * kDtN;
+    return (size_t)npad * (size_t)(ds.ndp + ds.mp) * 2 * sizeof(float) + (size_t)npad * ds.ndp * sizeof(double);
+}
+
+void dense_batch_rows(const svdb_matrix* a, const float* X, const int64_t* coff, const int32_t* o2m, int64_t count,
+                      int l, float* Y, float* bh, float* bl, cudaStream_t s) {
+    const DenseSplit* ds = dense_split_for(a);
+    if (!ds) throw Error(SVDB_ERR_ARG, "dense split: not available for this matrix");
+    const int64_t m = ds->rest_csr.nmajor, n = ds->rest_csr.nminor;
+    const int64_t npad = (count * l + kDtN - 1) / kDtN * kDtN;
+    k_bd_rows_b<<<(int)nblocks(npad * ds->ndp, 256), 256, 0, s>>>(X, coff, o2m, ds->cols.p, n, count, l, ds->ndp,
+                                                                   npad, bh, bl);
+    SVDB_CHECK_LAUNCH();
+    DtLaunch p{ds->D.p, m, ds->ndp, bh, bl};
+    p.n_tiles = (int)(npad / kDtN);
+    p.l = l;
+    p.mode = 2;
+    p.out_f32 = true;
+    p.out = Y;
+    p.bm = m;
+    p.bcount = count;
+    dt_launch(p, s);
+}
+
+template <typename OT>
+void dense_batch_cols(const svdb_matrix* a, const float* Y, const int64_t* coff, const int32_t* o2m, int64_t count,
+                      int l, OT* Z, float* bh, float* bl, double* part, cudaStream_t s) {
+    const DenseSplit* ds = dense_split_for(a);
+    if (!ds) throw Error(SVDB_ERR_ARG, "dense split: not available for this matrix");
+    const int64_t m = ds->rest_csr.nmajor, n = ds->rest_csr.nminor;
+    const int64_t npad = (count * l + kDtN - 1) / kDtN * kDtN;
+    dim3 tb(32, 8), tg((unsigned)(ds->mp / 32), (unsigned)((l + 31) / 32), (unsigned)count);
+    k_bd_cols_b<<<tg, tb, 0, s>>>(Y, m, l, ds->mp, bh, bl);
+    SVDB_CHECK_LAUNCH();
+    DtLaunch p{ds->Dt.p, ds->ndp, ds->mp, bh, bl};
+    p.n_tiles = (int)(npad / kDtN);
+    p.l = l;
+    p.mode = 1;
+    p.out = part;
+    dt_launch(p, s);
+    k_bd_reduce<OT><<<(int)nblocks(count * ds->nd * l, 256), 256, 0, s>>>(part, ds->ndp, ds->cols.p, ds->nd, o2m, coff,
+                                                                          n, count, l, Z);
+    SVDB_CHECK_LAUNCH();
+}
+
+template void dense_batch_cols<float>(const svdb_matrix*, const float*, const int64_t*, const int32_t*, int64_t, int,
+                                      float*, float*, float*, double*, cudaStream_t);
+template void dense_batch_cols<double>(const svdb_matrix*, const float*, const int64_t*, const int32_t*, int64_t, int,
+                                       double*, float*, float*, double*, cudaStream_t);
 
 }  // namespace svdb

@@ -207,6 +207,19 @@ void dense_split_spmm(const svdb_matrix* a, bool transpose, const XT* X, const f
                       cudaStream_t s);
 void dense_split_check();  // raises a wait timeout an earlier split SpMM recorded (synchronises)
 void dense_split_info(const svdb_matrix* a, uint64_t* nd, uint64_t* dense_nnz);
+// Batches of column subsets through the split (dense_split.cu): the split of
+// a (built on first use; null without one), the device workspace the two
+// products need for count subsets of l columns (the B operands of both GEMMs
+// and the partial tiles), and the products' dense parts: Y (count x m x l)
+// += the dense columns' share of A_b X_b (X_b at X + coff[b] l), and
+// Z_b rows of the dense columns = A_b^T Y_b there.
+const DenseSplit* dense_split_get(const svdb_matrix* a);
+size_t dense_batch_workspace(const DenseSplit& ds, int64_t count, int l);
+void dense_batch_rows(const svdb_matrix* a, const float* X, const int64_t* coff, const int32_t* o2m, int64_t count,
+                      int l, float* Y, float* bh, float* bl, cudaStream_t s);
+template <typename OT>
+void dense_batch_cols(const svdb_matrix* a, const float* Y, const int64_t* coff, const int32_t* o2m, int64_t count,
+                      int l, OT* Z, float* bh, float* bl, double* part, cudaStream_t s);
 
 struct DeviceProps {
     int sms = 148;

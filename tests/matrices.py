@@ -139,3 +139,16 @@ def zipf_planted_device(torch, m=1_000_000, n=200_000, seed=3):
         vals[c0:c1] += (u[rows[c0:c1]] * v[cols[c0:c1].long()] * sig).sum(1)
     del rows, u, v
     return indptr, cols, vals
+
+
+def dense_columns(m, n, nd, seed, dens=(0.05, 0.4), rest=0.004):
+    """nd columns of densities uniform in `dens`, the others of density `rest`;
+    values log1p(Poisson(3) + 1): a matrix with a dense-column split."""
+    rng = np.random.default_rng(seed)
+    dcols = rng.choice(n, nd, replace=False)
+    p = np.full(n, rest)
+    p[dcols] = rng.uniform(dens[0], dens[1], nd)
+    mask = rng.random((m, n)) < p[None, :]
+    r, c = np.nonzero(mask)
+    v = np.log1p(rng.poisson(3.0, len(r)) + 1.0)
+    return from_scipy(sp.csr_matrix((v, (r, c)), shape=(m, n)))

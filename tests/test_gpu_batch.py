@@ -97,3 +97,27 @@ def test_batch_uneven_subsets_and_csc_parent():
     for cols, g in zip(subs[:5], got[:5]):
         ref = single(A, upload("csr", A), cols, 10, 10, 1, PIN.QR, 5, "f64")
         np.testing.assert_allclose(g.s, ref.s, rtol=1e-10)
+
+
+def test_batch_dense_split_against_gather_and_f64(monkeypatch):
+    """Under SVDB_MIXED the dense columns of every subset go through one GEMM
+    over all subsets (the dense-column split); the rest through the batch's
+    gathers.  Against the same batch with the split off and single FP64 calls."""
+    import ctypes as C
+    A = M.dense_columns(5000, 2400, 300, 17)
+    subs = subsets_of(2400, 9, 150, 2000, 6)
+    rank, over, q, seed = 12, 8, 2, 4
+    h = upload("csr", A)
+    got = randomized.randomized_svd_batch(h, subs, rank, over, q, PIN.QR, seed, precision="mixed")
+    nd, nnz = C.c_uint64(0), C.c_uint64(0)
+    assert _abi.lib().svdb_dense_split_info(h.handle, C.byref(nd), C.byref(nnz)) == 0
+    assert nd.value == 300 and nnz.value > 0
+    monkeypatch.setenv("SVDB_DENSE_SPLIT", "0")
+    h2 = upload("csr", A)
+    gat = randomized.randomized_svd_batch(h2, subs, rank, over, q, PIN.QR, seed, precision="mixed")
+    assert _abi.lib().svdb_dense_split_info(h2.handle, C.byref(nd), C.byref(nnz)) == 0 and nd.value == 0
+    monkeypatch.delenv("SVDB_DENSE_SPLIT")
+    for cols, g, r in list(zip(subs, got, gat))[:4]:
+        ref = single(A, h2, cols, rank, over, q, PIN.QR, seed, "f64")
+        assert np.max(np.abs(g.s - ref.s) / ref.s) < 1e-6
+        assert np.max(np.abs(r.s - ref.s) / ref.s) < 1e-6
