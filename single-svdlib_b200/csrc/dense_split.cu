@@ -178,6 +178,13 @@ __device__ __forceinline__ float tf32_head(float x) {
     asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
     return __uint_as_float(r);
 }
+// The remainder of a 3xTF32 split, itself rounded to TF32.  The tensor cores
+// read an FP32 operand as TF32 by dropping its low 13 bits; left to them the
+// remainder would be truncated, an error of one sign that does not cancel
+// in long sums of terms of both signs (it cost a factor of about 100 in the
+// singular values of a randomized solve).  Rounded here, the operand is
+// exactly TF32 and the error is a rounding error.
+__device__ __forceinline__ float tf32_tail(double x, float head) { return tf32_head((float)(x - (double)head)); }
 
 __global__ void __launch_bounds__(kDtThreads, 1)
     k_dense_tc(const __grid_constant__ CUtensorMap amap, const __grid_constant__ CUtensorMap bhmap,
@@ -383,7 +390,7 @@ __global__ void __launch_bounds__(kDtThreads, 1)
                     for (int e = 0; e < 4; ++e) {
                         const float h = tf32_head(xs[e]);
                         hi[q * 4 + e] = __float_as_uint(h);
-                        lo[q * 4 + e] = __float_as_uint(xs[e] - h);
+                        lo[q * 4 + e] = __float_as_uint(tf32_head(xs[e] - h));
                     }
                 }
                 __syncwarp();
@@ -431,7 +438,7 @@ __global__ void k_dense_b_gather(const XT* __restrict__ X, int l, const int32_t*
         const double x = (j < l && c >= 0) ? (double)X[(int64_t)c * l + j] : 0.0;
         const float h = tf32_head((float)x);
         bh[i] = h;
-        bl[i] = (float)(x - (double)h);
+        bl[i] = tf32_tail(x, h);
     }
 }
 
@@ -456,7 +463,7 @@ __global__ void k_dense_b_transpose(const XT* __restrict__ Y, int64_t rows, int 
             const double x = tile[threadIdx.x][jj];
             const float h = tf32_head((float)x);
             bh[(int64_t)j * kp + k] = h;
-            bl[(int64_t)j * kp + k] = (float)(x - (double)h);
+            bl[(int64_t)j * kp + k] = tf32_tail(x, h);
         }
     }
 }
@@ -830,7 +837,7 @@ __global__ void k_bd_rows_b(const float* __restrict__ X, const int64_t* __restri
         }
         const float h = tf32_head((float)x);
         bh[i] = h;
-        bl[i] = (float)(x - (double)h);
+        bl[i] = tf32_tail(x, h);
     }
 }
 
@@ -857,7 +864,7 @@ __global__ void k_bd_cols_b(const float* __restrict__ Y, int64_t m, int l, int64
             const float h = tf32_head((float)x);
             const int64_t at = (b * l + c) * mp + k;
             bh[at] = h;
-            bl[at] = (float)(x - (double)h);
+            bl[at] = tf32_tail(x, h);
         }
     }
 }

@@ -98,8 +98,10 @@ __device__ __forceinline__ void sliced_rows(const SlicedOp& a, const VT* __restr
     double* xs = dyn;
     double* yacc = dyn + kSlW;
     const int tid = threadIdx.x, nthr = blockDim.x;
-    const int grp = tid / kSlG, sub = tid % kSlG;
-    const int ngrp = nthr / kSlG;
+    const int warp = tid >> 5, sub = tid % kSlG;
+    const int wrow = (tid & 31) / kSlG;  // the warp's rows: 32 / kSlG at a time
+    constexpr int kRowsPerWarp = 32 / kSlG;
+    const int nwarp = nthr >> 5;
     for (int64_t rg = blockIdx.x; rg < a.nranges; rg += gridDim.x) {
         const int64_t r0 = a.rstart[rg], r1 = a.rstart[rg + 1];
         const int nr = (int)(r1 - r0);
@@ -112,8 +114,12 @@ __device__ __forceinline__ void sliced_rows(const SlicedOp& a, const VT* __restr
             __syncthreads();
             const int32_t* pp = a.sptr + (int64_t)s * (a.nmajor + 1);
             const int64_t base = __ldg(a.sbase + s);
-            for (int64_t r = r0 + grp; r < r1; r += ngrp) {
-                const int64_t b = base + __ldg(pp + r), e = base + __ldg(pp + r + 1);
+            // the loop is uniform over the warp (every lane takes every trip), so
+            // the full-mask shuffles below always see all 32 lanes
+            for (int64_t rb = r0 + (int64_t)warp * kRowsPerWarp; rb < r1; rb += (int64_t)nwarp * kRowsPerWarp) {
+                const int64_t r = rb + wrow;
+                const bool valid = r < r1;
+                const int64_t b = valid ? base + __ldg(pp + r) : 0, e = valid ? base + __ldg(pp + r + 1) : 0;
                 double acc = 0.0;
                 for (int64_t k = b + sub; k < e; k += (int64_t)kSlG * kSlUnroll) {
                     double vv[kSlUnroll], xv[kSlUnroll];
@@ -133,7 +139,7 @@ __device__ __forceinline__ void sliced_rows(const SlicedOp& a, const VT* __restr
                 }
 #pragma unroll
                 for (int o = kSlG / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-                if (sub == 0) yacc[r - r0] += acc;
+                if (valid && sub == 0) yacc[r - r0] += acc;
             }
         }
         __syncthreads();
