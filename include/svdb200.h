@@ -312,14 +312,14 @@ int svdb_tridiag_device(int routine, uint64_t n, double* d, double* e, double* b
 int svdb_wait_selftest(int which, uint64_t limit_ns);
 
 /* The column-sliced SpMV of one orientation of this matrix (transposed = 1:
- * A^T x), with no counterpart in the reference: operators of at least 2^22
- * nonzeros and more than 20,480 columns whose column indices do not fall
- * within a row get, on their first SpMV (svdb_opa, svdb_opb, LAS2's host-
- * driven products), a copy of their entries grouped by slices of 20,480
- * columns, and the product stages each slice of x in shared memory instead
- * of gathering it from L2 at every nonzero.  Reports the slices and the CTA
- * row ranges, 0 and 0 when the operator has no such plan (SVDB_SPMV=gather
- * keeps the gather kernel). */
+ * A^T x), with no counterpart in the reference.  Opt-in: with the environment
+ * variable SVDB_SPMV=sliced, operators of at least 2^22 nonzeros and more
+ * than 18,432 columns whose column indices do not fall within a row get, on
+ * their first SpMV (svdb_opa, svdb_opb, LAS2's products), a copy of their
+ * entries grouped by slices of 18,432 columns, and the product stages each
+ * slice of x in shared memory instead of gathering it from L2 at every
+ * nonzero.  Reports the slices and the CTA row ranges, 0 and 0 when the
+ * operator has no such plan. */
 int svdb_sliced_spmv_info(const svdb_matrix* a, int transposed, int32_t* nslices, int32_t* nranges);
 
 /* The dense-column split the FP32 products (SVDB_MIXED) of this matrix use,

@@ -708,8 +708,8 @@ void Las2Run::run(int64_t dimensions, int64_t iterations, double endl, double en
     // gather products).
     if (!lz_cluster_) {
         const char* env = getenv("SVDB_SPMV");
-        const bool gather = env && std::string(env) == "gather";
-        if (!gather && sliced_prepare(*op1_, fp32_, s_) && sliced_prepare(*op2_, fp32_, s_)) {
+        const bool sliced = env && std::string(env) == "sliced";  // opt-in, as in spmv()
+        if (sliced && sliced_prepare(*op1_, fp32_, s_) && sliced_prepare(*op2_, fp32_, s_)) {
             const int sb = lanczos_sliced_blocks(512);
             if (sb > 0) {
                 lz_sliced_ = true;

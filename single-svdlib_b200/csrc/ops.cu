@@ -48,10 +48,12 @@ __global__ void __launch_bounds__(256) k_spmv(const int64_t* __restrict__ rp, co
     spmv_binned(rp, ci, v, bins, gwarp, nwarps, xl, [&](int64_t r, double acc) { y[r] = acc; });
 }
 
-// SVDB_SPMV=gather keeps the gather kernel for every operator.
+// The column-sliced kernel is opt-in (SVDB_SPMV=sliced): on the 1M x 200k
+// LAS2 matrix its short per-slice row pieces left it slower than the gather
+// kernel (2.2 against 0.94 ms for A x).
 static bool sliced_off() {
     const char* e = getenv("SVDB_SPMV");
-    return e && std::string(e) == "gather";
+    return !(e && std::string(e) == "sliced");
 }
 
 // One resident wave of k_spmv<VT> on the current device.  The occupancy is

@@ -74,14 +74,20 @@ __device__ __forceinline__ void spmv_binned(const int64_t* __restrict__ rp, cons
 // Shared by the standalone kernel (spmv_sliced.cu) and the cooperative
 // Lanczos block.  A CTA takes row ranges rg = blockIdx.x, += gridDim.x; for
 // each, every slice of x (scaled by rinv when SCALE) is copied into shared
-// memory and the range's entries of that slice are summed by 8-lane groups
-// into FP64 accumulators in shared memory; FIN(r, sum) is then called once
-// per row (by some thread of the CTA).  `dyn` holds kSlW + kSlRowCap doubles.
-constexpr int kSlW = 20480;       // columns per slice: 160 KB of FP64 x
-constexpr int kSlRowCap = 8192;   // rows per CTA range: 64 KB of FP64 accumulators
-constexpr int kSlG = 8;           // lanes per row
+// memory and the range's entries of that slice are summed into FP64
+// accumulators in shared memory; FIN(r, sum) is then called once per row (by
+// some thread of the CTA).  In a slice a row's piece is short (tens of
+// entries), so each thread takes whole rows and keeps four loads in flight;
+// pieces longer than kSlLong entries are listed in shared memory (room for
+// every row of the range, so the choice never depends on timing) and taken by
+// whole warps afterwards.  Which path a piece takes depends only on its
+// length, and every accumulator gets one sum per slice in slice order, so the
+// product is deterministic.  `dyn` holds kSlSmem bytes.
+constexpr int kSlW = 18432;        // columns per slice: 144 KB of FP64 x
+constexpr int kSlRowCap = 8192;    // rows per CTA range: 64 KB of FP64 accumulators
+constexpr int kSlLong = 128;       // a longer piece of a row is summed by a warp
 constexpr int kSlUnroll = 4;
-constexpr int kSlSmem = (kSlW + kSlRowCap) * 8;
+constexpr int kSlSmem = (kSlW + kSlRowCap) * 8 + kSlRowCap * 2 + 16;  // + the long-piece list
 
 struct SlicedOp {
     int64_t nmajor, nminor;
@@ -92,16 +98,39 @@ struct SlicedOp {
     const int64_t* rstart;  // nranges + 1
 };
 
+// sum of val[k] * xs[idx[k]] over k = k0, k0 + step, ... < e, four chains
+template <typename VT>
+__device__ __forceinline__ double sliced_piece(const VT* __restrict__ val, const uint16_t* __restrict__ idx,
+                                               const double* xs, int64_t k0, int64_t e, int step) {
+    double acc = 0.0;
+    for (int64_t k = k0; k < e; k += (int64_t)step * kSlUnroll) {
+        double vv[kSlUnroll], xv[kSlUnroll];
+#pragma unroll
+        for (int u = 0; u < kSlUnroll; ++u) {
+            const int64_t kk = k + (int64_t)u * step;
+            if (kk < e) {
+                vv[u] = (double)__ldg(val + kk);
+                xv[u] = xs[__ldg(idx + kk)];
+            } else {
+                vv[u] = 0.0;
+                xv[u] = 0.0;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kSlUnroll; ++u) acc = fma(vv[u], xv[u], acc);
+    }
+    return acc;
+}
+
 template <typename VT, bool SCALE, typename FIN>
 __device__ __forceinline__ void sliced_rows(const SlicedOp& a, const VT* __restrict__ val, const double* x,
                                             double rinv, double* dyn, FIN fin) {
     double* xs = dyn;
     double* yacc = dyn + kSlW;
+    uint16_t* longs = reinterpret_cast<uint16_t*>(dyn + kSlW + kSlRowCap);  // rows of the range, < kSlRowCap
+    int* nlong = reinterpret_cast<int*>(longs + kSlRowCap);
     const int tid = threadIdx.x, nthr = blockDim.x;
-    const int warp = tid >> 5, sub = tid % kSlG;
-    const int wrow = (tid & 31) / kSlG;  // the warp's rows: 32 / kSlG at a time
-    constexpr int kRowsPerWarp = 32 / kSlG;
-    const int nwarp = nthr >> 5;
+    const int lane = tid & 31, warp = tid >> 5, nwarp = nthr >> 5;
     for (int64_t rg = blockIdx.x; rg < a.nranges; rg += gridDim.x) {
         const int64_t r0 = a.rstart[rg], r1 = a.rstart[rg + 1];
         const int nr = (int)(r1 - r0);
@@ -109,37 +138,26 @@ __device__ __forceinline__ void sliced_rows(const SlicedOp& a, const VT* __restr
         for (int s = 0; s < a.nslices; ++s) {
             const int64_t c0 = (int64_t)s * kSlW;
             const int cw = (int)(a.nminor - c0 < kSlW ? a.nminor - c0 : kSlW);
-            __syncthreads();  // every group is done with the previous slice
+            __syncthreads();  // every thread is done with the previous slice
+            if (tid == 0) *nlong = 0;
             for (int i = tid; i < cw; i += nthr) xs[i] = SCALE ? mul_rn(x[c0 + i], rinv) : x[c0 + i];
             __syncthreads();
             const int32_t* pp = a.sptr + (int64_t)s * (a.nmajor + 1);
             const int64_t base = __ldg(a.sbase + s);
-            // the loop is uniform over the warp (every lane takes every trip), so
-            // the full-mask shuffles below always see all 32 lanes
-            for (int64_t rb = r0 + (int64_t)warp * kRowsPerWarp; rb < r1; rb += (int64_t)nwarp * kRowsPerWarp) {
-                const int64_t r = rb + wrow;
-                const bool valid = r < r1;
-                const int64_t b = valid ? base + __ldg(pp + r) : 0, e = valid ? base + __ldg(pp + r + 1) : 0;
-                double acc = 0.0;
-                for (int64_t k = b + sub; k < e; k += (int64_t)kSlG * kSlUnroll) {
-                    double vv[kSlUnroll], xv[kSlUnroll];
+            for (int64_t r = r0 + tid; r < r1; r += nthr) {
+                const int64_t b = base + __ldg(pp + r), e = base + __ldg(pp + r + 1);
+                if (e - b > kSlLong) longs[atomicAdd(nlong, 1)] = (uint16_t)(r - r0);
+                else yacc[r - r0] += sliced_piece(val, a.sidx, xs, b, e, 1);
+            }
+            __syncthreads();
+            const int nl = *nlong;
+            for (int li = warp; li < nl; li += nwarp) {  // uniform over the warp
+                const int64_t r = r0 + longs[li];
+                const int64_t b = base + __ldg(pp + r), e = base + __ldg(pp + r + 1);
+                double acc = sliced_piece(val, a.sidx, xs, b + lane, e, 32);
 #pragma unroll
-                    for (int u = 0; u < kSlUnroll; ++u) {
-                        const int64_t kk = k + (int64_t)u * kSlG;
-                        if (kk < e) {
-                            vv[u] = (double)__ldg(val + kk);
-                            xv[u] = xs[__ldg(a.sidx + kk)];
-                        } else {
-                            vv[u] = 0.0;
-                            xv[u] = 0.0;
-                        }
-                    }
-#pragma unroll
-                    for (int u = 0; u < kSlUnroll; ++u) acc = fma(vv[u], xv[u], acc);
-                }
-#pragma unroll
-                for (int o = kSlG / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-                if (valid && sub == 0) yacc[r - r0] += acc;
+                for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+                if (lane == 0) yacc[r - r0] += acc;
             }
         }
         __syncthreads();

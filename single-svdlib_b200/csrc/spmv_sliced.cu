@@ -4,14 +4,14 @@
 // The gather SpMV (k_spmv) reads x at every nonzero: on the 1M x 200k LAS2
 // matrix that is 200 M random 8-byte reads, each moving a 32-byte sector
 // through L2, and the kernel sits near a quarter of HBM bandwidth however
-// narrow the values are.  Here the columns are cut into slices of W (20,480)
+// narrow the values are.  Here the columns are cut into slices of W (18,432)
 // and the entries regrouped slice-major: per slice, a CSR over all rows
 // whose column indices are 16-bit offsets into the slice.  A CTA owns a
 // contiguous range of rows (balanced by nonzeros, at most kSlRowCap rows);
 // for each slice it copies x[sW, sW + W) into shared memory with coalesced
-// loads, then streams its rows' entries of that slice, reading x from shared
-// memory and adding each row's slice sum to an FP64 accumulator in shared
-// memory.  The matrix is read once, 2 + value bytes per nonzero, plus 4
+// loads, then sums its rows' entries of that slice (a thread per row, a warp
+// per long piece; spmv.cuh), reading x from shared memory and adding each
+// row's slice sum to an FP64 accumulator in shared memory.  The matrix is read once, 2 + value bytes per nonzero, plus 4
 // bytes per (row, slice) of offsets.  Sums run over slices in order and, in
 // a slice, over 8-lane groups in a fixed tree: deterministic.
 //

@@ -1,7 +1,7 @@
 """The column-sliced SpMV (csrc/spmv_sliced.cu) against FP64 products and the
 gather kernel: svd_opa of A and A^T (src/lanczos/mod.rs:1551-1602) on
 operators large enough to get the plan (more than 2^22 nonzeros, more than
-one slice of 20,480 columns), with skewed row lengths (rows longer than a
+one slice of 18,432 columns; the kernel is opt-in, SVDB_SPMV=sliced), with skewed row lengths (rows longer than a
 slice, empty rows, rows inside one slice), FP64 values within 1e-13 and FP32
 values (SVDB_MIXED) within 1e-6 of sum |a||x|; a LAS2 solve on the same
 operator against the checker."""
@@ -17,6 +17,11 @@ from gpu_util import upload
 from single_svdlib import _abi, legacy
 
 pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(autouse=True)
+def _sliced(monkeypatch):
+    monkeypatch.setenv("SVDB_SPMV", "sliced")  # the kernel is opt-in
 
 
 @pytest.fixture(scope="module")
@@ -66,7 +71,7 @@ def test_sliced_products(big, transposed, monkeypatch):
     got = opa_device(h, x, transposed, 0)
     ns, nr = info(h, transposed)
     n_minor = A["nrows"] if transposed else A["ncols"]
-    assert ns == (n_minor + 20479) // 20480 and nr >= 1
+    assert ns == (n_minor + 18431) // 18432 and nr >= 1
     assert np.max(np.abs(got - want) / mag) < 1e-13
     got32 = opa_device(h, x, transposed, 1)
     S32 = S.astype(np.float32).astype(np.float64)
