@@ -324,7 +324,7 @@ int svdb_sliced_spmv_info(const svdb_matrix* a, int transposed, int32_t* nslices
 
 /* The dense-column split the FP32 products (SVDB_MIXED) of this matrix use,
  * with no counterpart in the reference: the number of columns whose density
- * is at least SVDB_DENSE_MIN_DENSITY (0.03 by default) that are multiplied as
+ * is at least SVDB_DENSE_MIN_DENSITY (0.08 by default) that are multiplied as
  * a dense block on the tensor cores (3xTF32, FP64 drains), and the nonzeros
  * they hold; both 0 before the first FP32 product or when no split is used
  * (too few dense columns, more than 64 dense operand columns, or

@@ -60,26 +60,24 @@ namespace svdb {
 constexpr int kDtM = 128;                                  // rows per tile (tensor-memory lanes)
 constexpr int kDtN = 64;                                   // output columns per tile (l <= 64)
 constexpr int kDtK = 32;                                   // K per stage: one 128-byte swizzle row
-constexpr int kDtStages = 4;
-constexpr int kDtAbytes = kDtM * kDtK * 4;                 // 16 KB
-constexpr int kDtBbytes = kDtN * kDtK * 4;                 // 8 KB
-constexpr int kDtStageBytes = kDtAbytes + 2 * kDtBbytes;   // 32 KB
-constexpr int kDtAccBytes = kDtN * kDtM * 8;               // FP64 accumulators, [column][row]
-constexpr int kDtSmem = kDtStages * kDtStageBytes + kDtAccBytes + 1024;
-constexpr int kDtThreads = 192;
+constexpr int kDtStages = 4;                               // shared-memory ring
+constexpr int kDtAccs = 4;                                 // accumulators in tensor memory
+constexpr int kDtAbytes = kDtM * kDtK * 4;                 // 16 KB (head or remainder)
+constexpr int kDtBbytes = kDtN * kDtK * 4;                 // 8 KB (head or remainder)
+constexpr int kDtStageBytes = 2 * kDtAbytes + 2 * kDtBbytes;  // 48 KB
+constexpr int kDtSmem = kDtStages * kDtStageBytes + 1024;
+constexpr int kDtThreads = 320;                            // producer, MMA and 8 drain warps
 // Stages per FP64 drain.  The tensor cores add each MMA's products into the
 // FP32 accumulator with truncation, a bias toward zero that grows with the
 // number of MMAs summed in one accumulator: drained every 32 stages (1,024
 // columns of K) it shrank the randomized solve's singular values by 4-6e-6
-// relative; every stage keeps the FP32 part to 12 MMAs.
+// relative; drained every stage (12 MMAs) by 2e-7.
 constexpr int kDtChunk = SVDB_DT_CHUNK;
 // F32 accumulator, TF32 A and B, both K-major, N = 64, M = 128
 constexpr uint32_t kDtIdesc =
     (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kDtN >> 3) << 17) | ((uint32_t)(kDtM >> 4) << 24);
-// tensor memory: accumulators in columns [0, 128) (two buffers of 64), the A
-// operand in [128, 256) (two slots of 32 head + 32 remainder columns)
-constexpr uint32_t kDtTmemCols = 256;
-constexpr uint32_t kDtAcol = 128;
+// tensor memory: four accumulators of 64 columns
+constexpr uint32_t kDtTmemCols = kDtAccs * kDtN;
 
 __device__ int g_dense_err;
 
@@ -92,6 +90,7 @@ struct DtArgs {
     int64_t rows;     // valid rows of A (output rows in modes 0 and 2)
     int64_t k_total;  // K extent of A and B
     int64_t k_per;    // K per work item (a multiple of kDtK)
+    int64_t kst;      // K stages of A and B (k_total / kDtK): tiles per tile row of the pre-tiled operands
     int32_t m_tiles, k_splits, n_tiles;
     int32_t l;        // mode 0: output columns; mode 2: columns per subset
     int32_t mode;     // 0: out[row * ldo + g] += C (g < l)
@@ -106,6 +105,15 @@ struct DtArgs {
 
 __device__ __forceinline__ uint32_t dt_smem(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
+// The GEMM operands are stored pre-tiled: tiles of R rows x 32 K (R = 128
+// for A, 64 for B), each tile one contiguous R x 128-byte block, tiles in
+// row-of-tiles order (kst tiles per row of tiles).  A stage's TMA copy then
+// reads one contiguous block instead of R pieces of 128 bytes spread over R
+// rows.  Offset of element (r, k):
+__host__ __device__ __forceinline__ int64_t dt_tiled(int64_t r, int64_t k, int64_t kst, int R) {
+    return (((r / R) * kst + (k >> 5)) * R + (r % R)) * 32 + (k & 31);
+}
+
 // shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups 1024 B apart
 __device__ __forceinline__ uint64_t dt_desc(uint32_t saddr) {
     return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
@@ -118,12 +126,14 @@ __device__ __forceinline__ bool dt_wait(uint32_t bar, uint32_t parity, unsigned 
     const unsigned long long t0 = global_ns();
     uint32_t ok = 0, spins = 0;
     while (true) {
-        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-                     : "=r"(ok)
-                     : "r"(bar), "r"(parity)
-                     : "memory");
+        // the thread sleeps in the wait (up to the hint, 20 us) instead of spinning
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity), "r"(20000u)
+            : "memory");
         if (ok) return true;
-        if ((++spins & 63u) == 0) {
+        if ((++spins & 3u) == 0) {
             if (*abort) return false;
             if (global_ns() - t0 > limit) {
                 *abort = 1;
@@ -146,11 +156,11 @@ __device__ __forceinline__ void dt_tma(uint32_t dst, const CUtensorMap* map, int
         : "memory");
 }
 
-__device__ __forceinline__ void dt_mma(uint32_t d, uint32_t a_tmem, uint64_t b, uint32_t acc) {
+__device__ __forceinline__ void dt_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t acc) {
     asm volatile(
         "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-        " tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n}" ::"r"(d),
-        "r"(a_tmem), "l"(b), "r"(kDtIdesc), "r"(acc)
+        " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}" ::"r"(d),
+        "l"(a), "l"(b), "r"(kDtIdesc), "r"(acc)
         : "memory");
 }
 
@@ -158,16 +168,6 @@ __device__ __forceinline__ void dt_commit(uint32_t bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
                  : "memory");
 }
-
-#define DT_ST32(taddr, v)                                                                                           \
-    asm volatile("tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, " \
-                 "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32};" \
-                 ::"r"(taddr), "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]),          \
-                 "r"(v[7]), "r"(v[8]), "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]),        \
-                 "r"(v[15]), "r"(v[16]), "r"(v[17]), "r"(v[18]), "r"(v[19]), "r"(v[20]), "r"(v[21]), "r"(v[22]),     \
-                 "r"(v[23]), "r"(v[24]), "r"(v[25]), "r"(v[26]), "r"(v[27]), "r"(v[28]), "r"(v[29]), "r"(v[30]),     \
-                 "r"(v[31])                                                                                          \
-                 : "memory")
 
 #define DT_LD32(v, taddr)                                                                                          \
     asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, " \
@@ -195,29 +195,43 @@ __device__ __forceinline__ float tf32_head(float x) {
 // exactly TF32 and the error is a rounding error.
 __device__ __forceinline__ float tf32_tail(double x, float head) { return tf32_head((float)(x - (double)head)); }
 
+// hi + lo += v with Knuth's TwoSum: the rounding error of hi + v, recovered
+// exactly, goes into lo (explicit round-to-nearest additions, no contraction)
+__device__ __forceinline__ void two_sum(float& hi, float& lo, float v) {
+    const float s = __fadd_rn(hi, v);
+    const float bv = __fsub_rn(s, hi);
+    const float e = __fadd_rn(__fsub_rn(hi, __fsub_rn(s, bv)), __fsub_rn(v, bv));
+    hi = s;
+    lo = __fadd_rn(lo, e);
+}
+
+// C = (Ah + Al)(Bh + Bl)^T less the Al Bl term: three TF32 MMAs per K step
+// into an FP32 accumulator in tensor memory, drained into FP64 registers
+// every kDtChunk stages.  Warp 0: TMA producer (one thread); warp 1: tensor
+// memory owner and MMA issuer (one thread); warps 2-9: drains, warp w reading
+// tensor-memory lanes 32 (w % 4) to 32 (w % 4) + 31 (one output row a
+// thread) and accumulator columns 32 (w - 2) / 4 to that + 31.
 __global__ void __launch_bounds__(kDtThreads, 1)
-    k_dense_tc(const __grid_constant__ CUtensorMap amap, const __grid_constant__ CUtensorMap bhmap,
-               const __grid_constant__ CUtensorMap blmap, const DtArgs a) {
+    k_dense_tc(const __grid_constant__ CUtensorMap ahmap, const __grid_constant__ CUtensorMap almap,
+               const __grid_constant__ CUtensorMap bhmap, const __grid_constant__ CUtensorMap blmap,
+               const DtArgs a) {
     extern __shared__ unsigned char dyn[];
-    __shared__ __align__(8) uint64_t bar_full[kDtStages], bar_empty[kDtStages], bar_tmf[2], bar_tme[2],
-        bar_accf[2], bar_acce[2], bar_fin;
+    __shared__ __align__(8) uint64_t bar_full[kDtStages], bar_empty[kDtStages], bar_accf[kDtAccs],
+        bar_acce[kDtAccs], bar_fin;
     __shared__ uint32_t s_tmem;
     __shared__ int s_abort;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(dyn) + 1023) & ~uintptr_t(1023));
-    double* sacc = reinterpret_cast<double*>(sm + kDtStages * kDtStageBytes);
     volatile int* abort = &s_abort;
 
     if (tid == 0) {
         for (int s = 0; s < kDtStages; ++s) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(dt_smem(&bar_full[s])) : "memory");
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 5;" ::"r"(dt_smem(&bar_empty[s])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(dt_smem(&bar_empty[s])) : "memory");
         }
-        for (int t = 0; t < 2; ++t) {
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;" ::"r"(dt_smem(&bar_tmf[t])) : "memory");
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(dt_smem(&bar_tme[t])) : "memory");
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(dt_smem(&bar_accf[t])) : "memory");
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;" ::"r"(dt_smem(&bar_acce[t])) : "memory");
+        for (int b = 0; b < kDtAccs; ++b) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(dt_smem(&bar_accf[b])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 8;" ::"r"(dt_smem(&bar_acce[b])) : "memory");
         }
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(dt_smem(&bar_fin)) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -248,25 +262,33 @@ __global__ void __launch_bounds__(kDtThreads, 1)
         nst = (int)((ke - kb + kDtK - 1) / kDtK);
     };
 
-    uint32_t issued = 0;  // producer: stages issued; MMA: stages consumed
     if (warp == 0 && lane == 0) {
         // ------------------------------------------------------- producer --
+        uint32_t issued = 0;
         for (int64_t it = blockIdx.x; it < items && !*abort; it += gridDim.x) {
             int64_t m0, kb;
             int nst, ks, nt;
             item_geom(it, m0, kb, nst, ks, nt);
+            bool ok = true;
             for (int st = 0; st < nst; ++st, ++issued) {
                 const int s = issued % kDtStages;
-                if (!dt_wait(dt_smem(&bar_empty[s]), ((issued / kDtStages) & 1) ^ 1, a.limit_ns, abort)) break;
+                if (!dt_wait(dt_smem(&bar_empty[s]), ((issued / kDtStages) & 1) ^ 1, a.limit_ns, abort)) {
+                    ok = false;
+                    break;
+                }
                 unsigned char* base = sm + s * kDtStageBytes;
                 const uint32_t fb = dt_smem(&bar_full[s]);
                 asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fb), "r"(kDtStageBytes)
                              : "memory");
-                const int kx = (int)(kb + (int64_t)st * kDtK);
-                dt_tma(dt_smem(base), &amap, kx, (int)m0, fb);
-                dt_tma(dt_smem(base + kDtAbytes), &bhmap, kx, nt * kDtN, fb);
-                dt_tma(dt_smem(base + kDtAbytes + kDtBbytes), &blmap, kx, nt * kDtN, fb);
+                const int64_t kt = kb / kDtK + st;  // K tile
+                const int ya = (int)(((m0 / kDtM) * a.kst + kt) * kDtM);
+                const int yb = (int)(((int64_t)nt * a.kst + kt) * kDtN);
+                dt_tma(dt_smem(base), &ahmap, 0, ya, fb);
+                dt_tma(dt_smem(base + kDtAbytes), &almap, 0, ya, fb);
+                dt_tma(dt_smem(base + 2 * kDtAbytes), &bhmap, 0, yb, fb);
+                dt_tma(dt_smem(base + 2 * kDtAbytes + kDtBbytes), &blmap, 0, yb, fb);
             }
+            if (!ok) break;
         }
         // every copy issued must land before the CTA may exit
         for (uint32_t q = 0; q < kDtStages && q < issued; ++q) {
@@ -276,35 +298,40 @@ __global__ void __launch_bounds__(kDtThreads, 1)
         }
     } else if (warp == 1 && lane == 0) {
         // ------------------------------------------------------------ MMA --
-        uint32_t ch = 0;
+        uint32_t issued = 0, ch = 0;
         bool any = false;
         for (int64_t it = blockIdx.x; it < items && !*abort; it += gridDim.x) {
             int64_t m0, kb;
             int nst, ks, nt;
             item_geom(it, m0, kb, nst, ks, nt);
             bool ok = true;
-            for (int st = 0; st < nst && ok; ++st, ++issued) {
-                const int s = issued % kDtStages, t = issued & 1, b = ch & 1;
+            for (int st = 0; st < nst; ++st, ++issued) {
+                const int s = issued % kDtStages, b = ch % kDtAccs;
                 const bool first = (st % kDtChunk) == 0, last = (st % kDtChunk) == kDtChunk - 1 || st == nst - 1;
-                if (first && !dt_wait(dt_smem(&bar_acce[b]), ((ch >> 1) & 1) ^ 1, a.limit_ns, abort)) { ok = false; break; }
-                if (!dt_wait(dt_smem(&bar_full[s]), (issued / kDtStages) & 1, a.limit_ns, abort)) { ok = false; break; }
-                if (!dt_wait(dt_smem(&bar_tmf[t]), (issued >> 1) & 1, a.limit_ns, abort)) { ok = false; break; }
+                if (first && !dt_wait(dt_smem(&bar_acce[b]), ((ch / kDtAccs) & 1) ^ 1, a.limit_ns, abort)) {
+                    ok = false;
+                    break;
+                }
+                if (!dt_wait(dt_smem(&bar_full[s]), (issued / kDtStages) & 1, a.limit_ns, abort)) {
+                    ok = false;
+                    break;
+                }
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const unsigned char* base = sm + s * kDtStageBytes;
-                const uint64_t bh = dt_desc(dt_smem(base + kDtAbytes));
-                const uint64_t bl = dt_desc(dt_smem(base + kDtAbytes + kDtBbytes));
+                const uint64_t ah = dt_desc(dt_smem(base));
+                const uint64_t al = dt_desc(dt_smem(base + kDtAbytes));
+                const uint64_t bh = dt_desc(dt_smem(base + 2 * kDtAbytes));
+                const uint64_t bl = dt_desc(dt_smem(base + 2 * kDtAbytes + kDtBbytes));
                 const uint32_t d = tmem + (uint32_t)b * kDtN;
-                const uint32_t ah = tmem + kDtAcol + (uint32_t)t * 64, al = ah + 32;
 #pragma unroll
                 for (int kk = 0; kk < kDtK / 8; ++kk) {
                     const uint64_t koff = (uint64_t)((kk * 32) >> 4);  // 8 TF32 = 32 bytes along the swizzled row
-                    dt_mma(d, ah + kk * 8, bh + koff, (first && kk == 0) ? 0u : 1u);
-                    dt_mma(d, ah + kk * 8, bl + koff, 1u);
-                    dt_mma(d, al + kk * 8, bh + koff, 1u);
+                    dt_mma(d, ah + koff, bh + koff, (first && kk == 0) ? 0u : 1u);
+                    dt_mma(d, ah + koff, bl + koff, 1u);
+                    dt_mma(d, al + koff, bh + koff, 1u);
                 }
                 any = true;
                 dt_commit(dt_smem(&bar_empty[s]));
-                dt_commit(dt_smem(&bar_tme[t]));
                 if (last) {
                     dt_commit(dt_smem(&bar_accf[b]));
                     ++ch;
@@ -318,112 +345,95 @@ __global__ void __launch_bounds__(kDtThreads, 1)
             dt_wait(dt_smem(&bar_fin), 0, 2000000000ull, &never);
         }
     } else if (warp >= 2) {
-        // ------------------------------------- split, tensor-memory store, drain --
-        const int g = warp & 3;          // tensor-memory lane group of this warp
-        const int r = g * 32 + lane;     // row of the tile
-        const uint32_t lane_base = tmem + ((uint32_t)(g * 32) << 16);
-        for (int j = 0; j < kDtN; ++j) sacc[j * kDtM + r] = 0.0;
+        // ------------------------------- drain into FP32 pairs, write FP64 --
+        // Each output is kept as an unevaluated sum hi + lo of two floats;
+        // a drained value v is added with the error-free TwoSum (Knuth):
+        // s = hi + v exactly equals s + e, e from five more additions, and e
+        // goes into lo.  FP32 additions run at four times the rate of the
+        // FP32-to-FP64 conversions an FP64 sum would take per value.
+        constexpr int kH = kDtN / 2;             // accumulator columns per drain warp
+        const int g = warp & 3;                  // tensor-memory lane group of this warp
+        const int c0 = ((warp - 2) >> 2) * kH;   // first accumulator column of this warp
+        const int r = g * 32 + lane;
+        const uint32_t lane_base = tmem + ((uint32_t)(g * 32) << 16) + (uint32_t)c0;
+        float hi[kH], lo[kH];
+#pragma unroll
+        for (int j = 0; j < kH; ++j) hi[j] = lo[j] = 0.f;
         uint32_t ch = 0;
-        bool pending = false, pending_last = false;
-        int64_t pend_m0 = 0;
-        int pend_ks = 0, pend_nt = 0;
-        auto drain = [&]() -> bool {
-            const int b = ch & 1;
-            if (!dt_wait(dt_smem(&bar_accf[b]), (ch >> 1) & 1, a.limit_ns, abort)) return false;
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                uint32_t v[32];
-                DT_LD32(v, lane_base + (uint32_t)b * kDtN + h * 32);
-                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-                for (int j = 0; j < 32; ++j) sacc[(h * 32 + j) * kDtM + r] += (double)__uint_as_float(v[j]);
-            }
-            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-            __syncwarp();
-            if (lane == 0) dt_arrive(dt_smem(&bar_acce[b]));
-            ++ch;
-            if (pending_last) {
-                const int64_t row = pend_m0 + r;
-                const int64_t g0 = (int64_t)pend_nt * kDtN;
-                if (a.mode == 0) {
-                    if (row < a.rows) {
-                        const int jn = (int)min((int64_t)kDtN, (int64_t)a.l - g0);
-                        if (a.out_f32) {
-                            float* o = static_cast<float*>(a.out) + row * a.ldo + g0;
-                            for (int j = 0; j < jn; ++j) o[j] = (float)((double)o[j] + sacc[j * kDtM + r]);
-                        } else {
-                            double* o = static_cast<double*>(a.out) + row * a.ldo + g0;
-                            for (int j = 0; j < jn; ++j) o[j] += sacc[j * kDtM + r];
-                        }
-                    }
-                } else if (a.mode == 2) {
-                    if (row < a.rows) {
-                        for (int j = 0; j < kDtN; ++j) {
-                            const int64_t g = g0 + j, b = g / a.l, c = g - b * a.l;
-                            if (b >= a.bcount) break;
-                            const int64_t at = (b * a.bm + row) * a.l + c;
-                            if (a.out_f32) {
-                                float* o = static_cast<float*>(a.out);
-                                o[at] = (float)((double)o[at] + sacc[j * kDtM + r]);
-                            } else {
-                                static_cast<double*>(a.out)[at] += sacc[j * kDtM + r];
-                            }
-                        }
-                    }
-                } else {
-                    double* o = static_cast<double*>(a.out) +
-                                ((((int64_t)pend_ks * a.n_tiles + pend_nt) * a.m_tiles * kDtM) + row) * kDtN;
-                    for (int j = 0; j < kDtN; ++j) o[j] = sacc[j * kDtM + r];
-                }
-                for (int j = 0; j < kDtN; ++j) sacc[j * kDtM + r] = 0.0;
-            }
-            pending = false;
-            return true;
-        };
         bool ok = true;
         for (int64_t it = blockIdx.x; it < items && ok && !*abort; it += gridDim.x) {
             int64_t m0, kb;
             int nst, ks, nt;
             item_geom(it, m0, kb, nst, ks, nt);
-            for (int st = 0; st < nst; ++st, ++issued) {
-                const int s = issued % kDtStages, t = issued & 1;
-                if (!dt_wait(dt_smem(&bar_full[s]), (issued / kDtStages) & 1, a.limit_ns, abort)) { ok = false; break; }
-                const unsigned char* row_p = sm + s * kDtStageBytes + r * 128;
-                uint32_t hi[32], lo[32];
-#pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    const float4 x = *reinterpret_cast<const float4*>(row_p + ((q ^ (r & 7)) << 4));
-                    const float xs[4] = {x.x, x.y, x.z, x.w};
-#pragma unroll
-                    for (int e = 0; e < 4; ++e) {
-                        const float h = tf32_head(xs[e]);
-                        hi[q * 4 + e] = __float_as_uint(h);
-                        lo[q * 4 + e] = __float_as_uint(tf32_head(xs[e] - h));
-                    }
+            const int nch = (nst + kDtChunk - 1) / kDtChunk;
+            for (int c = 0; c < nch; ++c, ++ch) {
+                const int b = ch % kDtAccs;
+                if (!dt_wait(dt_smem(&bar_accf[b]), (ch / kDtAccs) & 1, a.limit_ns, abort)) {
+                    ok = false;
+                    break;
                 }
-                __syncwarp();
-                if (lane == 0) dt_arrive(dt_smem(&bar_empty[s]));
-                if (!dt_wait(dt_smem(&bar_tme[t]), ((issued >> 1) & 1) ^ 1, a.limit_ns, abort)) { ok = false; break; }
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint32_t slot = lane_base + kDtAcol + (uint32_t)t * 64;
-                DT_ST32(slot, hi);
-                DT_ST32(slot + 32, lo);
-                asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+                uint32_t v[32];
+                DT_LD32(v, lane_base + (uint32_t)b * kDtN);
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
                 asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
                 __syncwarp();
-                if (lane == 0) dt_arrive(dt_smem(&bar_tmf[t]));
-                if ((st % kDtChunk) == 0 && pending && !drain()) { ok = false; break; }
-                if ((st % kDtChunk) == kDtChunk - 1 || st == nst - 1) {
-                    pending = true;
-                    pending_last = (st == nst - 1);
-                    pend_m0 = m0;
-                    pend_ks = ks;
-                    pend_nt = nt;
-                }
+                if (lane == 0) dt_arrive(dt_smem(&bar_acce[b]));
+#pragma unroll
+                for (int j = 0; j < kH; ++j) two_sum(hi[j], lo[j], __uint_as_float(v[j]));
             }
+            if (!ok) break;
+#define DT_ACC(j) ((double)hi[j] + (double)lo[j])
+            const int64_t row = m0 + r;
+            const int64_t g0 = (int64_t)nt * kDtN + c0;  // product column of this thread's first value
+            if (a.mode == 0) {
+                if (row < a.rows) {
+                    const int jn = (int)min((int64_t)kH, (int64_t)a.l - g0);
+                    if (a.out_f32) {
+                        float* o = static_cast<float*>(a.out) + row * a.ldo + g0;
+#pragma unroll
+                        for (int j = 0; j < kH; ++j)
+                            if (j < jn) o[j] = (float)((double)o[j] + DT_ACC(j));
+                    } else {
+                        double* o = static_cast<double*>(a.out) + row * a.ldo + g0;
+#pragma unroll
+                        for (int j = 0; j < kH; ++j)
+                            if (j < jn) o[j] += DT_ACC(j);
+                    }
+                }
+            } else if (a.mode == 2) {
+                if (row < a.rows) {
+                    // column g0 + j is column c of product bb; step (bb, c) along j
+                    int64_t bb = g0 / a.l, cc = g0 - bb * a.l;
+#pragma unroll
+                    for (int j = 0; j < kH; ++j) {
+                        if (bb < a.bcount) {
+                            const int64_t at = (bb * a.bm + row) * a.l + cc;
+                            if (a.out_f32) {
+                                float* o = static_cast<float*>(a.out);
+                                o[at] = (float)((double)o[at] + DT_ACC(j));
+                            } else {
+                                static_cast<double*>(a.out)[at] += DT_ACC(j);
+                            }
+                        }
+                        if (++cc == a.l) {
+                            cc = 0;
+                            ++bb;
+                        }
+                    }
+                }
+            } else {
+                double2* o = reinterpret_cast<double2*>(static_cast<double*>(a.out) +
+                                                        ((((int64_t)ks * a.n_tiles + nt) * a.m_tiles * kDtM) + row) *
+                                                            kDtN +
+                                                        c0);
+#pragma unroll
+                for (int j = 0; j < kH / 2; ++j) o[j] = make_double2(DT_ACC(2 * j), DT_ACC(2 * j + 1));
+            }
+#undef DT_ACC
+#pragma unroll
+            for (int j = 0; j < kH; ++j) hi[j] = lo[j] = 0.f;
         }
-        if (ok && pending) drain();
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -434,15 +444,16 @@ __global__ void __launch_bounds__(kDtThreads, 1)
 }
 
 // ------------------------------------------------------- operand prep --
-// B of A X: Bh/Bl (64 x kp, K-major) = TF32 head / remainder of X[cols[k], j]
-// (zero past l and for padding columns cols[k] < 0), from the FP64 operand.
+// B of A X: Bh/Bl (64 x kp, pre-tiled) = TF32 head / remainder of
+// X[cols[k], j] (zero past l and for padding columns cols[k] < 0).  Thread i
+// writes element i of the tiled buffer: tile i / 2048 is K tile k / 32.
 template <typename XT>
 __global__ void k_dense_b_gather(const XT* __restrict__ X, int l, const int32_t* __restrict__ cols, int64_t kp,
                                  float* __restrict__ bh, float* __restrict__ bl) {
     const int64_t total = (int64_t)kDtN * kp;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
-        const int j = (int)(i / kp);
-        const int64_t k = i - (int64_t)j * kp;
+        const int j = (int)((i >> 5) & (kDtN - 1));
+        const int64_t k = (i / (kDtN * 32)) * 32 + (i & 31);
         const int32_t c = cols[k];
         const double x = (j < l && c >= 0) ? (double)X[(int64_t)c * l + j] : 0.0;
         const float h = tf32_head((float)x);
@@ -451,8 +462,8 @@ __global__ void k_dense_b_gather(const XT* __restrict__ X, int l, const int32_t*
     }
 }
 
-// B of A^T Y: Bh/Bl (64 x kp) = head / remainder of Y^T (Y: rows x l), zero
-// past rows and l.  32 x 32 tiles through shared memory.
+// B of A^T Y: Bh/Bl (64 x kp, pre-tiled) = head / remainder of Y^T (Y: rows
+// x l), zero past rows and l.  32 x 32 tiles through shared memory.
 template <typename XT>
 __global__ void k_dense_b_transpose(const XT* __restrict__ Y, int64_t rows, int l, int64_t kp,
                                     float* __restrict__ bh, float* __restrict__ bl) {
@@ -471,8 +482,9 @@ __global__ void k_dense_b_transpose(const XT* __restrict__ Y, int64_t rows, int 
         if (k < kp) {
             const double x = tile[threadIdx.x][jj];
             const float h = tf32_head((float)x);
-            bh[(int64_t)j * kp + k] = h;
-            bl[(int64_t)j * kp + k] = tf32_tail(x, h);
+            const int64_t at = dt_tiled(j, k, kp / kDtK, kDtN);
+            bh[at] = h;
+            bl[at] = tf32_tail(x, h);
         }
     }
 }
@@ -492,10 +504,13 @@ __global__ void k_dense_reduce(const double* __restrict__ part, int ksplits, int
 }
 
 // --------------------------------------------------------------- build --
-// D[r, k] and Dt[k, r] from column cols[k] of the CSC (one warp per column).
+// D[r, k] and Dt[k, r] from column cols[k] of the CSC (one warp per column),
+// as TF32 heads (D, Dt) and TF32-rounded remainders (Dl, Dtl), pre-tiled
+// (128-row tiles; D: ndp / 32 K tiles a row of tiles, Dt: mp / 32).
 __global__ void k_dense_scatter(const int64_t* __restrict__ cp, const int32_t* __restrict__ ri,
                                 const float* __restrict__ v, const int32_t* __restrict__ cols, int64_t nd,
-                                int64_t ndp, int64_t mp, float* __restrict__ D, float* __restrict__ Dt) {
+                                int64_t ndp, int64_t mp, float* __restrict__ D, float* __restrict__ Dl,
+                                float* __restrict__ Dt, float* __restrict__ Dtl) {
     const int lane = threadIdx.x & 31;
     const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -503,8 +518,12 @@ __global__ void k_dense_scatter(const int64_t* __restrict__ cp, const int32_t* _
         const int32_t c = cols[k];
         for (int64_t e = cp[c] + lane; e < cp[c + 1]; e += 32) {
             const int64_t r = ri[e];
-            D[r * ndp + k] = v[e];
-            Dt[k * mp + r] = v[e];
+            const float h = tf32_head(v[e]), t = tf32_head(v[e] - h);  // v - h is exact
+            const int64_t od = dt_tiled(r, k, ndp / kDtK, kDtM), ot = dt_tiled(k, r, mp / kDtK, kDtM);
+            D[od] = h;
+            Dl[od] = t;
+            Dt[ot] = h;
+            Dtl[ot] = t;
         }
     }
 }
@@ -572,16 +591,16 @@ static PFN_cuTensorMapEncodeTiled_v12000 dt_encode() {
     return fn;
 }
 
-// FP32 row-major [rows x cols] (cols a multiple of 32, rows of cols * 4 bytes,
-// 16-byte aligned base), boxes of box_rows x 32 with the 128-byte swizzle
-static CUtensorMap dt_map(const float* base, int64_t cols, int64_t rows, int box_rows) {
+// A pre-tiled FP32 operand seen as rows of 32 floats (128 bytes), `rows`
+// of them, copied in boxes of box_rows x 32 with the 128-byte swizzle
+static CUtensorMap dt_map(const float* base, int64_t rows, int box_rows) {
     CUtensorMap m;
-    const cuuint64_t gdim[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
-    const cuuint64_t gstr[1] = {(cuuint64_t)cols * 4};
+    const cuuint64_t gdim[2] = {(cuuint64_t)kDtK, (cuuint64_t)rows};
+    const cuuint64_t gstr[1] = {(cuuint64_t)kDtK * 4};
     const cuuint32_t box[2] = {(cuuint32_t)kDtK, (cuuint32_t)box_rows};
     const cuuint32_t estr[2] = {1, 1};
-    if ((reinterpret_cast<uintptr_t>(base) & 15) || (cols % kDtK))
-        throw Error(SVDB_ERR_CUDA, "dense split: operand not aligned for the tensor memory accelerator");
+    if ((reinterpret_cast<uintptr_t>(base) & 15) || rows % box_rows || rows >= ((int64_t)1 << 31))
+        throw Error(SVDB_ERR_CUDA, "dense split: operand not laid out for the tensor memory accelerator");
     CUresult r = dt_encode()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), gdim, gstr, box, estr,
                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
@@ -593,10 +612,12 @@ static int dt_grid(int64_t items) {
     return (int)std::max<int64_t>(1, std::min<int64_t>(items, device_props().sms));
 }
 
-// C = A (a_rows x a_cols) . B^T with B (n_tiles * 64 rows x a_cols) given as
-// its TF32 head bh and remainder bl; see DtArgs for the modes.
+// C = A (a_rows x a_cols) . B^T with A given as its TF32 head ah and
+// remainder al (pre-tiled, rows padded to 128), B (n_tiles * 64 rows x
+// a_cols, pre-tiled) as bh and bl; a_cols a multiple of 32; see DtArgs for
+// the modes.
 struct DtLaunch {
-    const float* A;
+    const float *ah, *al;
     int64_t a_rows, a_cols;
     const float *bh, *bl;
     int n_tiles = 1;
@@ -613,13 +634,18 @@ static void dt_launch(const DtLaunch& p, cudaStream_t s) {
     std::call_once(attr, [] {
         SVDB_CUDA(cudaFuncSetAttribute(k_dense_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kDtSmem));
     });
-    const CUtensorMap am = dt_map(p.A, p.a_cols, p.a_rows, kDtM);
-    const CUtensorMap hm = dt_map(p.bh, p.a_cols, (int64_t)p.n_tiles * kDtN, kDtN);
-    const CUtensorMap lm = dt_map(p.bl, p.a_cols, (int64_t)p.n_tiles * kDtN, kDtN);
+    if (p.a_cols % kDtK) throw Error(SVDB_ERR_CUDA, "dense split: K not a multiple of 32");
+    const int64_t kst = p.a_cols / kDtK;
+    const int64_t a_tiles = (p.a_rows + kDtM - 1) / kDtM;
+    const CUtensorMap ahm = dt_map(p.ah, a_tiles * kst * kDtM, kDtM);
+    const CUtensorMap alm = dt_map(p.al, a_tiles * kst * kDtM, kDtM);
+    const CUtensorMap hm = dt_map(p.bh, (int64_t)p.n_tiles * kst * kDtN, kDtN);
+    const CUtensorMap lm = dt_map(p.bl, (int64_t)p.n_tiles * kst * kDtN, kDtN);
     DtArgs g;
     g.rows = p.a_rows;
     g.k_total = p.a_cols;
     g.k_per = p.k_per ? p.k_per : p.a_cols;
+    g.kst = kst;
     g.m_tiles = (int)((p.a_rows + kDtM - 1) / kDtM);
     g.k_splits = p.ksplits;
     g.n_tiles = p.n_tiles;
@@ -632,7 +658,7 @@ static void dt_launch(const DtLaunch& p, cudaStream_t s) {
     g.bcount = p.bcount;
     g.limit_ns = wait_limit_ns();
     const int64_t items = (int64_t)g.m_tiles * p.ksplits * p.n_tiles;
-    k_dense_tc<<<dt_grid(items), kDtThreads, kDtSmem, s>>>(am, hm, lm, g);
+    k_dense_tc<<<dt_grid(items), kDtThreads, kDtSmem, s>>>(ahm, alm, hm, lm, g);
     SVDB_CHECK_LAUNCH();
 }
 
@@ -681,7 +707,7 @@ static void build_rest(const DevCompressed& src, const uint8_t* dense, bool by_m
 static double dense_min_density() {
     const char* e = getenv("SVDB_DENSE_MIN_DENSITY");
     if (e && *e) return atof(e);
-    return 0.03;
+    return 0.08;
 }
 
 static bool dense_enabled() {
@@ -715,12 +741,12 @@ static DenseSplit* dense_split_for(const svdb_matrix* a) {
         if ((double)(cp[j + 1] - cp[j]) >= thr) order.push_back((int32_t)j);
     std::stable_sort(order.begin(), order.end(),
                      [&](int32_t x, int32_t y) { return cp[x + 1] - cp[x] > cp[y + 1] - cp[y]; });
-    // memory: D and Dt take 8 m nd bytes; keep them under a quarter of the free memory and 16 GB
+    // memory: D, Dt and their remainders take 16 m nd bytes; keep them under a quarter of the free memory and 16 GB
     size_t free_b = 0, total_b = 0;
     SVDB_CUDA(cudaMemGetInfo(&free_b, &total_b));
     const double cap = std::min<double>(16e9, 0.25 * (double)free_b);
     const int64_t mp = (m + kDtK - 1) / kDtK * kDtK;
-    int64_t nd_max = (int64_t)(cap / (8.0 * (double)mp)) / kDtM * kDtM;
+    int64_t nd_max = (int64_t)(cap / (16.0 * (double)mp)) / kDtM * kDtM;
     int64_t nd = std::min<int64_t>((int64_t)order.size(), nd_max);
     if (nd < kDtM) return nullptr;
     order.resize(nd);
@@ -738,12 +764,17 @@ static DenseSplit* dense_split_for(const svdb_matrix* a) {
     DevBuf<uint8_t> dflag(n, s);
     SVDB_CUDA(cudaMemcpyAsync(ds->cols.p, cols.data(), ndp * sizeof(int32_t), cudaMemcpyHostToDevice, s));
     SVDB_CUDA(cudaMemcpyAsync(dflag.p, flag.data(), n, cudaMemcpyHostToDevice, s));
-    ds->D.alloc((size_t)m * ndp, s);
-    ds->Dt.alloc((size_t)ndp * mp, s);
-    SVDB_CUDA(cudaMemsetAsync(ds->D.p, 0, (size_t)m * ndp * sizeof(float), s));
-    SVDB_CUDA(cudaMemsetAsync(ds->Dt.p, 0, (size_t)ndp * mp * sizeof(float), s));
+    const int64_t m128 = (m + kDtM - 1) / kDtM * kDtM;  // D's rows, padded to whole tiles
+    for (DevBuf<float>* b : {&ds->D, &ds->Dl}) {
+        b->alloc((size_t)m128 * ndp, s);
+        SVDB_CUDA(cudaMemsetAsync(b->p, 0, (size_t)m128 * ndp * sizeof(float), s));
+    }
+    for (DevBuf<float>* b : {&ds->Dt, &ds->Dtl}) {
+        b->alloc((size_t)ndp * mp, s);
+        SVDB_CUDA(cudaMemsetAsync(b->p, 0, (size_t)ndp * mp * sizeof(float), s));
+    }
     k_dense_scatter<<<(int)nblocks(nd * 32, 256), 256, 0, s>>>(csc.ptr.p, csc.idx.p, csc.val32.p, ds->cols.p, nd, ndp,
-                                                              mp, ds->D.p, ds->Dt.p);
+                                                              mp, ds->D.p, ds->Dl.p, ds->Dt.p, ds->Dtl.p);
     SVDB_CHECK_LAUNCH();
     build_rest(csr, dflag.p, false, ds->rest_csr, s);
     build_rest(csc, dflag.p, true, ds->rest_csc, s);
@@ -786,7 +817,7 @@ void dense_split_spmm(const svdb_matrix* a, bool transpose, const XT* X, const f
         k_dense_b_gather<XT><<<(int)nblocks(kDtN * ds->ndp, 256), 256, 0, s>>>(X, l, ds->cols.p, ds->ndp, bh.p,
                                                                                bl.p);
         SVDB_CHECK_LAUNCH();
-        DtLaunch p{ds->D.p, m, ds->ndp, bh.p, bl.p};
+        DtLaunch p{ds->D.p, ds->Dl.p, m, ds->ndp, bh.p, bl.p};
         p.l = l;
         p.mode = 0;
         p.out_f32 = of32;
@@ -804,7 +835,7 @@ void dense_split_spmm(const svdb_matrix* a, bool transpose, const XT* X, const f
         const int64_t k_per = ((ds->mp + ks - 1) / ks + kDtK - 1) / kDtK * kDtK;
         ks = (int)((ds->mp + k_per - 1) / k_per);
         DevBuf<double> part((size_t)ks * ds->ndp * kDtN, s);
-        DtLaunch p{ds->Dt.p, ds->ndp, ds->mp, bh.p, bl.p};
+        DtLaunch p{ds->Dt.p, ds->Dtl.p, ds->ndp, ds->mp, bh.p, bl.p};
         p.k_per = k_per;
         p.ksplits = ks;
         p.l = l;
@@ -828,16 +859,19 @@ template void dense_split_spmm<float, float>(const svdb_matrix*, bool, const flo
 // all subsets' sample columns side by side (g = b l + c).  The sparse rest
 // runs through the batch's own gather kernels on split->rest_csr/rest_csc.
 
-// B of the row products: head / remainder of X_b[o2m_b(J[k]), c] for row
-// g = b l + c (zero when column J[k] is not in subset b, for padding columns,
-// and for g >= count l); X_b sits at X + coff[b] l.
+// B of the row products (npad x ndp, pre-tiled): head / remainder of
+// X_b[o2m_b(J[k]), c] for row g = b l + c (zero when column J[k] is not in
+// subset b, for padding columns, and for g >= count l); X_b sits at
+// X + coff[b] l.  Thread i writes element i of the tiled buffer.
 __global__ void k_bd_rows_b(const float* __restrict__ X, const int64_t* __restrict__ coff,
                             const int32_t* __restrict__ o2m, const int32_t* __restrict__ cols, int64_t n,
                             int64_t count, int l, int64_t ndp, int64_t npad, float* __restrict__ bh,
                             float* __restrict__ bl) {
     const int64_t total = npad * ndp;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t g = i / ndp, k = i - g * ndp;
+        const int64_t t = i / (kDtN * 32), kst = ndp / kDtK;  // tile t = (g / 64, k / 32)
+        const int64_t g = (t / kst) * kDtN + ((i >> 5) & (kDtN - 1));
+        const int64_t k = (t % kst) * 32 + (i & 31);
         const int64_t b = g / l, c = g - b * l;
         double x = 0.0;
         if (b < count && cols[k] >= 0) {
@@ -850,8 +884,8 @@ __global__ void k_bd_rows_b(const float* __restrict__ X, const int64_t* __restri
     }
 }
 
-// B of the column products: head / remainder of Y_b[k, c] (Y_b at Y + b m l)
-// for row g = b l + c, zero past m; 32 x 32 tiles per subset.
+// B of the column products (pre-tiled): head / remainder of Y_b[k, c] (Y_b
+// at Y + b m l) for row g = b l + c, zero past m; 32 x 32 tiles per subset.
 __global__ void k_bd_cols_b(const float* __restrict__ Y, int64_t m, int l, int64_t mp, float* __restrict__ bh,
                             float* __restrict__ bl) {
     __shared__ float tile[32][33];
@@ -871,7 +905,7 @@ __global__ void k_bd_cols_b(const float* __restrict__ Y, int64_t m, int l, int64
         if (c < l && k < mp) {
             const double x = (double)tile[threadIdx.x][cc];
             const float h = tf32_head((float)x);
-            const int64_t at = (b * l + c) * mp + k;
+            const int64_t at = dt_tiled(b * l + c, k, mp / kDtK, kDtN);
             bh[at] = h;
             bl[at] = tf32_tail(x, h);
         }
@@ -911,7 +945,7 @@ void dense_batch_rows(const svdb_matrix* a, const float* X, const int64_t* coff,
     k_bd_rows_b<<<(int)nblocks(npad * ds->ndp, 256), 256, 0, s>>>(X, coff, o2m, ds->cols.p, n, count, l, ds->ndp,
                                                                    npad, bh, bl);
     SVDB_CHECK_LAUNCH();
-    DtLaunch p{ds->D.p, m, ds->ndp, bh, bl};
+    DtLaunch p{ds->D.p, ds->Dl.p, m, ds->ndp, bh, bl};
     p.n_tiles = (int)(npad / kDtN);
     p.l = l;
     p.mode = 2;
@@ -932,7 +966,7 @@ void dense_batch_cols(const svdb_matrix* a, const float* Y, const int64_t* coff,
     dim3 tb(32, 8), tg((unsigned)(ds->mp / 32), (unsigned)((l + 31) / 32), (unsigned)count);
     k_bd_cols_b<<<tg, tb, 0, s>>>(Y, m, l, ds->mp, bh, bl);
     SVDB_CHECK_LAUNCH();
-    DtLaunch p{ds->Dt.p, ds->ndp, ds->mp, bh, bl};
+    DtLaunch p{ds->Dt.p, ds->Dtl.p, ds->ndp, ds->mp, bh, bl};
     p.n_tiles = (int)(npad / kDtN);
     p.l = l;
     p.mode = 1;

@@ -168,7 +168,7 @@ struct DenseSplit {
     int64_t nd = 0, ndp = 0, mp = 0;  // dense columns; padded to 128; rows padded to 32
     int64_t dense_nnz = 0;
     DevBuf<int32_t> cols;             // ndp original column ids, -1 for padding
-    DevBuf<float> D, Dt;
+    DevBuf<float> D, Dl, Dt, Dtl;     // A[:, J] and its transpose: TF32 heads and remainders
     DevCompressed rest_csr, rest_csc;
 };
 

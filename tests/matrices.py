@@ -141,7 +141,7 @@ def zipf_planted_device(torch, m=1_000_000, n=200_000, seed=3):
     return indptr, cols, vals
 
 
-def dense_columns(m, n, nd, seed, dens=(0.05, 0.4), rest=0.004):
+def dense_columns(m, n, nd, seed, dens=(0.1, 0.4), rest=0.004):
     """nd columns of densities uniform in `dens`, the others of density `rest`;
     values log1p(Poisson(3) + 1): a matrix with a dense-column split."""
     rng = np.random.default_rng(seed)

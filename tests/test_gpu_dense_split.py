@@ -1,7 +1,7 @@
 """The dense-column split of the FP32 SpMM (csrc/dense_split.cu) against the
 checker's products and the gather path.
 
-Matrices with a few hundred columns of density above the 3 % threshold (the
+Matrices with a few hundred columns of density above the 8 % threshold (the
 split takes them to the tensor cores as a 3xTF32 GEMM) plus a sparse rest.
 The products A X and A^T Y of the split must match the FP64 checker within
 an FP32 accumulation bound (1e-5 of each output entry's magnitude,
@@ -12,7 +12,6 @@ l from 1 to 64, and a masked view.
 """
 import numpy as np
 import pytest
-import scipy.sparse as sp
 
 import matrices as M
 import oracle as O
@@ -23,18 +22,9 @@ from single_svdlib.randomized import PowerIterationNormalizer as PIN
 pytestmark = pytest.mark.gpu
 
 
-def dense_cols_matrix(m, n, nd, seed, dens=(0.05, 0.4), rest=0.004):
-    """nd columns with densities uniform in `dens`, the others at `rest`; values log1p(Poisson(3) + 1)."""
-    rng = np.random.default_rng(seed)
-    dcols = rng.choice(n, nd, replace=False)
-    p = np.full(n, rest)
-    p[dcols] = rng.uniform(dens[0], dens[1], nd)
-    mask = rng.random((m, n)) < p[None, :]
-    r, c = np.nonzero(mask)
-    v = np.log1p(rng.poisson(3.0, len(r)) + 1.0)
-    S = sp.csr_matrix((v, (r, c)), shape=(m, n))
-    S.sort_indices()
-    return M.from_scipy(S)
+def dense_cols_matrix(m, n, nd, seed):
+    """nd columns with densities uniform in (0.1, 0.4), the others at 0.004."""
+    return M.dense_columns(m, n, nd, seed)
 
 
 def device_product(h, X, transpose):
