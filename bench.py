@@ -43,6 +43,7 @@ import statistics
 import subprocess
 import sys
 import tempfile
+import threading
 import time
 
 import numpy as np
@@ -89,7 +90,86 @@ def load_or_generate(rank, world):
 
 
 # ---------------------------------------------------------------- clocks --
-class ClockSampler:
+class NvmlClockSampler:
+    """SM clocks, power and clock-event (throttle) reasons sampled in-process
+    through NVML by a thread, every 50 ms, during the timed region: one sample
+    before it starts and one after it ends.  An nvidia-smi process polling the
+    same fields stalled the solves it overlapped (a 21 ms solve measured
+    44 ms), so NVML is the first choice and nvidia-smi the fallback."""
+
+    PERIOD_S = 0.05
+
+    def __init__(self, gpu_index):
+        import pynvml
+        self.nv = pynvml
+        self.idx = gpu_index
+        self.rows = []
+        self.stop = threading.Event()
+        self.thread = None
+
+    def _sample(self):
+        nv, h = self.nv, self.h
+        try:
+            reasons = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        except AttributeError:
+            reasons = nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+        self.rows.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM),
+                          nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM),
+                          nv.nvmlDeviceGetPowerUsage(h) / 1000.0, int(reasons)))
+
+    def _run(self):
+        while not self.stop.wait(self.PERIOD_S):
+            self._sample()
+
+    def _handle(self):
+        """The NVML device of CUDA device idx, matched by PCI address (NVML
+        numbers every GPU of the node, CUDA only the visible ones)."""
+        try:
+            import torch
+            p = torch.cuda.get_device_properties(self.idx)
+            bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+            return self.nv.nvmlDeviceGetHandleByPciBusId(bus.encode())
+        except Exception:
+            return self.nv.nvmlDeviceGetHandleByIndex(self.idx)
+
+    def __enter__(self):
+        self.nv.nvmlInit()
+        self.h = self._handle()
+        self._sample()
+        self.thread = threading.Thread(target=self._run, daemon=True)
+        self.thread.start()
+        return self
+
+    def __exit__(self, *a):
+        self.stop.set()
+        self.thread.join(timeout=5)
+        self._sample()
+        self.nv.nvmlShutdown()
+
+    def summary(self):
+        if not self.rows:
+            return None
+        nv = self.nv
+        bits = {"hw_slowdown": nv.nvmlClocksThrottleReasonHwSlowdown,
+                "hw_thermal_slowdown": nv.nvmlClocksThrottleReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": nv.nvmlClocksThrottleReasonSwThermalSlowdown,
+                "sw_power_cap": nv.nvmlClocksThrottleReasonSwPowerCap}
+        sm = [r[0] for r in self.rows]
+        loaded = [r[0] for r in self.rows if r[2] > 200] or sm
+        reasons = sorted({k for r in self.rows for k, b in bits.items() if r[3] & b})
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(r[1] for r in self.rows), "reasons": reasons,
+                "samples": len(self.rows), "source": "nvml"}
+
+
+def ClockSampler(gpu_index):
+    try:
+        import pynvml  # noqa: F401
+        return NvmlClockSampler(gpu_index)
+    except ImportError:
+        return SmiClockSampler(gpu_index)
+
+
+class SmiClockSampler:
     """nvidia-smi clocks / throttle reasons sampled during the timed region."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"

@@ -290,7 +290,8 @@ int svdb_release_cached_memory(void);
  * chain with SVDLIBC's / the current pythag (src/legacy.rs:1590-1700,
  * src/lanczos/mod.rs:901-1028), max_it its cap.  d and e (order n, e[0]
  * unused) are host arrays, overwritten with the results as the host routines
- * leave them; bnd (routines 0-1) gets the bounds row, perm (2-3) imtql2's
+ * leave them; bnd (routines 0-1, in and out: order 1 leaves it as given)
+ * gets the bounds row, perm (2-3) imtql2's
  * column order; the first rot_cap plane rotations (i, c, s) are returned and
  * *n_rot counts them all (routine 1 records none).  *device_ms is the kernel's
  * time.  Errors: SVDB_ERR_IMTQLB / SVDB_ERR_IMTQL2 as the crate raises them.

@@ -71,7 +71,7 @@ __device__ __forceinline__ bool grid_sync(GridBarrier* bar, unsigned int expecte
             unsigned int spins = 0;
             while (gen.load(cuda::memory_order_acquire) == g) {
                 if (err.load(cuda::memory_order_relaxed) != 0) { ok = 0; break; }
-                if ((++spins & 255u) == 0 && global_ns() - t0 > limit) {
+                if ((++spins & 15u) == 0 && global_ns() - t0 > limit) {
                     err.store(8 /* SVDB_ERR_TIMEOUT */, cuda::memory_order_relaxed);
                     ok = 0;
                     break;

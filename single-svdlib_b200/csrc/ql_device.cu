@@ -329,6 +329,8 @@ extern "C" int svdb_tridiag_device(int routine, uint64_t n, double* d, double* e
             DevBuf<int> dst(2, s);
             SVDB_CUDA(cudaMemcpyAsync(dd.p, d, n * 8, cudaMemcpyHostToDevice, s));
             SVDB_CUDA(cudaMemcpyAsync(de.p, e, n * 8, cudaMemcpyHostToDevice, s));
+            // bnd is in and out, as the reference's array: order 1 leaves it as given
+            if (routine <= 1) SVDB_CUDA(cudaMemcpyAsync(db.p, bnd, n * 8, cudaMemcpyHostToDevice, s));
             SVDB_CUDA(cudaEventCreate(&e0));
             SVDB_CUDA(cudaEventCreate(&e1));
             SVDB_CUDA(cudaEventRecord(e0, s));
