@@ -17,6 +17,9 @@ int group_for(double avg);
 // Instantiated for (double, double), (float, float) and (float, double).
 template <typename XT, typename OT>
 void spmm_dev(const DevCompressed& m, bool fp32, const XT* X, int l, OT* Y, cudaStream_t s);
+// FP32 values and operand, the operand's rows ldx floats apart (a multiple of 32), FP64 output
+bool spmm_f32_strided_ok(const DevCompressed& m, int l, int64_t ldx);
+void spmm_f32_strided(const DevCompressed& m, const float* X, int l, int64_t ldx, double* Y, cudaStream_t s);
 // Raises the error a TMA gather wait of an earlier SpMM recorded (synchronises).
 void spmm_tma_check();
 // FP32 SpMM by panels of X in shared memory (spmm_panel.cu); the plan is

@@ -253,6 +253,16 @@ __global__ void k_to_float(const double* __restrict__ in, float* __restrict__ ou
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         out[i] = (float)in[i];
 }
+
+// out (rows x ldx) = in (rows x c), rounded to FP32; columns c .. ldx-1 are not written
+__global__ void k_to_float_ld(const double* __restrict__ in, float* __restrict__ out, int64_t rows, int c,
+                              int64_t ldx) {
+    const int64_t n = rows * c;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = i / c;
+        out[r * ldx + (i - r * c)] = (float)in[i];
+    }
+}
 // copy the first `cout` columns of X (rows x c) into Out (rows x cout)
 __global__ void k_take_cols(const double* __restrict__ X, int64_t rows, int c, int cout, double* __restrict__ Out) {
     const int64_t total = rows * cout;
@@ -561,11 +571,19 @@ void randomized(const svdb_matrix* A, uint64_t target_rank, uint64_t n_oversampl
         if (!mixed) {
             spmm_dev<double, double>(M, false, X, c, Y, s);
         } else {
-            if ((int64_t)f_in.n < M.nminor * c) f_in.alloc(M.nminor * c, s);
-            k_to_float<<<nb(M.nminor * c, 256), 256, 0, s>>>(X, f_in.p, M.nminor * c);
-            SVDB_CHECK_LAUNCH();
-            if (split) dense_split_spmm<double, double>(A, &M == &Acsc, X, f_in.p, c, Y, s);
-            else spmm_dev<float, double>(M, true, f_in.p, c, Y, s);
+            const int64_t ldp = ((int64_t)c + 31) / 32 * 32;  // rows on whole 128-byte lines
+            if (!split && spmm_f32_strided_ok(M, c, ldp)) {
+                if ((int64_t)f_in.n < M.nminor * ldp) f_in.alloc(M.nminor * ldp, s);
+                k_to_float_ld<<<nb(M.nminor * c, 256), 256, 0, s>>>(X, f_in.p, M.nminor, c, ldp);
+                SVDB_CHECK_LAUNCH();
+                spmm_f32_strided(M, f_in.p, c, ldp, Y, s);
+            } else {
+                if ((int64_t)f_in.n < M.nminor * c) f_in.alloc(M.nminor * c, s);
+                k_to_float<<<nb(M.nminor * c, 256), 256, 0, s>>>(X, f_in.p, M.nminor * c);
+                SVDB_CHECK_LAUNCH();
+                if (split) dense_split_spmm<double, double>(A, &M == &Acsc, X, f_in.p, c, Y, s);
+                else spmm_dev<float, double>(M, true, f_in.p, c, Y, s);
+            }
         }
         SVDB_CUDA(cudaEventRecord(b, s));
         spmm_events.emplace_back(a, b);

@@ -167,6 +167,98 @@ __global__ void __launch_bounds__(256, sizeof(XT) == 4 ? 4 : 3) k_spmm_seg(const
     }
 }
 
+// FP32 values and FP32 dense operand, l <= 64 (H = 2) or <= 32 (H = 4),
+// rows of X 16-byte aligned: the same segments, lane groups and summation
+// order as k_spmm_seg (group g takes entries g, g + H, ... of a 32-entry
+// chunk, FP32 within the chunk, FP64 across chunks), with fewer instructions
+// per entry.  k_spmm_seg spent about 21 warp instructions per nonzero (its
+// shuffles, 64-bit address arithmetic and per-entry bounds tests), and with
+// X resident in L1 it was bound by instruction issue, not by memory.  Here a
+// chunk's (row offset, value) pairs are written once to a per-warp shared
+// buffer and read back by broadcast, offsets are 32-bit, and full chunks run
+// without bounds tests with eight gathers in flight per lane.
+constexpr int kF32Warps = 8;
+template <typename OT, int H>
+__global__ void __launch_bounds__(kF32Warps * 32, 2)
+    k_spmm_f32(const int32_t* __restrict__ ci, const float* __restrict__ val, const int32_t* __restrict__ seg_row,
+               const int64_t* __restrict__ seg_beg, const int64_t* __restrict__ seg_end, int64_t nseg,
+               const float* __restrict__ X, int32_t ldx, int l, OT* __restrict__ Y, int64_t ldy,
+               double* __restrict__ part) {
+    constexpr int GL = 32 / H;        // lanes per group
+    constexpr int PER = 32 / H;       // entries of a chunk per group
+    constexpr int U = 8;              // gathers in flight per lane
+    __shared__ int2 s_ent[kF32Warps][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int g = lane / GL, gl = lane % GL;
+    const int col0 = gl * 4;
+    const int ncols_here = (l - col0) < 4 ? (l - col0) : 4;
+    const bool active = ncols_here > 0;
+    const float* Xl = X + (active ? col0 : 0);
+    int2* E = s_ent[w];
+    const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t sg = gwarp; sg < nseg; sg += nwarps) {
+        const int32_t rr = __ldg(seg_row + sg);
+        const int64_t a = __ldg(seg_beg + sg), b = __ldg(seg_end + sg);
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        int32_t myc = 0;
+        float myv = 0.f;
+        if (a + lane < b) { myc = __ldg(ci + a + lane); myv = __ldg(val + a + lane); }
+        for (int64_t k0 = a; k0 < b; k0 += 32) {
+            const int cnt = (b - k0) < 32 ? (int)(b - k0) : 32;
+            __syncwarp();  // the previous chunk's entries have been read
+            E[lane] = make_int2(myc * ldx, __float_as_int(myv));
+            __syncwarp();
+            if (k0 + 32 + lane < b) {  // the next chunk's pairs, while this one is used
+                myc = __ldg(ci + k0 + 32 + lane);
+                myv = __ldg(val + k0 + 32 + lane);
+            }
+            float c4[4] = {0.f, 0.f, 0.f, 0.f};
+            if (cnt == 32) {
+#pragma unroll 1
+                for (int qb = 0; qb < PER; qb += U) {  // batches of U gathers, one batch live at a time
+                    float4 xv[U];
+                    float vv[U];
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        const int2 e = E[(qb + u) * H + g];
+                        vv[u] = __int_as_float(e.y);
+                        xv[u] = active ? *reinterpret_cast<const float4*>(Xl + e.x) : make_float4(0.f, 0.f, 0.f, 0.f);
+                    }
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        c4[0] = fmaf(vv[u], xv[u].x, c4[0]);
+                        c4[1] = fmaf(vv[u], xv[u].y, c4[1]);
+                        c4[2] = fmaf(vv[u], xv[u].z, c4[2]);
+                        c4[3] = fmaf(vv[u], xv[u].w, c4[3]);
+                    }
+                }
+            } else {
+                for (int q = g; q < cnt; q += H) {
+                    const int2 e = E[q];
+                    const float v = __int_as_float(e.y);
+                    const float4 x = active ? *reinterpret_cast<const float4*>(Xl + e.x)
+                                            : make_float4(0.f, 0.f, 0.f, 0.f);
+                    c4[0] = fmaf(v, x.x, c4[0]);
+                    c4[1] = fmaf(v, x.y, c4[1]);
+                    c4[2] = fmaf(v, x.z, c4[2]);
+                    c4[3] = fmaf(v, x.w, c4[3]);
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[j] += (double)c4[j];
+        }
+#pragma unroll
+        for (int o = GL; o < 32; o <<= 1)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[j] += __shfl_xor_sync(0xffffffffu, acc[j], o);
+        if (g == 0 && active) {
+            if (rr >= 0) store_cols<OT, 4>(Y + (int64_t)rr * ldy + col0, ncols_here, acc);
+            else store_cols<double, 4>(part + sg * (int64_t)l + col0, ncols_here, acc);
+        }
+    }
+}
+
 // rows split into several segments: add their partials in segment order
 template <typename OT>
 __global__ void k_spmm_merge(const int64_t* __restrict__ seg_first, const int32_t* __restrict__ multi_rows,
@@ -303,10 +395,52 @@ static void launch_seg(const DevCompressed& m, const VT* v, const XT* X, int64_t
     SVDB_CHECK_LAUNCH();
 }
 
+// k_spmm_f32 applies: FP32 values and operand, l <= 64 and a multiple of 4,
+// a 16-byte aligned operand, 32-bit element offsets (nminor * l < 2^31), and
+// SVDB_SPMM=seg not set (that keeps k_spmm_seg, for comparisons)
+template <typename VT, typename XT>
+static bool f32_eligible(const DevCompressed& m, const XT* X, int l) {
+    if constexpr (!(std::is_same<VT, float>::value && std::is_same<XT, float>::value)) {
+        return false;
+    } else {
+        const char* e = getenv("SVDB_SPMM");
+        if (e && std::string(e) == "seg") return false;
+        return l >= 1 && l <= 64 && l % 4 == 0 && (reinterpret_cast<uintptr_t>(X) % 16) == 0 &&
+               m.nminor * (int64_t)l < ((int64_t)1 << 31);
+    }
+}
+
+template <typename OT>
+static void launch_f32(const DevCompressed& m, const float* v, const float* X, int l, OT* Y, double* part,
+                       cudaStream_t s, int64_t ldx = 0) {
+    if (ldx == 0) ldx = l;
+    const int64_t ns = m.plan.nseg;
+    if (ns <= 0) return;
+    const int blocks = nblk(ns * 32, kF32Warps * 32, 2 * 8);
+    if (l <= 32)
+        k_spmm_f32<OT, 4><<<blocks, kF32Warps * 32, 0, s>>>(m.idx.p, v, m.plan.seg_row.p, m.plan.seg_beg.p,
+                                                            m.plan.seg_end.p, ns, X, (int32_t)ldx, l, Y, l, part);
+    else
+        k_spmm_f32<OT, 2><<<blocks, kF32Warps * 32, 0, s>>>(m.idx.p, v, m.plan.seg_row.p, m.plan.seg_beg.p,
+                                                            m.plan.seg_end.p, ns, X, (int32_t)ldx, l, Y, l, part);
+    SVDB_CHECK_LAUNCH();
+}
+
 template <typename VT, typename XT, typename OT>
 static void spmm_impl(const DevCompressed& m, const VT* v, const XT* X, int l, OT* Y, cudaStream_t s) {
     DevBuf<double> part;
     if (m.plan.nmulti) part.alloc(m.plan.nseg * (int64_t)std::min(l, 128), s);
+    if constexpr (std::is_same<VT, float>::value && std::is_same<XT, float>::value) {
+        if (f32_eligible<VT, XT>(m, X, l)) {
+            launch_f32<OT>(m, v, X, l, Y, part.p, s);
+            if (m.plan.nmulti) {
+                k_spmm_merge<OT><<<nblk(m.plan.nmulti * 32, 256, 16), 256, 0, s>>>(
+                    m.plan.seg_first.p, m.plan.multi_rows.p, m.plan.nmulti, part.p, l, Y, l);
+                SVDB_CHECK_LAUNCH();
+            }
+            return;
+        }
+    }
     for (int c0 = 0; c0 < l; c0 += 128) {
         const int lc = std::min(128, l - c0);
         const XT* Xc = X + c0;
@@ -578,6 +712,31 @@ static void heavy_segments_f32(const DevCompressed& m, const int32_t* row, const
         k_spmm_seg<float, float, double, 4, 2, 4><<<blocks, 256, 0, s>>>(m.idx.p, m.val32.p, row, beg, end, n, X, l,
                                                                          l, vec, Y, l, part);
     SVDB_CHECK_LAUNCH();
+}
+
+// FP32 products with the dense operand's rows ldx floats apart (ldx >= l, a
+// multiple of 32: every row starts on a 128-byte line, so a gathered row of
+// l <= 64 floats touches whole lines only).  False when k_spmm_f32 does not
+// apply (the caller then keeps the unpadded path).
+bool spmm_f32_strided_ok(const DevCompressed& m, int l, int64_t ldx) {
+    const char* e = getenv("SVDB_SPMM");
+    if (e && *e) return false;  // an explicit kernel choice keeps the unpadded path
+    return m.val32.p && m.nnz > 0 && l >= 1 && l <= 64 && l % 4 == 0 && ldx >= l && ldx % 32 == 0 &&
+           m.nminor * ldx < ((int64_t)1 << 31);
+}
+
+void spmm_f32_strided(const DevCompressed& m, const float* X, int l, int64_t ldx, double* Y, cudaStream_t s) {
+    if (m.nmajor == 0) return;
+    if (!spmm_f32_strided_ok(m, l, ldx) || (reinterpret_cast<uintptr_t>(X) % 16))
+        throw Error(SVDB_ERR_ARG, "spmm_f32_strided: operand layout not supported");
+    DevBuf<double> part;
+    if (m.plan.nmulti) part.alloc(m.plan.nseg * (int64_t)l, s);
+    launch_f32<double>(m, m.val32.p, X, l, Y, part.p, s, ldx);
+    if (m.plan.nmulti) {
+        k_spmm_merge<double><<<nblk(m.plan.nmulti * 32, 256, 16), 256, 0, s>>>(m.plan.seg_first.p, m.plan.multi_rows.p,
+                                                                              m.plan.nmulti, part.p, l, Y, l);
+        SVDB_CHECK_LAUNCH();
+    }
 }
 
 template <typename XT, typename OT>
