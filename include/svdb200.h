@@ -329,7 +329,7 @@ int svdb_sliced_spmv_info(const svdb_matrix* a, int transposed, int32_t* nslices
  * a dense block on the tensor cores (3xTF32, FP64 drains), and the nonzeros
  * they hold; both 0 before the first FP32 product or when no split is used
  * (too few dense columns, more than 64 dense operand columns, or
- * SVDB_DENSE_SPLIT=0). */
+ * SVDB_DENSE_SPLIT is not 1: the split is opt-in). */
 int svdb_dense_split_info(const svdb_matrix* a, uint64_t* dense_cols, uint64_t* dense_nnz);
 
 /* Number of kernels this library has launched in the process so far. */

@@ -107,6 +107,7 @@ def test_batch_dense_split_against_gather_and_f64(monkeypatch):
     A = M.dense_columns(5000, 2400, 300, 17)
     subs = subsets_of(2400, 9, 150, 2000, 6)
     rank, over, q, seed = 12, 8, 2, 4
+    monkeypatch.setenv("SVDB_DENSE_SPLIT", "1")  # the split is opt-in
     h = upload("csr", A)
     got = randomized.randomized_svd_batch(h, subs, rank, over, q, PIN.QR, seed, precision="mixed")
     nd, nnz = C.c_uint64(0), C.c_uint64(0)
@@ -116,7 +117,6 @@ def test_batch_dense_split_against_gather_and_f64(monkeypatch):
     h2 = upload("csr", A)
     gat = randomized.randomized_svd_batch(h2, subs, rank, over, q, PIN.QR, seed, precision="mixed")
     assert _abi.lib().svdb_dense_split_info(h2.handle, C.byref(nd), C.byref(nnz)) == 0 and nd.value == 0
-    monkeypatch.delenv("SVDB_DENSE_SPLIT")
     for cols, g, r in list(zip(subs, got, gat))[:4]:
         ref = single(A, h2, cols, rank, over, q, PIN.QR, seed, "f64")
         assert np.max(np.abs(g.s - ref.s) / ref.s) < 1e-6

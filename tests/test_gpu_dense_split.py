@@ -22,6 +22,11 @@ from single_svdlib.randomized import PowerIterationNormalizer as PIN
 pytestmark = pytest.mark.gpu
 
 
+@pytest.fixture(autouse=True)
+def _split_on(monkeypatch):
+    monkeypatch.setenv("SVDB_DENSE_SPLIT", "1")  # the split is opt-in
+
+
 def dense_cols_matrix(m, n, nd, seed):
     """nd columns with densities uniform in (0.1, 0.4), the others at 0.004."""
     return M.dense_columns(m, n, nd, seed)
@@ -66,7 +71,7 @@ def test_products_match_checker(m, n, nd, l, monkeypatch):
     rng = np.random.default_rng(l)
     for transpose in (False, True):
         X = rng.standard_normal((m if transpose else n, l))
-        monkeypatch.delenv("SVDB_DENSE_SPLIT", raising=False)
+        monkeypatch.setenv("SVDB_DENSE_SPLIT", "1")
         split = device_product(h, X, transpose)
         nd_used, dense_nnz = split_info(h)
         assert nd_used == nd and 0 < dense_nnz < len(A["data"])
