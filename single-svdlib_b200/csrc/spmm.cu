@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(256, sizeof(XT) == 4 ? 4 : 3) k_spmm_seg(const
 // without bounds tests with eight gathers in flight per lane.
 constexpr int kF32Warps = 8;
 template <typename OT, int H>
-__global__ void __launch_bounds__(kF32Warps * 32, 2)
+__global__ void __launch_bounds__(kF32Warps * 32, 4)
     k_spmm_f32(const int32_t* __restrict__ ci, const float* __restrict__ val, const int32_t* __restrict__ seg_row,
                const int64_t* __restrict__ seg_beg, const int64_t* __restrict__ seg_end, int64_t nseg,
                const float* __restrict__ X, int32_t ldx, int l, OT* __restrict__ Y, int64_t ldy,
@@ -416,7 +416,7 @@ static void launch_f32(const DevCompressed& m, const float* v, const float* X, i
     if (ldx == 0) ldx = l;
     const int64_t ns = m.plan.nseg;
     if (ns <= 0) return;
-    const int blocks = nblk(ns * 32, kF32Warps * 32, 2 * 8);
+    const int blocks = nblk(ns * 32, kF32Warps * 32, 4 * 8);
     if (l <= 32)
         k_spmm_f32<OT, 4><<<blocks, kF32Warps * 32, 0, s>>>(m.idx.p, v, m.plan.seg_row.p, m.plan.seg_beg.p,
                                                             m.plan.seg_end.p, ns, X, (int32_t)ldx, l, Y, l, part);
