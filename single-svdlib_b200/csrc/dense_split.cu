@@ -710,7 +710,7 @@ static double dense_min_density() {
     return 0.08;
 }
 
-// Opt-in (SVDB_DENSE_SPLIT=1): with the lean gather kernel (k_spmm_f32) the
+// Opt-in (SVDB_DENSE_SPLIT=1): with the lean gather kernel (k_spmm_lean) the
 // split no longer shortens the randomized solve of the count-like workload
 // (17.66 against 17.68 ms) and its sigma moves from 1e-8 to 2e-7 of the FP64
 // solve, so the row gathers are the default.
