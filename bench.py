@@ -1179,6 +1179,10 @@ def main():
     peak, peak_kind = peak_hbm()
     dominant = "spmm_csc_AtY" if ms_atx >= ms_ax else "spmm_csr_AZ"
     ach = gbs_atx if ms_atx >= ms_ax else gbs_ax
+    # what bounds the kernel: every nonzero gathers a row of l FP32 values of
+    # the dense operand (which sits in L2), l * 4 bytes through L2 and L1
+    gathered = nnz * l * 4
+    gather = {"bytes_per_launch": gathered, "tbps_AZ": gathered / ms_ax / 1e9, "tbps_AtY": gathered / ms_atx / 1e9}
 
     ms_mixed = max_over_ranks(ms_mixed, world)
     ms_f64 = max_over_ranks(ms_f64, world)
@@ -1214,8 +1218,8 @@ def main():
             "sigma_rel_err_vs_f64": sigma_err,
             "sigma_rel_err_vs_oracle": sig_oracle,
             "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                         "traffic": profiled_traffic("spmm_randomized_100kx30k.md"), "kernel": dominant,
-                         "peak_source": peak_kind,
+                         "traffic": profiled_traffic("spmm_f32_randomized_100kx30k.md"), "kernel": dominant,
+                         "kernel_name": "k_spmm_f32", "peak_source": peak_kind, "l2_row_gathers": gather,
                          "spmm_csr_AZ": {"ms": ms_ax, "gbs": gbs_ax, "bytes": bytes_ax},
                          "spmm_csc_AtY": {"ms": ms_atx, "gbs": gbs_atx, "bytes": bytes_atx}},
             "cpu_baseline": cpu,
