@@ -212,6 +212,197 @@ __global__ void __launch_bounds__(256) k_b_spmm_cols(const int64_t* __restrict__
     }
 }
 
+// ------------------------------------------------- lean batch products ----
+// The products of an SVDB_MIXED batch (FP32 values and dense operands, l a
+// multiple of 4 up to 64) with the instruction stream of k_spmm_f32: a
+// chunk's 32 entries are loaded by the warp one chunk ahead, the entries
+// that count are staged once in a per-warp shared buffer as (row offset,
+// value) and read back by broadcast, lane groups of 32 / H lanes take every
+// H-th staged entry with one 16-byte gather of four columns each (FP32 sums
+// per chunk, FP64 across chunks, groups combined in a fixed xor tree).  The
+// kernels above spend a warp instruction per entry and subset (a shuffle, a
+// membership test and scalar gathers per entry).
+constexpr int kBLeanWarps = 8;
+constexpr int kBLeanU = 8;  // gathers in flight per lane
+
+// sum over staged entries q = g, g + H, ... < cnt of v_q X[off_q + col0 ..
+// col0 + 3]: batches of kBLeanU gathers issued before their FMAs; a full
+// chunk (cnt == 32) needs no bounds tests
+template <int H>
+__device__ __forceinline__ void lean_chunk(const int2* __restrict__ E, int cnt, int g, bool active,
+                                           const float* __restrict__ Xl, float (&c4)[4]) {
+    constexpr int PER = 32 / H;
+    if (cnt == 32) {
+#pragma unroll 1
+        for (int qb = 0; qb < PER; qb += kBLeanU) {
+            float4 xv[kBLeanU];
+            float vv[kBLeanU];
+#pragma unroll
+            for (int u = 0; u < kBLeanU; ++u) {
+                const int2 en = E[(qb + u) * H + g];
+                vv[u] = __int_as_float(en.y);
+                xv[u] = active ? *reinterpret_cast<const float4*>(Xl + en.x) : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+#pragma unroll
+            for (int u = 0; u < kBLeanU; ++u) {
+                c4[0] = fmaf(vv[u], xv[u].x, c4[0]);
+                c4[1] = fmaf(vv[u], xv[u].y, c4[1]);
+                c4[2] = fmaf(vv[u], xv[u].z, c4[2]);
+                c4[3] = fmaf(vv[u], xv[u].w, c4[3]);
+            }
+        }
+    } else {
+#pragma unroll 1
+        for (int qb = g; qb < cnt; qb += H * kBLeanU) {
+            float4 xv[kBLeanU];
+            float vv[kBLeanU];
+#pragma unroll
+            for (int u = 0; u < kBLeanU; ++u) {
+                const int q = qb + u * H;
+                const bool ok = q < cnt && active;
+                const int2 en = E[q < cnt ? q : 0];
+                vv[u] = ok ? __int_as_float(en.y) : 0.f;
+                xv[u] = ok ? *reinterpret_cast<const float4*>(Xl + en.x) : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+#pragma unroll
+            for (int u = 0; u < kBLeanU; ++u) {
+                c4[0] = fmaf(vv[u], xv[u].x, c4[0]);
+                c4[1] = fmaf(vv[u], xv[u].y, c4[1]);
+                c4[2] = fmaf(vv[u], xv[u].z, c4[2]);
+                c4[3] = fmaf(vv[u], xv[u].w, c4[3]);
+            }
+        }
+    }
+}
+
+// Items are taken in order from a counter (*next, zero at launch), one per
+// warp at a time: the items in flight stay one contiguous window of the
+// subset-major order, so only a few subsets' dense operands are in use at
+// once (with a static grid stride, warps held by long columns fall behind
+// and the window spreads over many subsets, whose operands then compete for
+// L2).  An item's sums do not depend on which warp takes it.
+__device__ __forceinline__ int64_t lean_next(unsigned long long* next, int lane) {
+    unsigned long long it = 0;
+    if (lane == 0) it = atomicAdd(next, 1ull);
+    return (int64_t)__shfl_sync(0xffffffffu, it, 0);
+}
+
+// Y_b = A_b X_b, one warp per (subset, row) item, subset-major; an entry
+// (c, v) of row r counts for subset b when o2m_b[c] >= 0, and the staged
+// list holds only those (ballot compaction, in entry order).
+template <int H>
+__global__ void __launch_bounds__(kBLeanWarps * 32, 4)
+    k_b_rows_lean(const int64_t* __restrict__ rp, const int32_t* __restrict__ ci, const float* __restrict__ val,
+                  int64_t m, const int32_t* __restrict__ o2m, int64_t n, const int64_t* __restrict__ coff,
+                  int64_t count, int l, const float* __restrict__ X, float* __restrict__ Y,
+                  unsigned long long* __restrict__ next) {
+    constexpr int GL = 32 / H;
+    __shared__ int2 s_ent[kBLeanWarps][32];
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int g = lane / GL, gl = lane % GL;
+    const int col0 = gl * 4;
+    const int ncols_here = (l - col0) < 4 ? (l - col0) : 4;
+    const bool active = ncols_here > 0;
+    int2* E = s_ent[w];
+    const int64_t items = count * m;
+    for (int64_t it = lean_next(next, lane); it < items; it = lean_next(next, lane)) {
+        const int64_t b = it / m, r = it - b * m;
+        const float* Xb = X + coff[b] * l + (active ? col0 : 0);
+        const int32_t* om = o2m + b * n;
+        const int64_t s = __ldg(rp + r), e = __ldg(rp + r + 1);
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        // chunk k's membership (jm) and value, and chunk k + 1's column, are
+        // loaded before chunk k is used, so a lookup overlaps a chunk's gathers
+        int32_t jm = -1, nxc = 0;
+        float myv = 0.f, nxv = 0.f;
+        if (s + lane < e) { myv = __ldg(val + s + lane); jm = __ldg(om + __ldg(ci + s + lane)); }
+        if (s + 32 + lane < e) { nxc = __ldg(ci + s + 32 + lane); nxv = __ldg(val + s + 32 + lane); }
+        for (int64_t k0 = s; k0 < e; k0 += 32) {
+            const unsigned mask = __ballot_sync(full, jm >= 0);
+            const int nk = __popc(mask);
+            __syncwarp();  // the previous chunk's entries have been read
+            if (jm >= 0) E[__popc(mask & ((1u << lane) - 1u))] = make_int2(jm * l, __float_as_int(myv));
+            __syncwarp();
+            jm = (k0 + 32 + lane < e) ? __ldg(om + nxc) : -1;
+            myv = nxv;
+            if (k0 + 64 + lane < e) {
+                nxc = __ldg(ci + k0 + 64 + lane);
+                nxv = __ldg(val + k0 + 64 + lane);
+            }
+            float c4[4] = {0.f, 0.f, 0.f, 0.f};
+            lean_chunk<H>(E, nk, g, active, Xb, c4);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[j] += (double)c4[j];
+        }
+#pragma unroll
+        for (int o = GL; o < 32; o <<= 1)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[j] += __shfl_xor_sync(full, acc[j], o);
+        if (g == 0 && active) {
+            float* yr = Y + (b * m + r) * l + col0;
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                if (j < ncols_here) yr[j] = (float)acc[j];
+        }
+    }
+}
+
+// Z_b[j] = sum over the entries (r, v) of column m2o_b[j] of A of v Y_b[r],
+// one warp per (subset, masked column) item, subset-major.
+template <typename OT, int H>
+__global__ void __launch_bounds__(kBLeanWarps * 32, 4)
+    k_b_cols_lean(const int64_t* __restrict__ cp, const int32_t* __restrict__ ri, const float* __restrict__ cv,
+                  int64_t m, const int32_t* __restrict__ m2o, const int64_t* __restrict__ coff, int64_t count, int l,
+                  const float* __restrict__ Y, OT* __restrict__ Z, unsigned long long* __restrict__ next) {
+    constexpr int GL = 32 / H;
+    __shared__ int2 s_ent[kBLeanWarps][32];
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int g = lane / GL, gl = lane % GL;
+    const int col0 = gl * 4;
+    const int ncols_here = (l - col0) < 4 ? (l - col0) : 4;
+    const bool active = ncols_here > 0;
+    int2* E = s_ent[w];
+    const int64_t total = coff[count];
+    int64_t b = 0;
+    for (int64_t it = lean_next(next, lane); it < total; it = lean_next(next, lane)) {
+        while (coff[b + 1] <= it) ++b;  // a warp's items rise, so b only moves forward
+        const float* Yb = Y + b * m * l + (active ? col0 : 0);
+        const int32_t c = m2o[it];
+        const int64_t s = __ldg(cp + c), e = __ldg(cp + c + 1);
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        int32_t myr = 0;
+        float myv = 0.f;
+        if (s + lane < e) { myr = __ldg(ri + s + lane); myv = __ldg(cv + s + lane); }
+        for (int64_t k0 = s; k0 < e; k0 += 32) {
+            const int cnt = (e - k0) < 32 ? (int)(e - k0) : 32;
+            __syncwarp();
+            E[lane] = make_int2(myr * l, __float_as_int(myv));
+            __syncwarp();
+            if (k0 + 32 + lane < e) {
+                myr = __ldg(ri + k0 + 32 + lane);
+                myv = __ldg(cv + k0 + 32 + lane);
+            }
+            float c4[4] = {0.f, 0.f, 0.f, 0.f};
+            lean_chunk<H>(E, cnt, g, active, Yb, c4);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[j] += (double)c4[j];
+        }
+#pragma unroll
+        for (int o = GL; o < 32; o <<= 1)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[j] += __shfl_xor_sync(full, acc[j], o);
+        if (g == 0 && active) {
+            OT* zr = Z + it * l + col0;
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                if (j < ncols_here) zr[j] = (OT)acc[j];
+        }
+    }
+}
+
+
 // --------------------------------------------------------- CholeskyQR2 ----
 // Gram partials: block (chunk, b) sums X_b^T X_b over its rows (32-row tiles
 // staged in shared memory; a 16 x 16 thread grid holds an NC x NC tile).
@@ -404,6 +595,7 @@ struct svdb_batch {
     svdb::DevBuf<double> Om64, Y64, Z64, Bt;
     svdb::DevBuf<double> part, G, R1, R2, R3, Ri, Rout, Rtmp, Ur, Vr, sig, U, Vt;
     svdb::DevBuf<int> flags, shifted, jstat;
+    svdb::DevBuf<unsigned long long> next;  // the lean product kernels' item counter
     // SVDB_MIXED with a dense-column split of A: the dense columns' share of
     // every product as one GEMM over all subsets (dense_split.cu); the B
     // operands of the row and column GEMMs and the column GEMM's tiles
@@ -433,11 +625,37 @@ static T* dense_ptr(svdb_batch& B, DevBuf<float>& f, DevBuf<double>& d) {
     else return d.p;
 }
 
+// the lean kernels apply to SVDB_MIXED batches with l a multiple of 4
+// (16-byte rows), 32-bit offsets, and SVDB_BATCH_SPMM=warp not set
+static bool lean_batch(const svdb_batch& B, int64_t rows_per_item_operand) {
+    const char* e = getenv("SVDB_BATCH_SPMM");
+    if (e && std::string(e) == "warp") return false;
+    return B.mixed && B.l % 4 == 0 && B.l <= 64 && rows_per_item_operand * B.l < ((int64_t)1 << 31);
+}
+
 // Y_b = A_b X_b with `gs` subsets per row item
 template <typename T>
 static void rows_product(svdb_batch& B, const T* X, T* Y, int gs) {
     // with the split: the rest of A here, the dense columns below
     const DevCompressed& A = B.dsplit ? B.dsplit->rest_csr : csr_of(B.A);
+    if constexpr (std::is_same<T, float>::value) {
+        if (lean_batch(B, B.n)) {
+            const int blocks = grid_cap(4);  // the resident blocks; items come from the counter
+            SVDB_CUDA(cudaMemsetAsync(B.next.p, 0, sizeof(unsigned long long), B.s));
+            if (B.l <= 32)
+                k_b_rows_lean<4><<<blocks, kBLeanWarps * 32, 0, B.s>>>(A.ptr.p, A.idx.p, A.val32.p, B.m, B.o2m.p,
+                                                                       B.n, B.coff.p, B.count, (int)B.l, X, Y,
+                                                                       B.next.p);
+            else
+                k_b_rows_lean<2><<<blocks, kBLeanWarps * 32, 0, B.s>>>(A.ptr.p, A.idx.p, A.val32.p, B.m, B.o2m.p,
+                                                                       B.n, B.coff.p, B.count, (int)B.l, X, Y,
+                                                                       B.next.p);
+            SVDB_CHECK_LAUNCH();
+            if (B.dsplit)
+                dense_batch_rows(B.A, X, B.coff.p, B.o2m.p, B.count, (int)B.l, Y, B.dbh_r.p, B.dbl_r.p, B.s);
+            return;
+        }
+    }
     const int blocks = grid_cap(6);
 #define SVDB_ROWS(GS)                                                                                             \
     case GS:                                                                                                      \
@@ -468,6 +686,25 @@ static void cols_product(svdb_batch& B, const T* Y, OT* Z) {
     // with the split: the rest of A^T here (rows of the dense columns empty,
     // so their Z rows are written as 0), the dense columns below
     const DevCompressed& At = B.dsplit ? B.dsplit->rest_csc : csc_of(B.A);
+    if constexpr (std::is_same<T, float>::value) {
+        if (lean_batch(B, B.m)) {
+            const int blocks = grid_cap(4);  // the resident blocks; items come from the counter
+            SVDB_CUDA(cudaMemsetAsync(B.next.p, 0, sizeof(unsigned long long), B.s));
+            if (B.l <= 32)
+                k_b_cols_lean<OT, 4><<<blocks, kBLeanWarps * 32, 0, B.s>>>(At.ptr.p, At.idx.p, At.val32.p, B.m,
+                                                                           B.m2o.p, B.coff.p, B.count, (int)B.l, Y, Z,
+                                                                           B.next.p);
+            else
+                k_b_cols_lean<OT, 2><<<blocks, kBLeanWarps * 32, 0, B.s>>>(At.ptr.p, At.idx.p, At.val32.p, B.m,
+                                                                           B.m2o.p, B.coff.p, B.count, (int)B.l, Y, Z,
+                                                                           B.next.p);
+            SVDB_CHECK_LAUNCH();
+            if (B.dsplit)
+                dense_batch_cols<OT>(B.A, Y, B.coff.p, B.o2m.p, B.count, (int)B.l, Z, B.dbh_c.p, B.dbl_c.p,
+                                     B.dpart.p, B.s);
+            return;
+        }
+    }
     const int blocks = grid_cap(8);
     if (B.mixed)
         k_b_spmm_cols<float, T, OT, 2><<<blocks, 256, 0, B.s>>>(At.ptr.p, At.idx.p, At.val32.p, B.m, B.m2o.p,
@@ -684,6 +921,7 @@ void batch_create(const svdb_matrix* A, const uint64_t* col_off, const uint64_t*
     B->U.alloc(count * m * (int64_t)target_rank, s);
     B->Vt.alloc(tc * (int64_t)target_rank, s);
     B->flags.alloc(count, s);
+    B->next.alloc(1, s);
     B->shifted.alloc(count, s);
     B->jstat.alloc(count, s);
     {

@@ -521,6 +521,8 @@ static void launch_lean(const DevCompressed& m, const T* v, const T* X, int l, O
     if (ns <= 0) return;
     constexpr bool f32 = std::is_same<T, float>::value;
     constexpr int U = f32 ? 8 : 4, MINB = f32 ? 4 : 3;
+    // 8x the resident blocks: timed against the resident blocks only, 1.10
+    // against 1.20 ms for A X of the 100k x 30k workload
     const int blocks = nblk(ns * 32, kF32Warps * 32, MINB * 8);
     if constexpr (f32) {
         if (l <= 32)
