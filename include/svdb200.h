@@ -422,7 +422,7 @@ typedef struct svdb_batch_options {
 
 typedef struct svdb_batch_info {
     uint64_t count;
-    int32_t subsets_per_row_item; /* autotuned: subsets sharing one read of a row of A */
+    int32_t subsets_per_row_item; /* autotuned: subsets sharing one read of a row of A (1, untuned, under SVDB_MIXED) */
     int32_t columns_per_lane;     /* autotuned: dense columns per lane (vector width) */
     uint64_t graph_nodes;         /* kernels and copies in the captured graph (0 without) */
     uint64_t kernels_per_run;     /* kernel launches of one run */

@@ -965,6 +965,11 @@ void batch_create(const svdb_matrix* A, const uint64_t* col_off, const uint64_t*
         auto it = g_tuned.find(key);
         if (it != g_tuned.end()) { gs = it->second; cached = true; }
     }
+    // the lean row kernel (SVDB_MIXED) takes one subset per item: nothing to tune
+    if (!cached && lean_batch(*B, n)) {
+        gs = 1;
+        cached = true;
+    }
     if (!cached && o.autotune) {
         auto t0 = std::chrono::steady_clock::now();
         cudaEvent_t e0, e1;
