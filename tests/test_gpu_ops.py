@@ -102,15 +102,19 @@ def test_empty_rows_and_columns():
 
 @pytest.mark.parametrize("l", [1, 8, 30, 40, 60, 64, 96])
 @pytest.mark.parametrize("transpose", [False, True])
-@pytest.mark.parametrize("impl", ["seg", "tma"])
+@pytest.mark.parametrize("impl", ["lean", "seg", "tma"])
 def test_device_fp32_spmm_against_numpy(l, transpose, impl, monkeypatch):
     """svdb_multiply_with_dense_device with FP32 operands against numpy on
-    FP32-rounded inputs, through the register-gather kernel and the opt-in
-    tensor-memory gather kernel (SVDB_SPMM=tma; it takes rows that are 16-byte
-    multiples of at most 64 columns); includes a row long enough to be split
-    into several segments."""
+    FP32-rounded inputs, through the default kernels (k_spmm_f32 where l is a
+    multiple of 4 up to 64, else k_spmm_seg), the register-gather kernel
+    (SVDB_SPMM=seg) and the opt-in tensor-memory gather kernel (SVDB_SPMM=tma;
+    it takes rows that are 16-byte multiples of at most 64 columns); includes a
+    row long enough to be split into several segments."""
     import torch
-    monkeypatch.setenv("SVDB_SPMM", impl)
+    if impl == "lean":
+        monkeypatch.delenv("SVDB_SPMM", raising=False)
+    else:
+        monkeypatch.setenv("SVDB_SPMM", impl)
     from single_svdlib import _abi
     from single_svdlib._core import check
     rng = np.random.default_rng(l)
