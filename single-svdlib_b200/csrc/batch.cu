@@ -225,12 +225,13 @@ __global__ void __launch_bounds__(256) k_b_spmm_cols(const int64_t* __restrict__
 constexpr int kBLeanWarps = 8;
 constexpr int kBLeanU = 8;  // gathers in flight per lane
 
-// sum over staged entries q = g, g + H, ... < cnt of v_q X[off_q + col0 ..
-// col0 + 3]: batches of kBLeanU gathers issued before their FMAs; a full
-// chunk (cnt == 32) needs no bounds tests
+// sum over staged entries q = g, g + H, ... < cnt of v_q X[off_q + c0 ..
+// c0 + 3]: batches of kBLeanU gathers issued before their FMAs; a full chunk
+// (cnt == 32) needs no bounds tests.  X is the same for the whole warp and
+// the offsets are 32-bit (no 64-bit per-lane address arithmetic).
 template <int H>
 __device__ __forceinline__ void lean_chunk(const int2* __restrict__ E, int cnt, int g, bool active,
-                                           const float* __restrict__ Xl, float (&c4)[4]) {
+                                           const float* __restrict__ X, uint32_t c0, float (&c4)[4]) {
     constexpr int PER = 32 / H;
     if (cnt == 32) {
 #pragma unroll 1
@@ -241,7 +242,8 @@ __device__ __forceinline__ void lean_chunk(const int2* __restrict__ E, int cnt, 
             for (int u = 0; u < kBLeanU; ++u) {
                 const int2 en = E[(qb + u) * H + g];
                 vv[u] = __int_as_float(en.y);
-                xv[u] = active ? *reinterpret_cast<const float4*>(Xl + en.x) : make_float4(0.f, 0.f, 0.f, 0.f);
+                xv[u] = active ? *reinterpret_cast<const float4*>(X + ((uint32_t)en.x + c0))
+                               : make_float4(0.f, 0.f, 0.f, 0.f);
             }
 #pragma unroll
             for (int u = 0; u < kBLeanU; ++u) {
@@ -262,7 +264,7 @@ __device__ __forceinline__ void lean_chunk(const int2* __restrict__ E, int cnt, 
                 const bool ok = q < cnt && active;
                 const int2 en = E[q < cnt ? q : 0];
                 vv[u] = ok ? __int_as_float(en.y) : 0.f;
-                xv[u] = ok ? *reinterpret_cast<const float4*>(Xl + en.x) : make_float4(0.f, 0.f, 0.f, 0.f);
+                xv[u] = ok ? *reinterpret_cast<const float4*>(X + ((uint32_t)en.x + c0)) : make_float4(0.f, 0.f, 0.f, 0.f);
             }
 #pragma unroll
             for (int u = 0; u < kBLeanU; ++u) {
@@ -313,7 +315,8 @@ __global__ void __launch_bounds__(kBLeanWarps * 32, 4)
     const int64_t items = count * m;
     for (int64_t it = lean_next(next, lane); it < items; it = lean_next(next, lane)) {
         const int64_t b = it / m, r = it - b * m;
-        const float* Xb = X + coff[b] * l + (active ? col0 : 0);
+        const float* Xb = X + coff[b] * l;
+        const uint32_t c0a = active ? (uint32_t)col0 : 0u;
         const int32_t* om = o2m + b * n;
         const int64_t s = __ldg(rp + r), e = __ldg(rp + r + 1);
         double acc[4] = {0.0, 0.0, 0.0, 0.0};
@@ -337,7 +340,7 @@ __global__ void __launch_bounds__(kBLeanWarps * 32, 4)
             if (fill >= 32) {
                 __syncwarp();
                 float c4[4] = {0.f, 0.f, 0.f, 0.f};
-                lean_chunk<H>(E, 32, g, active, Xb, c4);
+                lean_chunk<H>(E, 32, g, active, Xb, c0a, c4);
 #pragma unroll
                 for (int j = 0; j < 4; ++j) acc[j] += (double)c4[j];
                 __syncwarp();  // every lane has read E[0 .. 32)
@@ -351,7 +354,7 @@ __global__ void __launch_bounds__(kBLeanWarps * 32, 4)
         if (fill > 0) {
             __syncwarp();
             float c4[4] = {0.f, 0.f, 0.f, 0.f};
-            lean_chunk<H>(E, fill, g, active, Xb, c4);
+            lean_chunk<H>(E, fill, g, active, Xb, c0a, c4);
 #pragma unroll
             for (int j = 0; j < 4; ++j) acc[j] += (double)c4[j];
         }
@@ -389,7 +392,8 @@ __global__ void __launch_bounds__(kBLeanWarps * 32, 4)
     int64_t b = 0;
     for (int64_t it = lean_next(next, lane); it < total; it = lean_next(next, lane)) {
         while (coff[b + 1] <= it) ++b;  // a warp's items rise, so b only moves forward
-        const float* Yb = Y + b * m * l + (active ? col0 : 0);
+        const float* Yb = Y + b * m * l;
+        const uint32_t c0a = active ? (uint32_t)col0 : 0u;
         const int32_t c = m2o[it];
         const int64_t s = __ldg(cp + c), e = __ldg(cp + c + 1);
         double acc[4] = {0.0, 0.0, 0.0, 0.0};
@@ -406,7 +410,7 @@ __global__ void __launch_bounds__(kBLeanWarps * 32, 4)
                 myv = __ldg(cv + k0 + 32 + lane);
             }
             float c4[4] = {0.f, 0.f, 0.f, 0.f};
-            lean_chunk<H>(E, cnt, g, active, Yb, c4);
+            lean_chunk<H>(E, cnt, g, active, Yb, c0a, c4);
 #pragma unroll
             for (int j = 0; j < 4; ++j) acc[j] += (double)c4[j];
         }
