@@ -211,7 +211,7 @@ __global__ void __launch_bounds__(kF32Warps * 32, MINB)
     const int col0 = gl * 4;
     const int ncols_here = (l - col0) < 4 ? (l - col0) : 4;
     const bool active = ncols_here > 0;
-    const T* Xl = X + (active ? col0 : 0);
+    const uint32_t c0a = active ? (uint32_t)col0 : 0u;  // gathers at X + a 32-bit offset
     LeanEntry<T>* E = s_ent[w];
     const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -244,7 +244,7 @@ __global__ void __launch_bounds__(kF32Warps * 32, MINB)
                     for (int u = 0; u < U; ++u) {
                         const LeanEntry<T> e = E[(qb + u) * H + g];
                         vv[u] = e.v;
-                        if (active) load4(Xl + e.off, xv[u]);
+                        if (active) load4(X + ((uint32_t)e.off + c0a), xv[u]);
                         else xv[u][0] = xv[u][1] = xv[u][2] = xv[u][3] = T(0);
                     }
 #pragma unroll
@@ -256,7 +256,7 @@ __global__ void __launch_bounds__(kF32Warps * 32, MINB)
                 for (int q = g; q < cnt; q += H) {
                     const LeanEntry<T> e = E[q];
                     T x[4] = {T(0), T(0), T(0), T(0)};
-                    if (active) load4(Xl + e.off, x);
+                    if (active) load4(X + ((uint32_t)e.off + c0a), x);
 #pragma unroll
                     for (int j = 0; j < 4; ++j) c4[j] = fma((CT)e.v, (CT)x[j], c4[j]);
                 }
